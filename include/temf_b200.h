@@ -1,0 +1,182 @@
+/*
+ * temf_b200.h -- C ABI of the B200-native FETD time-stepping hot path.
+ *
+ * Drop-in boundary for TEMF3DT's forward modelling (yxddyxzh2016/TEMF3DT,
+ * Fortran 90).  The reference builds three MKL CSR matrices in mesh_process
+ * and then, inside adap_euler, forms the step matrix with mkl_add_3, factors
+ * and solves it with MKL cluster_sparse_solver through the module
+ * pardiso_multi_real_mpi, and computes the BDF2 right-hand side with
+ * mkl_sparse_d_mv.  Every one of those calls is replaced by a function below.
+ *
+ * Conventions (all chosen so a Fortran caller can pass its arrays unchanged
+ * through ISO_C_BINDING):
+ *   - every index array is 1-based, exactly as in the reference's arrays;
+ *   - two-dimensional arrays are Fortran column-major with the leading
+ *     dimension equal to the first extent, e.g. tet_vex(tet_num,4) is passed
+ *     as a pointer to tet_num*4 ints, vertex 1 of all tets first;
+ *   - all floating point data are double precision (real(8));
+ *   - functions return 0 on success and a negative TEMF_E* code on failure;
+ *     temf_last_error() gives the message.  No function calls exit() or
+ *     stop(): the reference's `stop` on a solver error becomes a status.
+ *   - one context is one GPU and one CUDA stream; a context is not
+ *     thread-safe.  Device memory is owned by the context; host arrays are
+ *     only read (or written) during the call.
+ */
+#ifndef TEMF_B200_H
+#define TEMF_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TEMF_OK 0
+#define TEMF_EARG (-1)     /* invalid argument */
+#define TEMF_ECUDA (-2)    /* CUDA runtime error */
+#define TEMF_ESTATE (-3)   /* call out of order (e.g. solve before factor) */
+#define TEMF_EINTERNAL (-4)
+
+typedef struct temf_ctx temf_ctx;
+
+/* ---- context --------------------------------------------------------- */
+/* Create a context on CUDA device `device`. */
+int temf_create(int device, temf_ctx** ctx);
+int temf_destroy(temf_ctx* ctx);
+/* Text of the last error of this context (never NULL). */
+const char* temf_last_error(const temf_ctx* ctx);
+/* Library version string. */
+const char* temf_version(void);
+
+/* ---- mesh topology helper (host only, no GPU needed) -----------------
+ * Rebuilds the reference's global edge list from tet_vex:
+ * model_mesh, src/FETD_FWD.f90:168-244 (unique sorted (min,max) vertex
+ * pairs in lexicographic order; tet_edg by binary search; tet_drc = +1 when
+ * the first local vertex of the edge has the smaller global index).
+ * Call temf_mesh_count_edges first to size edg_vex. */
+int temf_mesh_count_edges(int n_tets, const int* tet_vex, int* n_edges);
+int temf_mesh_topology(int n_tets, const int* tet_vex, int n_edges, int* edg_vex, int* tet_edg, int* tet_drc);
+
+/* ---- model ---------------------------------------------------------------
+ * temf_set_mesh: the geometry/topology the reference keeps in type(model)
+ * (src/FETD_FWD.f90:33-106): nod_cor(n_nodes,3), tet_vex(n_tets,4),
+ * edg_vex(n_edges,2), tet_edg(n_tets,6), tet_drc(n_tets,6). */
+int temf_set_mesh(temf_ctx* ctx, int n_nodes, const double* nod_cor, int n_tets, const int* tet_vex,
+                  int n_edges, const int* edg_vex, const int* tet_edg, const int* tet_drc);
+/* Per-tet conductivity (S/m) and permeability (H/m): sig_3d and mag_3d of
+ * model_ctl (src/FETD_FWD.f90:347-364).  May be called again to change the
+ * model; temf_assemble must then be repeated. */
+int temf_set_media(temf_ctx* ctx, const double* sig_tet, const double* mu_tet);
+
+/* Ordering + symbolic factorisation of the step-matrix pattern (once per
+ * mesh; replaces the reorder/symbolic half of PARDISO phase 12,
+ * src/FETD_UTILITY.f90:912-917).  Must follow temf_set_mesh. */
+int temf_analyse(temf_ctx* ctx);
+
+/* K1: assemble M_sigma (b_mkl) and the curl-curl matrix K (c_mkl) on the GPU:
+ * mesh_process, src/FETD_FWD.f90:588-711.  Needs temf_analyse and media. */
+int temf_assemble(temf_ctx* ctx);
+
+/* Export an assembled matrix as the reference's 1-based upper-triangular CSR
+ * (what mkl_to_csr returns, src/FETD_FWD.f90:1974-2004), in the original edge
+ * numbering.  which: 0 = M_sigma, 1 = K.  Pass ia = ja = va = NULL to get
+ * *nnz only; otherwise ia has n_edges+1 and ja/va have *nnz entries. */
+int temf_get_matrix(temf_ctx* ctx, int which, int* nnz, int* ia, int* ja, double* va);
+
+/* ---- factor / solve (the pardiso_multi_real_mpi replacement) -------------
+ * temf_factor: A = 3 M_sigma + 2 dt K (mkl_add_3 call sites
+ * src/FETD_FWD.f90:1288,1354) and its numeric LL^T into slot 1 or 2
+ * (pardiso_direct_1, src/FETD_UTILITY.f90:879-936).  Returns 0, a negative
+ * error, or a positive value = 1-based edge index of the first non-positive
+ * pivot (the case in which the reference retries with mtype -2). */
+int temf_factor(temf_ctx* ctx, int slot, double dt);
+/* x = A^{-1} b with the factor in `slot` (pardiso_direct_2,
+ * src/FETD_UTILITY.f90:938-957).  b and x are host arrays of n_edges x nrhs,
+ * column-major with leading dimension ld >= n_edges (original numbering).
+ * b and x may alias. */
+int temf_solve(temf_ctx* ctx, int slot, int nrhs, const double* b, double* x, int ld);
+/* Forget the factor in `slot` (pardiso_direct_3, src/FETD_UTILITY.f90:959-975).
+ * Device memory is kept for reuse until temf_destroy. */
+int temf_release(temf_ctx* ctx, int slot);
+/* y = M_sigma x for host vectors (the mkl_sparse_d_mv of the BDF2 right-hand
+ * side, src/FETD_FWD.f90:1330,1367,1427).  which: 0 = M_sigma, 1 = K. */
+int temf_spmv(temf_ctx* ctx, int which, int nrhs, const double* x, double* y, int ld);
+
+/* ---- sources and receivers -----------------------------------------------
+ * Sources: one edge list per right-hand-side column.  col_ptr[nrhs+1] holds
+ * 0-based offsets into src_edg (1-based edge numbers) and src_drc (+1/-1):
+ * src_edg/src_drc of model_ctl (src/FETD_FWD.f90:435-448).  The waveform is
+ * time_const_p (src/FETD_UTILITY.f90:1050-1078): source_type 1; pulse_type
+ * 1 step-on, 2 impulse, 3 step-off (DC pass first); t0 = pulse width;
+ * current = amplitude.  Repeated edges in a column follow the reference's
+ * assignment semantics (the last entry wins, src/FETD_FWD.f90:1507). */
+int temf_set_sources(temf_ctx* ctx, int nrhs, const int* col_ptr, const int* src_edg, const int* src_drc,
+                     int source_type, int pulse_type, double t0, double current);
+/* Receivers: rec_tet (1-based, from p_in_tet, src/FETD_FWD.f90:1009-1049),
+ * rec_cor(nrec,3), and the RHS column each receiver samples (0-based; NULL =
+ * all column 0).  The interpolation and -curl operators n_arr/d_arr of
+ * src/FETD_FWD.f90:712-731 are built on the GPU. */
+int temf_set_receivers(temf_ctx* ctx, int nrec, const int* rec_tet, const double* rec_cor, const int* rec_rhs);
+/* Copy back n_arr(rec,6,3) and d_arr(rec,6,3) in Fortran layout (checks). */
+int temf_get_receiver_operators(temf_ctx* ctx, double* n_arr, double* d_arr);
+/* Point location on the GPU: for each point, the first tet (in tet order)
+ * whose centroid is within rec_charac and whose five 4x4 determinants share a
+ * sign (p_in_tet, src/FETD_FWD.f90:1009-1049); 0 when none. */
+int temf_locate_points(temf_ctx* ctx, int npts, const double* pts, double rec_charac, int* tet_out);
+
+/* ---- the time loop ----------------------------------------------------------
+ * Runs time_solver/adap_euler (src/FETD_FWD.f90:1174-1464) on the GPU:
+ * sp_division, sp_double, sp_dblesize and time_maximum as in the .cntl file.
+ * flags: bit 0 = legacy time column (the shipped LINUX/*.field files advance
+ * an accepted trial's time by one extra old step), bit 1 = disable CUDA
+ * graphs.  forced (may be NULL): per trial 1 = accept, 0 = reject, -1 = the
+ * reference's own test (used to replay a given schedule).  max_steps 0 = no
+ * limit.  Results are kept in the context; see temf_result_*. */
+int temf_run(temf_ctx* ctx, int sp_division, int sp_double, int sp_dblesize, double time_maximum, int flags,
+             const int* forced, int n_forced, int max_steps);
+/* Number of output rows of the last run (the rows of the .field file). */
+int temf_result_rows(temf_ctx* ctx, int* rows);
+/* Output rows: step(rows), time(rows), dt(rows) and fields(9, nrec, rows)
+ * = ex ey ez dBx/dt dBy/dt dBz/dt bx by bz per receiver, as a_f of
+ * solution_output (src/FETD_FWD.f90:1530-1622), Fortran order (component
+ * fastest).  Any pointer may be NULL. */
+int temf_result_get(temf_ctx* ctx, int* step, double* time, double* dt, double* fields);
+/* Trial statistics: number of trials, errors and accept flags (NULL ok). */
+int temf_result_trials(temf_ctx* ctx, int* n_trials, double* errors, int* accepted);
+/* Time-gate interpolation (.field2, src/FETD_FWD.f90:1625-1640): for each of
+ * n_gates times, fields(9, nrec, n_gates) and a done flag. */
+int temf_result_gates(temf_ctx* ctx, int n_gates, const double* gates, double* fields, int* done);
+/* Timing of the last run in milliseconds (CUDA events): factorisations,
+ * stepping (SpMV+solve+receivers), whole run; counts of factorisations,
+ * solves and kernel launches. */
+int temf_result_timing(temf_ctx* ctx, double* ms_factor, double* ms_steps, double* ms_total, int* n_factor,
+                       int* n_solve, long long* n_launch);
+
+/* ---- statistics of the symbolic analysis ----------------------------------
+ * stats[0..9] = n, nnz(A full), supernodes, levels, nnz(L), stored doubles,
+ * factor flops, update tiles, seconds ordering, seconds symbolic. */
+int temf_analysis_stats(temf_ctx* ctx, double* stats);
+
+/* Host-only ordering + symbolic analysis of a symmetric pattern (no GPU
+ * needed): 0-based adjacency without the diagonal (xadj[n+1], adj), one point
+ * per unknown in xyz(3,n) (x,y,z of each unknown contiguous).  perm_out[new]
+ * = old (0-based).  stats[0..7] = n, supernodes, levels, nnz(L), stored
+ * doubles, factor flops, seconds ordering, seconds symbolic. */
+int temf_symbolic_host(int n, const long long* xadj, const int* adj, const double* xyz, int* perm_out,
+                       double* stats);
+
+/* ---- PARDISO-compatible shim ------------------------------------------------
+ * Same argument meaning as the reference's module pardiso_multi_real_mpi
+ * (src/FETD_UTILITY.f90:826-1028) so adap_euler can keep its five calls.
+ * direct_1 takes the 1-based upper CSR (ia, ja, va) of A; its pattern must be
+ * the assembled step-matrix pattern of the mesh set on the context (the
+ * pattern mkl_add_3 produces), which is checked. */
+int temf_pardiso_alloc(temf_ctx* ctx, int max_matrix);
+int temf_pardiso_direct_1(temf_ctx* ctx, int num_m, int symm, int n, int nnz, const int* ia, const int* ja,
+                          const double* va);
+int temf_pardiso_direct_2(temf_ctx* ctx, int num_m, const double* b, double* x);
+int temf_pardiso_direct_3(temf_ctx* ctx, int num_m);
+int temf_pardiso_dealloc(temf_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TEMF_B200_H */

@@ -1,0 +1,706 @@
+"""CPU FP64 restatement of TEMF3DT's FETD forward path (the oracle).
+
+TEST INFRASTRUCTURE ONLY -- the checker, never the product.  Only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may use it.
+
+Every function restates one routine of the reference (yxddyxzh2016/TEMF3DT,
+Fortran 90) and cites it as ``file:line`` within that project.  The reference
+solves its linear systems with Intel MKL cluster_sparse_solver (PARDISO,
+closed, not vendored; oneAPI 2021.5 per ``src/x64/Release/BuildLog.htm``);
+here the same systems are solved exactly (to FP64 rounding) with SuperLU from
+scipy, which is an independent direct solver.  Nothing here is tuned: the
+restatement keeps the reference's loop structure so the schedule, indexing
+and sign conventions can be compared line by line.
+
+Parity is pinned against the reference's shipped example outputs
+``LINUX/mod_big_sig_0.001.field`` and ``LINUX/mod_small_sig_0.001.field``
+(see ``tests/test_oracle_golden.py``).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+# src/FETD_FWD.f90:14-16
+PI = 3.141592653589793238462643383279502884197
+MU0 = PI * 4.0e-7
+EPS0 = 8.8541878176e-12
+
+# Local edge -> local vertex pair, src/FETD_FWD.f90:23 (ind_tet), 0-based here.
+IND_TET = np.array([[0, 1], [0, 2], [0, 3], [1, 2], [3, 1], [2, 3]], dtype=np.int64)
+
+
+# --------------------------------------------------------------------------
+# Input files
+# --------------------------------------------------------------------------
+def _f(tok: str) -> float:
+    """Fortran list-directed real (accepts ``1.d-12``)."""
+    return float(tok.replace("d", "e").replace("D", "E"))
+
+
+def read_mesh(path: str) -> Dict[str, np.ndarray]:
+    """MEDIT ``.mesh`` reader, src/FETD_FWD.f90:129-166.
+
+    Sections are recognised by the first five characters of the first token
+    (``Verti``, ``Edges``, ``Trian``, ``Tetra``).  Source segments are the
+    ``Edges`` rows whose physical tag is non-zero (src/FETD_FWD.f90:146-151).
+    Indices stay 1-based, as in the reference.
+    """
+    with open(path, "r") as fh:
+        lines = fh.read().splitlines()
+    out: Dict[str, np.ndarray] = {}
+    i, n = 0, len(lines)
+
+    def block(start: int, count: int, ncol: int, conv=float) -> np.ndarray:
+        toks: List[str] = []
+        for ln in lines[start:start + count]:
+            toks.extend(ln.split()[:ncol])
+        arr = np.array([conv(t) for t in toks]) if conv is not float else np.array(
+            [_f(t) for t in toks], dtype=np.float64)
+        return arr.reshape(count, ncol)
+
+    while i < n:
+        toks = lines[i].split()
+        word = toks[0][:5] if toks else ""
+        if word == "Verti":
+            cnt = int(lines[i + 1].split()[0])
+            out["nod_cor"] = block(i + 2, cnt, 3)
+            i += 2 + cnt
+            continue
+        if word == "Edges":
+            cnt = int(lines[i + 1].split()[0])
+            arr = block(i + 2, cnt, 3, int).astype(np.int64)
+            keep = arr[:, 2] != 0
+            out["src_vex"] = arr[keep, :2]
+            out["src_phy"] = arr[keep, 2]
+            i += 2 + cnt
+            continue
+        if word == "Trian":
+            cnt = int(lines[i + 1].split()[0])
+            i += 2 + cnt
+            continue
+        if word == "Tetra":
+            cnt = int(lines[i + 1].split()[0])
+            arr = block(i + 2, cnt, 5, int).astype(np.int64)
+            out["tet_vex"] = arr[:, :4]
+            out["tet_phy"] = arr[:, 4]
+            i += 2 + cnt
+            continue
+        i += 1
+    if "src_vex" not in out:
+        out["src_vex"] = np.zeros((0, 2), dtype=np.int64)
+        out["src_phy"] = np.zeros((0,), dtype=np.int64)
+    return out
+
+
+def _parse_code(line: str):
+    """``parseCode``, src/FETD_UTILITY.f90:678-731 (returns None for comments)."""
+    s = line.replace("\t", " ")
+    st = s.lstrip(" ")
+    if st == "" or st[0] in "%!":
+        return None
+    if ":" not in s:
+        return ("", "")
+    idx = s.index(":")
+    code = s[:idx].strip().lower()
+    val = s[idx + 1:].strip()
+    for c in "%!":
+        j = val.find(c)
+        if j > 0:
+            val = val[:j]
+    return (code, val.strip())
+
+
+@dataclass
+class Control:
+    """The subset of ``type(model)`` filled by ``model_ctl`` (src/FETD_FWD.f90:284-497)."""
+    rec_cor: np.ndarray = None
+    rec_charac: float = 10.0
+    dom_ind: np.ndarray = None
+    sig_dom: np.ndarray = None
+    per_dom: np.ndarray = None
+    mag_dom: np.ndarray = None
+    bound_cond: int = 0
+    src_num: int = 0
+    src_sourcetype: int = 0
+    src_pulsetype: int = 0
+    src_pulsewidth: float = 0.0
+    src_current: float = 0.0
+    step_mthd: int = 0
+    step_dvsi: int = 0
+    time_maxm: float = 0.0
+    step_dble: int = 0
+    step_dblesize: int = 0
+    o_f: np.ndarray = field(default_factory=lambda: np.zeros(9, dtype=bool))
+    time_channels: Optional[np.ndarray] = None
+    vtk_num: int = 0
+
+
+def read_cntl(path: str) -> Control:
+    """``.cntl`` keyword file, src/FETD_FWD.f90:311-487 (isotropic media only)."""
+    c = Control()
+    with open(path, "r") as fh:
+        lines = fh.read().splitlines()
+    i = 0
+    while i < len(lines):
+        pc = _parse_code(lines[i])
+        i += 1
+        if pc is None:
+            continue
+        code, val = pc
+        if code == "time_points":
+            k = int(val.split()[0])
+            c.time_channels = np.array([_f(lines[i + q].split()[0]) for q in range(k)])
+            i += k
+        elif code == "rec_charac":
+            c.rec_charac = _f(val.split()[0])
+        elif code == "receivers":
+            k = int(val.split()[0])
+            c.rec_cor = np.array([[_f(t) for t in lines[i + q].split()[:3]] for q in range(k)])
+            i += k
+        elif code == "isotropic":
+            k = int(val.split()[0])
+            rows = [lines[i + q].split() for q in range(k)]
+            i += k
+            c.dom_ind = np.array([int(r[0]) for r in rows])
+            c.sig_dom = np.array([_f(r[1]) for r in rows])
+            c.per_dom = np.array([_f(r[2]) for r in rows]) * EPS0
+            c.mag_dom = np.array([_f(r[3]) for r in rows]) * MU0
+        elif code == "anisotropic":
+            raise NotImplementedError("anisotropic media are outside the restated path")
+        elif code == "boundary condition":
+            c.bound_cond = int(val.split()[0])
+        elif code == "source":
+            c.src_num = int(val.split()[0])
+            t = lines[i].split()
+            i += 1
+            c.src_sourcetype, c.src_pulsetype = int(t[0]), int(t[1])
+            c.src_pulsewidth, c.src_current = _f(t[2]), _f(t[3])
+        elif code == "sp_mthd":
+            c.step_mthd = int(val.split()[0])
+        elif code == "sp_division":
+            c.step_dvsi = int(val.split()[0])
+        elif code == "time_maximum":
+            c.time_maxm = _f(val.split()[0])
+        elif code == "sp_double":
+            c.step_dble = int(val.split()[0])
+        elif code == "sp_dblesize":
+            c.step_dblesize = int(val.split()[0])
+        elif code == "output":
+            t = lines[i].split()
+            i += 1
+            c.o_f = np.array([int(x) == 1 for x in t[:9]])
+        elif code == "vtkout":
+            c.vtk_num = int(val.split()[0])
+            i += max(c.vtk_num, 0)
+    # src/FETD_FWD.f90:490-497
+    if c.rec_cor is None or len(c.rec_cor) == 0:
+        raise ValueError("cmod%rec_num error")
+    if c.dom_ind is None:
+        raise ValueError("cmod%dom_num error")
+    if c.src_num == 0:
+        raise ValueError("cmod%src_num error")
+    if c.step_mthd == 0 or c.step_dvsi == 0 or abs(c.time_maxm) < 1e-20 or c.step_dble == 0:
+        raise ValueError("time control error")
+    if not c.o_f.any():
+        raise ValueError("cmod%o_f error")
+    return c
+
+
+# --------------------------------------------------------------------------
+# Topology and geometry (model_mesh)
+# --------------------------------------------------------------------------
+def _bsearch_pair(e1: np.ndarray, e2: np.ndarray, va: int, vb: int) -> int:
+    """``bSearch_Ii`` (src/FETD_UTILITY.f90:623-676): 1-based index or 0."""
+    lo = int(np.searchsorted(e1, va, side="left"))
+    hi = int(np.searchsorted(e1, va, side="right"))
+    if lo == hi:
+        return 0
+    k = int(np.searchsorted(e2[lo:hi], vb, side="left"))
+    if k < hi - lo and e2[lo + k] == vb:
+        return lo + k + 1
+    return 0
+
+
+def build_topology(tet_vex: np.ndarray):
+    """Global edges and per-tet edge map, src/FETD_FWD.f90:168-244.
+
+    Edges are the unique (min,max) vertex pairs in lexicographic order
+    (``unique_ii`` -> ``sort_ii``, src/FETD_UTILITY.f90:358-429).  ``tet_drc``
+    is +1 when the first local vertex of the edge has the lower global index.
+    """
+    T = tet_vex.shape[0]
+    p = tet_vex[:, IND_TET[:, 0]]
+    q = tet_vex[:, IND_TET[:, 1]]
+    lo = np.minimum(p, q).reshape(-1)
+    hi = np.maximum(p, q).reshape(-1)
+    pairs = np.unique(np.stack([lo, hi], axis=1), axis=0)  # lexicographic
+    edg_vex = pairs
+    key_all = lo * (int(tet_vex.max()) + 1) + hi
+    key_edg = edg_vex[:, 0] * (int(tet_vex.max()) + 1) + edg_vex[:, 1]
+    tet_edg = (np.searchsorted(key_edg, key_all) + 1).reshape(T, 6)
+    tet_drc = np.where(p < q, 1, -1).astype(np.int64)
+    return edg_vex, tet_edg, tet_drc
+
+
+def _det3(m: np.ndarray) -> np.ndarray:
+    return np.linalg.det(m)
+
+
+def geometry(nod_cor: np.ndarray, tet_vex: np.ndarray):
+    """Simplex coefficients a,b,c,d, volume and edge lengths, src/FETD_FWD.f90:245-281.
+
+    a_k, b_k, c_k, d_k are the signed 3x3 minors such that the barycentric
+    coordinate of vertex k is (a_k + b_k x + c_k y + d_k z) / (6 V), with
+    V = det([1 x y z]) / 6 (``tet_volume``, src/FETD_UTILITY.f90:105-112).
+    """
+    X = nod_cor[tet_vex - 1]  # (T,4,3)
+    x, y, z = X[..., 0], X[..., 1], X[..., 2]
+    T = X.shape[0]
+    one = np.ones((T, 3))
+    rest = {0: [1, 2, 3], 1: [0, 2, 3], 2: [0, 1, 3], 3: [0, 1, 2]}
+    a = np.empty((T, 4)); b = np.empty((T, 4)); c = np.empty((T, 4)); d = np.empty((T, 4))
+    sa = [1.0, -1.0, 1.0, -1.0]
+    sb = [-1.0, 1.0, -1.0, 1.0]
+    for k in range(4):
+        r = rest[k]
+        a[:, k] = sa[k] * _det3(np.stack([x[:, r], y[:, r], z[:, r]], axis=2))
+        b[:, k] = sb[k] * _det3(np.stack([one, y[:, r], z[:, r]], axis=2))
+        c[:, k] = sa[k] * _det3(np.stack([one, x[:, r], z[:, r]], axis=2))
+        d[:, k] = sb[k] * _det3(np.stack([one, x[:, r], y[:, r]], axis=2))
+    vol = np.linalg.det(np.stack([np.ones((T, 4)), x, y, z], axis=2)) / 6.0
+    P = X[:, IND_TET[:, 0], :]
+    Q = X[:, IND_TET[:, 1], :]
+    tet_len = np.sqrt(((P - Q) ** 2).sum(axis=2))
+    return a, b, c, d, vol, tet_len
+
+
+# --------------------------------------------------------------------------
+# Element integrals and assembly (mesh_process)
+# --------------------------------------------------------------------------
+def f_kind_iso(b, c, d, vol, tet_len, scal):
+    """Mass integral  s * int N_i . N_j dV, src/FETD_FWD.f90:826-851 (all tets at once)."""
+    G = np.stack([b, c, d], axis=2)                 # (T,4,3)
+    gram = np.einsum("tkx,tlx->tkl", G, G)          # (T,4,4)
+    F = np.empty((G.shape[0], 6, 6))
+    for i in range(6):
+        pi_, qi = IND_TET[i]
+        for j in range(6):
+            pj, qj = IND_TET[j]
+            v = (gram[:, qi, qj] * (1 + (pi_ == pj))
+                 - gram[:, pi_, qj] * (1 + (qi == pj))
+                 - gram[:, qi, pj] * (1 + (pi_ == qj))
+                 + gram[:, pi_, pj] * (1 + (qi == qj)))
+            F[:, i, j] = tet_len[:, i] * tet_len[:, j] / (720.0 * vol) * v
+    return F * scal[:, None, None]
+
+
+def e_kind_iso(b, c, d, vol, tet_len, scal):
+    """Curl-curl integral  s * int curl N_i . curl N_j dV, src/FETD_FWD.f90:797-824."""
+    G = np.stack([b, c, d], axis=2)
+    t = np.cross(G[:, IND_TET[:, 0], :], G[:, IND_TET[:, 1], :])   # (T,6,3)
+    dots = np.einsum("tix,tjx->tij", t, t)
+    coef = 4.0 * vol / (6.0 * vol) ** 4
+    E = tet_len[:, :, None] * tet_len[:, None, :] * coef[:, None, None] * dots
+    return E * scal[:, None, None]
+
+
+def assemble_upper(n_edges: int, tet_edg, tet_drc, emat) -> sp.csr_matrix:
+    """Upper-triangle COO scatter with orientation signs + COO->CSR duplicate sum.
+
+    src/FETD_FWD.f90:642-662 (scatter), :696-709 (mkl_sparse_d_create_coo /
+    convert_csr).  Returns the 0-based upper-triangular CSR.
+    """
+    rows = np.repeat(tet_edg[:, :, None], 6, axis=2)
+    cols = np.repeat(tet_edg[:, None, :], 6, axis=1)
+    sgn = tet_drc[:, :, None] * tet_drc[:, None, :]
+    keep = rows <= cols
+    m = sp.coo_matrix(((emat * sgn)[keep], (rows[keep] - 1, cols[keep] - 1)),
+                      shape=(n_edges, n_edges)).tocsr()
+    m.sum_duplicates()
+    m.sort_indices()
+    return m
+
+
+def full_from_upper(u: sp.csr_matrix) -> sp.csr_matrix:
+    """Symmetric matrix described by its upper triangle (MKL DESCR SYMMETRIC/UPPER,
+    src/FETD_FWD.f90:1191-1193)."""
+    return (u + u.T - sp.diags(u.diagonal())).tocsr()
+
+
+def receiver_operators(a, b, c, d, vol, tet_len, rec_tet, rec_cor):
+    """n_arr (E interpolation) and d_arr (= -curl N_j), src/FETD_FWD.f90:712-731."""
+    R = len(rec_tet)
+    n_arr = np.zeros((R, 6, 3)); d_arr = np.zeros((R, 6, 3))
+    for r in range(R):
+        it = rec_tet[r] - 1
+        x, y, z = rec_cor[r]
+        for j in range(6):
+            p, q = IND_TET[j]
+            lp = a[it, p] + b[it, p] * x + c[it, p] * y + d[it, p] * z
+            lq = a[it, q] + b[it, q] * x + c[it, q] * y + d[it, q] * z
+            gp = np.array([b[it, p], c[it, p], d[it, p]])
+            gq = np.array([b[it, q], c[it, q], d[it, q]])
+            s = tet_len[it, j] / (6.0 * vol[it]) ** 2
+            n_arr[r, j] = (lp * gq - lq * gp) * s
+            cr = np.array([c[it, p] * d[it, q] - c[it, q] * d[it, p],
+                           b[it, q] * d[it, p] - b[it, p] * d[it, q],
+                           b[it, p] * c[it, q] - b[it, q] * c[it, p]])
+            d_arr[r, j] = -2.0 * cr * s
+    return n_arr, d_arr
+
+
+def p_in_tet(nod_cor, tet_vex, p, rec_charac: float) -> int:
+    """Receiver point location, src/FETD_FWD.f90:1009-1049 (1-based tet, 0 = none)."""
+    X = nod_cor[tet_vex - 1]
+    mid = X.mean(axis=1)
+    cand = np.nonzero(np.sqrt(((mid - p) ** 2).sum(axis=1)) <= rec_charac)[0]
+    for i in cand:
+        M = np.concatenate([X[i], np.ones((4, 1))], axis=1)
+        dets = [np.linalg.det(M)]
+        for k in range(4):
+            Mk = M.copy()
+            Mk[k, :3] = p
+            dets.append(np.linalg.det(Mk))
+        dets = np.array(dets)
+        if (dets >= 0).all() or (dets <= 0).all():
+            return int(i) + 1
+    return 0
+
+
+# --------------------------------------------------------------------------
+# Source waveforms (source_mod)
+# --------------------------------------------------------------------------
+def erfstepon1(t: float, t0: float) -> float:
+    """src/FETD_UTILITY.f90:1088-1093 (first derivative of the erf step)."""
+    return (1.0 / math.sqrt(3.141592653589793) * math.exp(1.0 / t0 ** 2 * (t - t0 / 2.0) ** 2 * (-25.0)) * 5.0) / t0
+
+
+def deltafunc1(t: float, t0: float) -> float:
+    """src/FETD_UTILITY.f90:1144-1147 (first derivative of the impulse)."""
+    return (-1.0 / t0 ** 2 * math.exp(-1.0 / t0 ** 2 * (t * 5.436563656918091 - t0 * 2.718281828459046) ** 2)
+            * (t * 59.11244879144521 - t0 * 29.55622439572261))
+
+
+def time_const_p(source_type: int, pulse_type: int, t: float, t0: float, cur: float) -> float:
+    """src/FETD_UTILITY.f90:1050-1078."""
+    if source_type == 1 and pulse_type == 1:
+        return erfstepon1(t, t0) * cur
+    if source_type == 1 and pulse_type == 2:
+        return deltafunc1(t, t0) * cur
+    if source_type == 1 and pulse_type == 3:
+        return -erfstepon1(t, t0) * cur
+    raise ValueError("no such kind of source")
+
+
+# --------------------------------------------------------------------------
+# The model (model_mesh + model_ctl + mesh_process)
+# --------------------------------------------------------------------------
+@dataclass
+class OracleModel:
+    nod_cor: np.ndarray
+    tet_vex: np.ndarray
+    tet_phy: np.ndarray
+    edg_vex: np.ndarray
+    tet_edg: np.ndarray
+    tet_drc: np.ndarray
+    edg_len: np.ndarray
+    sig: np.ndarray
+    mag: np.ndarray
+    B: sp.csr_matrix          # sigma-mass, upper triangle (b_mkl)
+    C: sp.csr_matrix          # curl-curl, upper triangle (c_mkl)
+    src_edg: np.ndarray       # 1-based
+    src_drc: np.ndarray
+    rec_tet: np.ndarray       # 1-based
+    rec_cor: np.ndarray
+    n_arr: np.ndarray
+    d_arr: np.ndarray
+    ctl: Control
+
+    @property
+    def n(self) -> int:
+        return self.edg_vex.shape[0]
+
+
+def source_edges(edg_vex, src_vex):
+    """src_edg by scanning the edge list; src_drc hack (+1, last = -1),
+    src/FETD_FWD.f90:435-448."""
+    nseg = src_vex.shape[0]
+    src_edg = np.zeros(nseg, dtype=np.int64)
+    for i in range(nseg):
+        lo, hi = min(src_vex[i]), max(src_vex[i])
+        k = _bsearch_pair(edg_vex[:, 0], edg_vex[:, 1], lo, hi)
+        if k == 0:
+            raise ValueError("source segment %d is not a mesh edge" % (i + 1))
+        src_edg[i] = k
+    src_drc = np.ones(nseg, dtype=np.int64)
+    if nseg:
+        src_drc[-1] = -1
+    return src_edg, src_drc
+
+
+def build_model(mesh: Dict[str, np.ndarray], ctl: Control,
+                src_edg=None, src_drc=None, rec_tet=None) -> OracleModel:
+    nod_cor, tet_vex, tet_phy = mesh["nod_cor"], mesh["tet_vex"], mesh["tet_phy"]
+    edg_vex, tet_edg, tet_drc = build_topology(tet_vex)
+    a, b, c, d, vol, tet_len = geometry(nod_cor, tet_vex)
+    edg_len = np.sqrt(((nod_cor[edg_vex[:, 0] - 1] - nod_cor[edg_vex[:, 1] - 1]) ** 2).sum(axis=1))
+    # per-tet media, src/FETD_FWD.f90:347-364
+    sig = np.empty(tet_vex.shape[0]); mag = np.empty(tet_vex.shape[0])
+    found = np.zeros(tet_vex.shape[0], dtype=bool)
+    for j, dom in enumerate(ctl.dom_ind):
+        m = tet_phy == dom
+        sig[m] = ctl.sig_dom[j]; mag[m] = ctl.mag_dom[j]; found |= m
+    if not found.all():
+        raise ValueError("error - physical domain not found!")
+    if ctl.bound_cond != 0:
+        raise NotImplementedError("first-order ABC is outside the restated path")
+    n = edg_vex.shape[0]
+    Bm = assemble_upper(n, tet_edg, tet_drc, f_kind_iso(b, c, d, vol, tet_len, sig))
+    Cm = assemble_upper(n, tet_edg, tet_drc, e_kind_iso(b, c, d, vol, tet_len, 1.0 / mag))
+    if src_edg is None:
+        src_edg, src_drc = source_edges(edg_vex, mesh["src_vex"])
+    if rec_tet is None:
+        rec_tet = np.array([p_in_tet(nod_cor, tet_vex, p, ctl.rec_charac) for p in ctl.rec_cor])
+        if (rec_tet == 0).any():
+            raise ValueError("no rec tet No. %d" % (int(np.argmin(rec_tet)) + 1))
+    n_arr, d_arr = receiver_operators(a, b, c, d, vol, tet_len, rec_tet, ctl.rec_cor)
+    return OracleModel(nod_cor, tet_vex, tet_phy, edg_vex, tet_edg, tet_drc, edg_len, sig, mag,
+                       Bm, Cm, np.asarray(src_edg), np.asarray(src_drc), np.asarray(rec_tet),
+                       ctl.rec_cor, n_arr, d_arr, ctl)
+
+
+# --------------------------------------------------------------------------
+# Time stepping (time_solver / adap_euler / sys_right / solution_output)
+# --------------------------------------------------------------------------
+def two_error(a: np.ndarray, b: np.ndarray) -> float:
+    """||a - b||_2 / ||b||_2, src/FETD_UTILITY.f90:578-599."""
+    return float(np.sqrt(np.sum((a - b) ** 2)) / np.sqrt(np.sum(b * b)))
+
+
+def interp_lin(x1, y1, x2, y2, x0):
+    """src/FETD_UTILITY.f90:21-31."""
+    a = (y1 - y2) / (x1 - x2)
+    return a * x0 + (y1 - a * x1)
+
+
+class SuperLUSlots:
+    """Two factor slots, the role of ``pardiso_multi_real_mpi`` (src/FETD_UTILITY.f90:826-1028)."""
+
+    def __init__(self, model: OracleModel):
+        self.B = full_from_upper(model.B)
+        self.C = full_from_upper(model.C)
+        self.slots: Dict[int, object] = {}
+        self.n_factor = 0
+        self.n_solve = 0
+
+    def factor(self, slot: int, dt: float) -> None:
+        A = (3.0 * self.B + (2.0 * dt) * self.C).tocsc()   # mkl_add_3, src/FETD_FWD.f90:2006-2039
+        self.slots[slot] = spla.splu(A, permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.0,
+                                     options={"SymmetricMode": True})
+        self.n_factor += 1
+
+    def solve(self, slot: int, rhs: np.ndarray) -> np.ndarray:
+        self.n_solve += 1
+        return self.slots[slot].solve(rhs)
+
+    def release(self, slot: int) -> None:
+        self.slots.pop(slot, None)
+
+    def spmv_B(self, x: np.ndarray) -> np.ndarray:
+        return self.B @ x
+
+
+@dataclass
+class FetdResult:
+    steps: List[int]
+    times: List[float]
+    dts: List[float]
+    fields: np.ndarray           # (rows, rec, 9): ex ey ez dx dy dz bx by bz
+    channels: Dict[int, np.ndarray]
+    trial_errors: List[float]
+    trial_accepted: List[bool]
+    final_e: Optional[np.ndarray] = None
+
+
+class _Output:
+    """``solution_output`` (src/FETD_FWD.f90:1513-1641) without file writing."""
+
+    def __init__(self, model: OracleModel):
+        self.m = model
+        self.rows: List[np.ndarray] = []
+        self.steps: List[int] = []
+        self.times: List[float] = []
+        self.dts: List[float] = []
+        chan = model.ctl.time_channels
+        self.chan_t = chan if chan is not None else np.zeros(0)
+        self.chan_ok = np.zeros(len(self.chan_t), dtype=bool)
+        self.chan_val: Dict[int, np.ndarray] = {}
+
+    def __call__(self, step: int, t: float, step_cur: float, e: np.ndarray) -> None:
+        m = self.m
+        R = len(m.rec_tet)
+        row = np.zeros((R, 9))
+        for r in range(R):
+            it = m.rec_tet[r] - 1
+            ev = m.tet_drc[it] * e[m.tet_edg[it] - 1]          # (6,)
+            row[r, 0:3] = (m.n_arr[r] * ev[:, None]).sum(axis=0)
+            row[r, 3:6] = (m.d_arr[r] * ev[:, None]).sum(axis=0)
+        if step == 0:
+            row[:, 3:6] = 0.0
+        if not self.rows:
+            row[:, 6:9] = row[:, 3:6] * step_cur
+        else:
+            row[:, 6:9] = self.rows[-1][:, 6:9] + row[:, 3:6] * step_cur
+        self.rows.append(row)
+        self.steps.append(step); self.times.append(t); self.dts.append(step_cur)
+        ind_f = len(self.rows)
+        for i in range(len(self.chan_t)):
+            if t >= self.chan_t[i] and not self.chan_ok[i]:
+                if ind_f == 1:
+                    self.chan_val[i] = row.copy()
+                    break                      # the reference exits the channel loop here
+                self.chan_val[i] = interp_lin(self.times[-2], self.rows[-2], t, row, self.chan_t[i])
+                self.chan_ok[i] = True
+
+
+def adap_euler(model: OracleModel, slots: SuperLUSlots, out: Optional[_Output],
+               pulse_sign: float = 1.0, res_e: Optional[np.ndarray] = None,
+               max_steps: Optional[int] = None, time_maximum: Optional[float] = None,
+               legacy_time_column: bool = False):
+    """Adaptive BDF2 time loop, src/FETD_FWD.f90:1229-1464.
+
+    ``pulse_sign`` = -1 reproduces the ``r_h = -r_h`` of the DC pass of pulse
+    type 3 (:1322,1364,1426).  ``legacy_time_column`` reproduces the time
+    column of the shipped ``LINUX/*.field`` files, which advance the time of an
+    accepted doubling trial by one extra old step compared with the source's
+    ``tmp_time_cur = time_cur - step_cur + tmp_step_cur`` (:1350); the field
+    values themselves do not depend on it once the source is off.
+    """
+    ctl = model.ctl
+    n = model.n
+    dbl = ctl.step_dble
+    dsz = ctl.step_dblesize
+    if dbl < dsz + 2:
+        raise ValueError("sp_double must exceed sp_dblesize + 1 (history indexing, :1365)")
+    step = 0
+    time_cur = 0.0
+    not_changed = 0
+    step_cur = ctl.src_pulsewidth / ctl.step_dvsi        # time_solver :1188
+    time_limit = ctl.time_maxm if time_maximum is None else time_maximum
+    all_e: List[np.ndarray] = []                           # all_e(1:all_e_index,:)
+    errors: List[float] = []
+    accepted: List[bool] = []
+
+    def rhs_at(step_, t_, dt_, x2, x3):
+        r_h = np.zeros(n)
+        if step_ < ctl.step_dvsi:                          # sys_right, :1484
+            didt = time_const_p(ctl.src_sourcetype, ctl.src_pulsetype, t_, ctl.src_pulsewidth, ctl.src_current)
+            for i in range(len(model.src_edg)):
+                k = model.src_edg[i] - 1
+                r_h[k] = didt * model.src_drc[i] * model.edg_len[k]
+        r_h = pulse_sign * r_h
+        return slots.spmv_B(4.0 * x2 - x3) - 2.0 * dt_ * r_h
+
+    e1 = e2 = e3 = None
+    ind = 1
+    while time_cur < time_limit:
+        if max_steps is not None and step >= max_steps:
+            break
+        step += 1
+        time_cur += step_cur
+        if step == 1:
+            e1 = np.zeros(n); e2 = np.zeros(n); e3 = np.zeros(n)
+            if res_e is not None:
+                e2 = res_e.copy(); e3 = res_e.copy()
+            if out is not None:
+                out(0, time_cur - step_cur, step_cur, e2)
+            slots.factor(ind, step_cur)
+        if step % dbl == 0:
+            tmp_e2, tmp_e3 = e2.copy(), e3.copy()
+            tmp_time_cur, tmp_step_cur = time_cur, step_cur
+            e_record_1 = None
+            for i in range(1, dsz + 1):
+                rh = rhs_at(step, tmp_time_cur, tmp_step_cur, tmp_e2, tmp_e3)
+                tmp_e1 = slots.solve(ind, rh)
+                if i == dsz:
+                    break
+                if i == 1:
+                    e_record_1 = tmp_e1
+                tmp_e3, tmp_e2 = tmp_e2, tmp_e1
+                tmp_time_cur += tmp_step_cur
+            e_veri_1 = tmp_e1
+            tmp_step_cur = step_cur * dsz
+            tmp_time_cur = time_cur - step_cur + tmp_step_cur
+            other = 2 if ind == 1 else 1
+            slots.factor(other, tmp_step_cur)
+            rh = rhs_at(step, tmp_time_cur, tmp_step_cur, all_e[-1], all_e[-1 - dsz])
+            e_veri_2 = slots.solve(other, rh)
+            error = two_error(e_veri_2, e_veri_1)
+            errors.append(error)
+            if error > 1.0e-4 and not_changed < 2:         # :1382
+                accepted.append(False)
+                slots.release(other)
+                e1 = e_record_1
+                if out is not None:
+                    out(step, time_cur, step_cur, e1)
+                e3, e2 = e2, e1
+                not_changed += 1
+                all_e = []
+            else:
+                accepted.append(True)
+                slots.release(ind)
+                ind = other
+                e3 = all_e[-1]
+                e2 = e_veri_1
+                time_cur = tmp_time_cur + (step_cur if legacy_time_column else 0.0)
+                step_cur = tmp_step_cur
+                if out is not None:
+                    out(step, time_cur, step_cur, e2)
+                not_changed = 0
+                all_e = []
+            continue
+        rh = rhs_at(step, time_cur, step_cur, e2, e3)
+        e1 = slots.solve(ind, rh)
+        if out is not None:
+            out(step, time_cur, step_cur, e1)
+        all_e.append(e1)
+        e3, e2 = e2, e1
+    slots.release(ind)
+    return e1, errors, accepted
+
+
+def run_fetd(model: OracleModel, max_steps: Optional[int] = None, time_maximum: Optional[float] = None,
+             legacy_time_column: bool = False) -> FetdResult:
+    """``time_solver`` (src/FETD_FWD.f90:1174-1227) with MKL replaced by SuperLU."""
+    slots = SuperLUSlots(model)
+    out = _Output(model)
+    ctl = model.ctl
+    if ctl.step_mthd != 2:
+        raise NotImplementedError("only sp_mthd 2 (adaptive BDF2) is implemented by the reference")
+    if ctl.src_pulsetype == 3:
+        # DC pass with the negated (turn-on) source, then the turn-off pass (:1212-1215)
+        res_e, _, _ = adap_euler(model, slots, None, pulse_sign=-1.0, max_steps=None,
+                                 time_maximum=time_maximum)
+        e_last, errs, acc = adap_euler(model, slots, out, res_e=res_e, max_steps=max_steps,
+                                       time_maximum=time_maximum, legacy_time_column=legacy_time_column)
+    else:
+        e_last, errs, acc = adap_euler(model, slots, out, max_steps=max_steps, time_maximum=time_maximum,
+                                       legacy_time_column=legacy_time_column)
+    return FetdResult(out.steps, out.times, out.dts, np.array(out.rows), out.chan_val, errs, acc, e_last)
+
+
+def read_field(path: str) -> np.ndarray:
+    """Parse a ``.field`` file written by ``solution_output`` (src/FETD_FWD.f90:1623)."""
+    rows = []
+    with open(path) as fh:
+        for ln in fh:
+            t = ln.split()
+            if t:
+                rows.append([float(v) for v in t])
+    return np.array(rows)

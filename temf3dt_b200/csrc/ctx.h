@@ -1,0 +1,125 @@
+// The library context: mesh, media, assembled matrices, symbolic plan,
+// factor slots and the state of a running FETD simulation.
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "symbolic.h"
+
+namespace temf {
+
+// Permuted full-symmetric CSR of the step-matrix pattern plus the list of
+// element-matrix entries that sum into each nonzero (deterministic assembly).
+struct Pattern {
+  int n = 0;
+  int64_t nnz = 0;
+  std::vector<int> rowptr;       // n+1 (int32: nnz < 2^31 is checked)
+  std::vector<int> col;          // nnz, ascending per row
+  std::vector<int> contrib_ptr;  // nnz+1
+  std::vector<int> contrib_idx;  // packed element entry: k * n_tets + t, k in [0,21)
+};
+
+// One entry of the factor update schedule: a 64x64 tile (rows i0.., cols j0..)
+// of the Schur update L21 * L21^T of supernode s (indices into its row list).
+struct UpdTile {
+  int s;
+  int i0;
+  int j0;
+};
+
+struct FactorPlan {
+  // device copies of the supernode partition
+  DBuf<int> sn_first, sn_parent, sn_rows, level_sn;
+  DBuf<int64_t> sn_rows_ptr, sn_Lptr;
+  std::vector<int> level_ptr;  // host
+  // A -> L load map (lower triangle incl. diagonal of the permuted CSR)
+  DBuf<int> a2l_src;           // CSR position
+  DBuf<int64_t> a2l_dst;       // offset into the panels
+  int64_t n_a2l = 0;
+  // update scatter metadata
+  DBuf<int> row_grp;           // per below-diagonal row entry: global target-group id
+  DBuf<int> grp_target, grp_jfirst;
+  DBuf<int64_t> grp_relind;    // offset of the group's relative-index run
+  DBuf<int> relind;
+  DBuf<UpdTile> tiles;
+  std::vector<int64_t> tile_level_ptr;  // host, nlevels+1
+  int64_t n_relind = 0;
+  int64_t n_tiles = 0;
+};
+
+struct SolvePlan {
+  DBuf<int64_t> uoff;          // nsn+1: offsets of the per-supernode update vectors
+  DBuf<int64_t> in_ptr;        // n+1: incoming update entries per column
+  DBuf<int64_t> in_idx;        // positions in the update buffer
+  int64_t u_len = 0;
+};
+
+struct FactorSlot {
+  DBuf<double> L;
+  bool valid = false;
+  double dt = 0.0;
+  int status = 0;
+};
+
+struct Source {
+  int nrhs = 0;
+  int source_type = 1, pulse_type = 1;
+  double t0 = 0.0, current = 0.0;
+  // per RHS column: source entries (permuted edge index, drc*len)
+  std::vector<int> ptr;        // nrhs+1
+  std::vector<int> idx;        // permuted unknown index
+  std::vector<int> rhs_col;    // which RHS column each entry belongs to
+  std::vector<double> coef;    // drc * edge length
+  DBuf<int> d_idx, d_col;
+  DBuf<double> d_coef;
+};
+
+struct Receivers {
+  int nrec = 0;
+  std::vector<int> rec_tet;    // 0-based
+  std::vector<int> rec_rhs;    // RHS column each receiver reads
+  std::vector<double> xyz;     // nrec*3
+  DBuf<int> d_edges;           // nrec*6 permuted unknown indices
+  DBuf<int> d_rhs;
+  DBuf<double> d_w;            // nrec*36: rows (ex,ey,ez,dx,dy,dz) x 6 edges, tet_drc folded in
+  std::vector<double> w_host;  // same, copied back (n_arr/d_arr for checks)
+};
+
+}  // namespace temf
+
+struct temf_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // mesh (0-based, row-major per tet)
+  int n_nodes = 0, n_tets = 0, n_edges = 0;
+  std::vector<double> xyz;       // n_nodes*3
+  std::vector<int> tet_vex;      // n_tets*4
+  std::vector<int> edg_vex;      // n_edges*2
+  std::vector<int> tet_edg;      // n_tets*6
+  std::vector<int> tet_drc;      // n_tets*6
+  std::vector<double> sig, mu;   // per tet
+  bool have_mesh = false, have_media = false;
+  // symbolic + pattern
+  temf::SymbolicOptions sym_opt;
+  temf::Symbolic sym;
+  temf::Pattern pat;
+  bool analysed = false;
+  // device mesh / matrices
+  temf::DBuf<double> d_xyz, d_sig, d_mu;
+  temf::DBuf<int> d_tet_vex, d_tet_drc;
+  temf::DBuf<int> d_rowptr, d_col, d_contrib_ptr, d_contrib_idx;
+  temf::DBuf<double> d_elemM, d_elemK, d_M, d_K;
+  bool assembled = false;
+  temf::FactorPlan fplan;
+  temf::SolvePlan splan;
+  temf::FactorSlot slots[2];
+  temf::DBuf<int> d_status;      // device status words (pivot failure etc.)
+  temf::Source src;
+  temf::Receivers rec;
+  // scratch vectors
+  temf::DBuf<double> d_u;        // solve update buffer (u_len * nrhs)
+  int u_nrhs = 0;
+};

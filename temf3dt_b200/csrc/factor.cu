@@ -1,0 +1,338 @@
+// K2 + K3: step-matrix formation and supernodal numeric Cholesky on the GPU.
+//
+// Replaces mkl_add_3 + mkl_to_csr (src/FETD_FWD.f90:2006-2039, 1974-2004)
+// and the numeric part of PARDISO phase 12 (src/FETD_UTILITY.f90:912-917,
+// mtype 2 = real SPD).  A(dt) = 0*A_eps + 3*M_sigma + 2*dt*K is formed
+// directly into the supernodal panels (the pattern is dt-independent).
+//
+// Schedule: bottom-up levels of the supernodal elimination tree.  Per level:
+//   k_potrf_trsm : one CTA per supernode: dense Cholesky of the (<=64 x 64)
+//                  diagonal block in shared memory, then the below-diagonal
+//                  rows solved against it (one row per thread, in registers).
+//   k_update     : the Schur update L21 L21^T of every supernode of the level,
+//                  in 64x64 tiles on the FP64 tensor cores (DMMA
+//                  mma.sync.m8n8k4.f64), scattered into the ancestor panels
+//                  through precomputed relative indices.  Several supernodes
+//                  of one level may update the same ancestor entry, so the
+//                  scatter uses FP64 atomics (red.global.add.f64).
+// Pivot failures are reported through a status word (first failing column),
+// never by trapping.
+#include <algorithm>
+#include <climits>
+
+#include "factor.h"
+
+namespace temf {
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+__global__ void k_load_A(int64_t n, const int* __restrict__ src, const int64_t* __restrict__ dst,
+                         const double* __restrict__ M, double a, const double* __restrict__ K, double b,
+                         double* __restrict__ L) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int p = src[q];
+  L[dst[q]] = a * M[p] + b * K[p];
+}
+
+constexpr int kFacThreads = 128;
+
+__global__ void __launch_bounds__(kFacThreads) k_potrf_trsm(
+    const int* __restrict__ level_sn, const int* __restrict__ sn_first,
+    const int64_t* __restrict__ rows_ptr, const int64_t* __restrict__ Lptr, double* __restrict__ L,
+    int* __restrict__ status) {
+  constexpr int CB = kSnCols;
+  __shared__ double D[CB][CB + 1];
+  const int s = level_sn[blockIdx.x];
+  const int f = sn_first[s];
+  const int c = sn_first[s + 1] - f;
+  const int64_t r = rows_ptr[s + 1] - rows_ptr[s];
+  const int64_t ld = c + r;
+  double* P = L + Lptr[s];
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < c * c; idx += blockDim.x) {
+    const int j = idx / c, i = idx % c;
+    D[i][j] = (i >= j) ? P[(int64_t)j * ld + i] : 0.0;
+  }
+  __syncthreads();
+  for (int k = 0; k < c; ++k) {
+    if (tid == 0) {
+      double d = D[k][k];
+      if (!(d > 0.0)) {  // non-positive or NaN pivot: record and continue with 1
+        atomicMin(status, f + k + 1);
+        d = 1.0;
+      }
+      D[k][k] = sqrt(d);
+    }
+    __syncthreads();
+    const double piv = D[k][k];
+    for (int i = k + 1 + tid; i < c; i += blockDim.x) D[i][k] /= piv;
+    __syncthreads();
+    const int m = c - k - 1;
+    for (int idx = tid; idx < m * m; idx += blockDim.x) {
+      const int jj = k + 1 + idx / m, ii = k + 1 + idx % m;
+      if (ii >= jj) D[ii][jj] -= D[ii][k] * D[jj][k];
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < c * c; idx += blockDim.x) {
+    const int j = idx / c, i = idx % c;
+    if (i >= j) P[(int64_t)j * ld + i] = D[i][j];
+  }
+  // below-diagonal rows: x L11^T = a  (forward substitution per row)
+  for (int64_t i = tid; i < r; i += blockDim.x) {
+    double x[CB];
+#pragma unroll
+    for (int j = 0; j < CB; ++j) x[j] = (j < c) ? P[(int64_t)j * ld + c + i] : 0.0;
+#pragma unroll
+    for (int j = 0; j < CB; ++j) {
+      if (j < c) {
+        double v = x[j];
+#pragma unroll
+        for (int k = 0; k < j; ++k) v -= x[k] * D[j][k];
+        x[j] = v / D[j][j];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < CB; ++j)
+      if (j < c) P[(int64_t)j * ld + c + i] = x[j];
+  }
+}
+
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int kLdsU = kUpdTile + 8;  // 72 doubles: two 128-byte wavefronts per fragment load
+
+__global__ void __launch_bounds__(128) k_update(
+    const UpdTile* __restrict__ tiles, const int* __restrict__ sn_first,
+    const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows,
+    const int64_t* __restrict__ Lptr, const int* __restrict__ row_grp,
+    const int* __restrict__ grp_target, const int* __restrict__ grp_jfirst,
+    const int64_t* __restrict__ grp_relind, const int* __restrict__ relind, double* __restrict__ L) {
+  extern __shared__ double sm[];
+  double* As = sm;                       // [kSnCols][kLdsU]
+  double* Bs = sm + kSnCols * kLdsU;     // [kSnCols][kLdsU]
+  const UpdTile tile = tiles[blockIdx.x];
+  const int s = tile.s;
+  const int f = sn_first[s];
+  const int c = sn_first[s + 1] - f;
+  const int64_t rp = rows_ptr[s];
+  const int r = (int)(rows_ptr[s + 1] - rp);
+  const int64_t ld = c + r;
+  const double* P = L + Lptr[s] + c;  // row 0 of L21
+  const int kpad = (c + 3) & ~3;
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < kpad * kUpdTile; idx += blockDim.x) {
+    const int k = idx / kUpdTile, ii = idx % kUpdTile;
+    const int gi = tile.i0 + ii, gj = tile.j0 + ii;
+    As[k * kLdsU + ii] = (k < c && gi < r) ? P[(int64_t)k * ld + gi] : 0.0;
+    Bs[k * kLdsU + ii] = (k < c && gj < r) ? P[(int64_t)k * ld + gj] : 0.0;
+  }
+  __syncthreads();
+  const int warp = tid >> 5, lane = tid & 31;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  const int g = lane >> 2, q = lane & 3;
+  double acc[4][4][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+  for (int k0 = 0; k0 < kpad; k0 += 4) {
+    double fa[4], fb[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) fa[a] = As[(k0 + q) * kLdsU + wr + a * 8 + g];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) fb[b] = Bs[(k0 + q) * kLdsU + wc + b * 8 + g];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) dmma_8x8x4(acc[a][b][0], acc[a][b][1], fa[a], fb[b]);
+  }
+  // scatter-subtract into the ancestors
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int j = tile.j0 + wc + b * 8 + 2 * q + e;
+      if (j >= r) continue;
+      const int grp = row_grp[rp + j];
+      const int t = grp_target[grp];
+      const int ft = sn_first[t];
+      const int ct = sn_first[t + 1] - ft;
+      const int64_t ldt = ct + (rows_ptr[t + 1] - rows_ptr[t]);
+      double* dstcol = L + Lptr[t] + (int64_t)(sn_rows[rp + j] - ft) * ldt;
+      const int* rel = relind + grp_relind[grp] - grp_jfirst[grp];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int i = tile.i0 + wr + a * 8 + g;
+        if (i < r && i >= j) atomicAdd(dstcol + rel[i], -acc[a][b][e]);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host plan
+// ---------------------------------------------------------------------------
+void build_factor_plan(temf_ctx& c) {
+  const Symbolic& S = c.sym;
+  FactorPlan& F = c.fplan;
+  cudaStream_t st = c.stream;
+  const int nsn = S.nsn;
+  F.sn_first.upload(S.sn_first.data(), S.sn_first.size(), st);
+  F.sn_parent.upload(S.sn_parent.data(), S.sn_parent.size(), st);
+  F.sn_rows.upload(S.sn_rows.data(), S.sn_rows.size(), st);
+  F.sn_rows_ptr.upload(S.sn_rows_ptr.data(), S.sn_rows_ptr.size(), st);
+  F.sn_Lptr.upload(S.sn_Lptr.data(), S.sn_Lptr.size(), st);
+  F.level_sn.upload(S.level_sn.data(), S.level_sn.size(), st);
+  F.level_ptr = S.level_ptr;
+
+  auto width = [&](int s) { return S.sn_first[s + 1] - S.sn_first[s]; };
+  auto nrows = [&](int s) { return (int64_t)(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]); };
+  // position of global row i in the panel of supernode t (i >= first column of t)
+  auto panel_row = [&](int t, int i) -> int64_t {
+    const int ft = S.sn_first[t], ct = width(t);
+    if (i < ft + ct) return i - ft;
+    const int* b = S.sn_rows.data() + S.sn_rows_ptr[t];
+    const int* e = S.sn_rows.data() + S.sn_rows_ptr[t + 1];
+    const int* p = std::lower_bound(b, e, i);
+    if (p == e || *p != i) throw StateError("symbolic structure inconsistent (row not in ancestor)");
+    return ct + (p - b);
+  };
+
+  // A -> L map
+  {
+    std::vector<int> src;
+    std::vector<int64_t> dst;
+    const Pattern& P = c.pat;
+    for (int i = 0; i < P.n; ++i) {
+      for (int p = P.rowptr[i]; p < P.rowptr[i + 1]; ++p) {
+        const int j = P.col[p];
+        if (j > i) break;
+        const int s = S.col2sn[j];
+        const int64_t ld = width(s) + nrows(s);
+        src.push_back(p);
+        dst.push_back(S.sn_Lptr[s] + (int64_t)(j - S.sn_first[s]) * ld + panel_row(s, i));
+      }
+    }
+    F.n_a2l = (int64_t)src.size();
+    F.a2l_src.upload(src.data(), src.size(), st);
+    F.a2l_dst.upload(dst.data(), dst.size(), st);
+  }
+  // update groups + relative indices
+  {
+    std::vector<int> row_grp(S.sn_rows.size());
+    std::vector<int> gt, gj;
+    std::vector<int64_t> gr;
+    std::vector<int> rel;
+    for (int s = 0; s < nsn; ++s) {
+      const int64_t rp = S.sn_rows_ptr[s];
+      const int r = (int)nrows(s);
+      int j = 0;
+      while (j < r) {
+        const int t = S.col2sn[S.sn_rows[rp + j]];
+        int j2 = j;
+        while (j2 < r && S.col2sn[S.sn_rows[rp + j2]] == t) ++j2;
+        const int grp = (int)gt.size();
+        gt.push_back(t);
+        gj.push_back(j);
+        gr.push_back((int64_t)rel.size());
+        for (int jj = j; jj < j2; ++jj) row_grp[rp + jj] = grp;
+        // relative positions of rows j..r-1 inside t's panel (merge of sorted lists)
+        const int ft = S.sn_first[t], ct = width(t);
+        const int* tb = S.sn_rows.data() + S.sn_rows_ptr[t];
+        const int64_t tr = nrows(t);
+        int64_t k = 0;
+        for (int i = j; i < r; ++i) {
+          const int gi = S.sn_rows[rp + i];
+          if (gi < ft + ct) { rel.push_back(gi - ft); continue; }
+          while (k < tr && tb[k] < gi) ++k;
+          if (k >= tr || tb[k] != gi) throw StateError("symbolic structure inconsistent (update row)");
+          rel.push_back((int)(ct + k));
+        }
+        j = j2;
+      }
+    }
+    F.n_relind = (int64_t)rel.size();
+    F.row_grp.upload(row_grp.data(), row_grp.size(), st);
+    F.grp_target.upload(gt.data(), gt.size(), st);
+    F.grp_jfirst.upload(gj.data(), gj.size(), st);
+    F.grp_relind.upload(gr.data(), gr.size(), st);
+    F.relind.upload(rel.data(), rel.size(), st);
+  }
+  // tiles per level
+  {
+    std::vector<UpdTile> tiles;
+    F.tile_level_ptr.assign(S.nlevels + 1, 0);
+    for (int l = 0; l < S.nlevels; ++l) {
+      for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+        const int s = S.level_sn[q];
+        const int r = (int)nrows(s);
+        const int nt = ceil_div(r, kUpdTile);
+        for (int ti = 0; ti < nt; ++ti)
+          for (int tj = 0; tj <= ti; ++tj) tiles.push_back({s, ti * kUpdTile, tj * kUpdTile});
+      }
+      F.tile_level_ptr[l + 1] = (int64_t)tiles.size();
+    }
+    F.n_tiles = (int64_t)tiles.size();
+    F.tiles.upload(tiles.data(), tiles.size(), st);
+  }
+  TEMF_CUDA(cudaStreamSynchronize(st));
+}
+
+int numeric_factor(temf_ctx& c, int slot, double dt) {
+  // A(dt) = 0*A_eps + 3*M_sigma + 2*dt*K  (mkl_add_3 at src/FETD_FWD.f90:1288,1354)
+  return numeric_factor_values(c, slot, c.d_M.p, 3.0, c.d_K.p, 2.0 * dt);
+}
+
+int numeric_factor_values(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b) {
+  const Symbolic& S = c.sym;
+  FactorPlan& F = c.fplan;
+  FactorSlot& fs = c.slots[slot];
+  cudaStream_t st = c.stream;
+  if (fs.L.n < (size_t)S.stored) fs.L.alloc(S.stored);
+  TEMF_CUDA(cudaMemsetAsync(fs.L.p, 0, S.stored * sizeof(double), st));
+  int init = INT_MAX;
+  TEMF_CUDA(cudaMemcpyAsync(c.d_status.p, &init, sizeof(int), cudaMemcpyHostToDevice, st));
+  if (F.n_a2l) {
+    k_load_A<<<ceil_div(F.n_a2l, 256), 256, 0, st>>>(F.n_a2l, F.a2l_src.p, F.a2l_dst.p, X, a, Y, b, fs.L.p);
+    TEMF_CHECK_LAUNCH();
+  }
+  const size_t upd_smem = 2 * kSnCols * kLdsU * sizeof(double);
+  TEMF_CUDA(cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem));
+  for (int l = 0; l < S.nlevels; ++l) {
+    const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
+    if (cnt > 0) {
+      k_potrf_trsm<<<cnt, kFacThreads, 0, st>>>(F.level_sn.p + S.level_ptr[l], F.sn_first.p, F.sn_rows_ptr.p,
+                                                F.sn_Lptr.p, fs.L.p, c.d_status.p);
+      TEMF_CHECK_LAUNCH();
+    }
+    const int64_t t0 = F.tile_level_ptr[l], t1 = F.tile_level_ptr[l + 1];
+    if (t1 > t0) {
+      if (t1 - t0 > INT_MAX) throw StateError("too many update tiles in one level");
+      k_update<<<(unsigned)(t1 - t0), 128, upd_smem, st>>>(F.tiles.p + t0, F.sn_first.p, F.sn_rows_ptr.p,
+                                                          F.sn_rows.p, F.sn_Lptr.p, F.row_grp.p, F.grp_target.p,
+                                                          F.grp_jfirst.p, F.grp_relind.p, F.relind.p, fs.L.p);
+      TEMF_CHECK_LAUNCH();
+    }
+  }
+  int status = 0;
+  TEMF_CUDA(cudaMemcpyAsync(&status, c.d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  TEMF_CUDA(cudaStreamSynchronize(st));
+  fs.dt = b * 0.5;
+  if (status != INT_MAX) {
+    fs.valid = false;
+    fs.status = c.sym.perm[status - 1] + 1;
+    return fs.status;
+  }
+  fs.valid = true;
+  fs.status = 0;
+  return 0;
+}
+
+}  // namespace temf

@@ -1,0 +1,15 @@
+#pragma once
+#include "ctx.h"
+
+namespace temf {
+constexpr int kSnCols = 64;     // maximum supernode width (columns per panel)
+constexpr int kUpdTile = 64;    // update tile edge
+
+void build_factor_plan(temf_ctx& c);
+// Numeric LL^T of A = 3 M + 2 dt K into `slot`.  Returns 0 or the 1-based
+// (original numbering) column of the first non-positive pivot.
+int numeric_factor(temf_ctx& c, int slot, double dt);
+// General form: L = LL^T factor of a*X + b*Y where X, Y are values on the
+// permuted full pattern (device arrays).  Same return convention.
+int numeric_factor_values(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b);
+}  // namespace temf

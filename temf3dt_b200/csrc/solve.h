@@ -1,0 +1,25 @@
+#pragma once
+#include "ctx.h"
+
+namespace temf {
+void build_solve_plan(temf_ctx& c);
+void ensure_update_buffer(temf_ctx& c, int nrhs);
+
+// x (device, permuted order, row-major n x nrhs) is overwritten: b -> A^{-1} b.
+// `Lbase` points at a device word holding the panel base of the factor to use
+// (an indirection so captured graphs can follow the factor slot).
+void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st);
+
+// y = M (4 e2 - e3) for nrhs columns (row-major), permuted order.
+void launch_bdf_rhs(temf_ctx& c, const double* e2, const double* e3, double* y, int nrhs, cudaStream_t st);
+// y[src_idx] -= coef_dev[0] * src_coef   (source term of sys_right)
+void launch_source(temf_ctx& c, const double* coef_dev, double* y, int nrhs, cudaStream_t st);
+// receiver samples of x: out[rec*6 + q] = sum_j W[rec][q][j] x[edge_j]
+void launch_receivers(temf_ctx& c, const double* x, int nrhs, double* out, cudaStream_t st);
+// ||a-b||^2 and ||b||^2 per RHS column -> out[2*nrhs] (deterministic);
+// `out` must hold two_error_len(nrhs) doubles (the tail is block partials).
+inline size_t two_error_len(int nrhs) { return (size_t)(1 + 296) * 2 * nrhs; }
+void launch_two_error(temf_ctx& c, const double* a, const double* b, int nrhs, double* out, cudaStream_t st);
+// plain y = M x (full symmetric)
+void launch_spmv(temf_ctx& c, const double* M, const double* x, double* y, int nrhs, cudaStream_t st);
+}  // namespace temf

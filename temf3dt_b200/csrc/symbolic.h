@@ -1,0 +1,58 @@
+// Host-side symbolic analysis of the FETD step matrix  A(dt) = 3 M_sigma + 2 dt K.
+//
+// The pattern of A does not depend on dt (every entry of M and K comes from
+// the same per-tetrahedron 6x6 blocks, src/FETD_FWD.f90:642-662), so the
+// ordering, elimination tree and supernode partition are computed once per
+// mesh and reused by every refactorisation at a dt-doubling point.  This
+// replaces the reorder + symbolic part of PARDISO phase 12
+// (src/FETD_UTILITY.f90:912-917) whose ordering the reference leaves at MKL's
+// default (iparm = 0, :909-910).
+#pragma once
+#include <cstdint>
+#include <vector>
+#include <string>
+
+namespace temf {
+
+struct SymbolicOptions {
+  int leaf_size = 96;          // nested-dissection leaf size
+  int max_sn_cols = 64;        // supernodes are split into column blocks of at most this width
+  bool amalgamate = true;      // relaxed supernode amalgamation
+};
+
+struct Symbolic {
+  int n = 0;
+  std::vector<int> perm;        // perm[new] = old
+  std::vector<int> iperm;       // iperm[old] = new
+  // supernode partition (on the permuted matrix)
+  int nsn = 0;
+  std::vector<int> sn_first;        // nsn+1: first column of each supernode
+  std::vector<int> sn_parent;       // parent supernode or -1
+  std::vector<int64_t> sn_rows_ptr; // nsn+1: offsets of the below-diagonal row lists
+  std::vector<int> sn_rows;         // below-diagonal rows (permuted indices, ascending)
+  std::vector<int64_t> sn_Lptr;     // nsn+1: panel offsets in doubles; panel = (c+r) x c, column-major
+  std::vector<int> col2sn;          // n
+  std::vector<int> sn_level;        // bottom-up level (leaves = 0)
+  int nlevels = 0;
+  std::vector<int> level_ptr;       // nlevels+1
+  std::vector<int> level_sn;        // supernodes grouped by level
+  // statistics
+  int64_t nnzL = 0;                 // structural nonzeros of L (lower triangle incl. diagonal)
+  int64_t stored = 0;               // doubles stored in the panels
+  double flops = 0.0;               // factor flops (mul+add counted as 2)
+  double t_order = 0, t_etree = 0, t_colcount = 0, t_super = 0;
+};
+
+// Nested-dissection ordering on the symmetric graph (xadj/adj without the
+// diagonal) using recursive coordinate bisection with vertex separators.
+// Returns perm[new] = old.
+std::vector<int> nested_dissection(int n, const int64_t* xadj, const int* adj,
+                                   const double* xyz, int leaf_size);
+
+// Full symbolic analysis.  (xadj, adj) is the symmetric pattern of A in the
+// original numbering without the diagonal; xyz gives a point per unknown
+// (edge midpoints) for the geometric bisection.
+void analyse(int n, const int64_t* xadj, const int* adj, const double* xyz,
+             const SymbolicOptions& opt, Symbolic& out);
+
+}  // namespace temf

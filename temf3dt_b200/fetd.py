@@ -1,0 +1,302 @@
+"""Host-side mirror of TEMF3DT's forward driver over the C ABI.
+
+``FetdGPU`` owns one library context (one GPU).  Its methods follow the
+reference's phases: model_mesh/model_ctl (arrays), mesh_process (assembly),
+time_solver/adap_euler (the time loop) -- see include/temf_b200.h for the
+reference routine each C entry point replaces.  ``run_case`` is the
+equivalent of ``./FETD -f ROOT`` for a ``.mesh``/``.cntl`` pair.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import meshio
+from ._lib import (TemfError, as_f64, as_i32, dptr, fortran_f64, fortran_i32, iptr, lib)
+
+
+def mesh_topology(tet_vex: np.ndarray):
+    """Global edges, tet->edge map and orientation (src/FETD_FWD.f90:168-244),
+    computed by the library's host helper.  Returns 1-based arrays."""
+    L = lib()
+    T = int(tet_vex.shape[0])
+    tv = fortran_i32(tet_vex)
+    ne = C.c_int(0)
+    rc = L.temf_mesh_count_edges(T, iptr(tv), C.byref(ne))
+    if rc:
+        raise TemfError(rc, "temf_mesh_count_edges")
+    ev = np.zeros(2 * ne.value, dtype=np.int32)
+    te = np.zeros(6 * T, dtype=np.int32)
+    td = np.zeros(6 * T, dtype=np.int32)
+    rc = L.temf_mesh_topology(T, iptr(tv), ne.value, iptr(ev), iptr(te), iptr(td))
+    if rc:
+        raise TemfError(rc, "temf_mesh_topology")
+    return ev.reshape(2, -1).T.copy(), te.reshape(6, T).T.copy(), td.reshape(6, T).T.copy()
+
+
+def source_edges(edg_vex: np.ndarray, src_vex: np.ndarray):
+    """Map source segments to global edges and apply the reference's
+    orientation convention: +1 for every segment except the last, which is -1
+    (src/FETD_FWD.f90:435-448)."""
+    key = edg_vex[:, 0].astype(np.int64) * (1 << 32) + edg_vex[:, 1]
+    lo = np.minimum(src_vex[:, 0], src_vex[:, 1]).astype(np.int64)
+    hi = np.maximum(src_vex[:, 0], src_vex[:, 1]).astype(np.int64)
+    k = lo * (1 << 32) + hi
+    pos = np.searchsorted(key, k)
+    if len(k) and (np.any(pos >= len(key)) or np.any(key[np.minimum(pos, len(key) - 1)] != k)):
+        raise ValueError("a source segment is not an edge of the mesh")
+    drc = np.ones(len(k), dtype=np.int32)
+    if len(k):
+        drc[-1] = -1
+    return (pos + 1).astype(np.int32), drc
+
+
+@dataclass
+class RunOutput:
+    steps: np.ndarray
+    times: np.ndarray
+    dts: np.ndarray
+    fields: np.ndarray          # (rows, nrec, 9)
+    trial_errors: np.ndarray
+    trial_accepted: np.ndarray
+    ms_factor: float
+    ms_steps: float
+    ms_total: float
+    n_factor: int
+    n_solve: int
+    n_launch: int
+
+
+class FetdGPU:
+    """One FETD model on one GPU."""
+
+    def __init__(self, device: int = 0):
+        self._L = lib()
+        h = C.c_void_p()
+        rc = self._L.temf_create(device, C.byref(h))
+        self._h = h
+        if rc:
+            msg = self.last_error()
+            raise TemfError(rc, msg)
+        self.n_edges = 0
+        self.n_tets = 0
+        self.nrec = 0
+
+    # -- plumbing -----------------------------------------------------------
+    def last_error(self) -> str:
+        s = self._L.temf_last_error(self._h)
+        return s.decode() if s else ""
+
+    def _ck(self, rc: int, what: str) -> int:
+        if rc < 0:
+            raise TemfError(rc, "%s: %s" % (what, self.last_error()))
+        return rc
+
+    def close(self) -> None:
+        if self._h:
+            self._L.temf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- model ----------------------------------------------------------------
+    def set_mesh(self, nod_cor, tet_vex, edg_vex, tet_edg, tet_drc) -> None:
+        nod = fortran_f64(nod_cor)
+        tv, ev, te, td = fortran_i32(tet_vex), fortran_i32(edg_vex), fortran_i32(tet_edg), fortran_i32(tet_drc)
+        self.n_tets = int(np.asarray(tet_vex).shape[0])
+        self.n_edges = int(np.asarray(edg_vex).shape[0])
+        self._ck(self._L.temf_set_mesh(self._h, int(np.asarray(nod_cor).shape[0]), dptr(nod), self.n_tets, iptr(tv),
+                                       self.n_edges, iptr(ev), iptr(te), iptr(td)), "temf_set_mesh")
+
+    def set_media(self, sig, mu) -> None:
+        s, m = as_f64(sig), as_f64(mu)
+        self._ck(self._L.temf_set_media(self._h, dptr(s), dptr(m)), "temf_set_media")
+
+    def analyse(self) -> None:
+        self._ck(self._L.temf_analyse(self._h), "temf_analyse")
+
+    def assemble(self) -> None:
+        self._ck(self._L.temf_assemble(self._h), "temf_assemble")
+
+    def stats(self) -> Dict[str, float]:
+        s = np.zeros(10)
+        self._ck(self._L.temf_analysis_stats(self._h, dptr(s)), "temf_analysis_stats")
+        keys = ["n", "nnz_A", "supernodes", "levels", "nnz_L", "stored", "flops", "update_tiles",
+                "t_order", "t_symbolic"]
+        return dict(zip(keys, s.tolist()))
+
+    def get_matrix(self, which: int):
+        """1-based upper CSR (ia, ja, va) of M_sigma (0) or K (1), original numbering."""
+        nnz = C.c_int(0)
+        self._ck(self._L.temf_get_matrix(self._h, which, C.byref(nnz), None, None, None), "temf_get_matrix")
+        ia = np.zeros(self.n_edges + 1, dtype=np.int32)
+        ja = np.zeros(nnz.value, dtype=np.int32)
+        va = np.zeros(nnz.value)
+        self._ck(self._L.temf_get_matrix(self._h, which, C.byref(nnz), iptr(ia), iptr(ja), dptr(va)), "temf_get_matrix")
+        return ia, ja, va
+
+    # -- linear algebra -------------------------------------------------------
+    def factor(self, slot: int, dt: float) -> int:
+        return self._ck(self._L.temf_factor(self._h, slot, float(dt)), "temf_factor")
+
+    def solve(self, slot: int, b: np.ndarray) -> np.ndarray:
+        b = np.asarray(b, dtype=np.float64)
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        bb = np.ascontiguousarray(b.reshape(self.n_edges, nrhs).T)   # column-major
+        x = np.zeros_like(bb)
+        self._ck(self._L.temf_solve(self._h, slot, nrhs, dptr(bb), dptr(x), self.n_edges), "temf_solve")
+        return x.T.reshape(b.shape)
+
+    def release(self, slot: int) -> None:
+        self._ck(self._L.temf_release(self._h, slot), "temf_release")
+
+    def spmv(self, which: int, x: np.ndarray) -> np.ndarray:
+        x = np.asarray(x, dtype=np.float64)
+        nrhs = 1 if x.ndim == 1 else x.shape[1]
+        xx = np.ascontiguousarray(x.reshape(self.n_edges, nrhs).T)
+        y = np.zeros_like(xx)
+        self._ck(self._L.temf_spmv(self._h, which, nrhs, dptr(xx), dptr(y), self.n_edges), "temf_spmv")
+        return y.T.reshape(x.shape)
+
+    # -- sources / receivers --------------------------------------------------
+    def set_sources(self, columns: Sequence[Tuple[np.ndarray, np.ndarray]], source_type: int, pulse_type: int,
+                    t0: float, current: float) -> None:
+        ptr = [0]
+        e, d = [], []
+        for edg, drc in columns:
+            e.extend(np.asarray(edg).tolist())
+            d.extend(np.asarray(drc).tolist())
+            ptr.append(len(e))
+        P, E, D = as_i32(ptr), as_i32(e if e else [0]), as_i32(d if d else [0])
+        self._ck(self._L.temf_set_sources(self._h, len(columns), iptr(P), iptr(E), iptr(D), source_type, pulse_type,
+                                          float(t0), float(current)), "temf_set_sources")
+
+    def locate(self, points: np.ndarray, rec_charac: float) -> np.ndarray:
+        pts = fortran_f64(points)
+        out = np.zeros(len(points), dtype=np.int32)
+        self._ck(self._L.temf_locate_points(self._h, len(points), dptr(pts), float(rec_charac), iptr(out)),
+                 "temf_locate_points")
+        return out
+
+    def set_receivers(self, rec_tet, rec_cor, rec_rhs=None) -> None:
+        rt = as_i32(rec_tet)
+        rc = fortran_f64(rec_cor)
+        rr = as_i32(rec_rhs) if rec_rhs is not None else None
+        self.nrec = len(rt)
+        self._ck(self._L.temf_set_receivers(self._h, len(rt), iptr(rt), dptr(rc), iptr(rr) if rr is not None else None),
+                 "temf_set_receivers")
+
+    def receiver_operators(self):
+        n = np.zeros(self.nrec * 18)
+        d = np.zeros(self.nrec * 18)
+        self._ck(self._L.temf_get_receiver_operators(self._h, dptr(n), dptr(d)), "temf_get_receiver_operators")
+        return n.reshape(3, 6, self.nrec).transpose(2, 1, 0), d.reshape(3, 6, self.nrec).transpose(2, 1, 0)
+
+    # -- time loop ------------------------------------------------------------------
+    def run(self, sp_division: int, sp_double: int, sp_dblesize: int, time_maximum: float,
+            legacy_time_column: bool = False, graphs: bool = True, forced: Optional[Sequence[int]] = None,
+            max_steps: int = 0) -> RunOutput:
+        flags = (1 if legacy_time_column else 0) | (0 if graphs else 2)
+        f = as_i32(forced) if forced is not None else None
+        self._ck(self._L.temf_run(self._h, int(sp_division), int(sp_double), int(sp_dblesize), float(time_maximum),
+                                  flags, iptr(f) if f is not None else None, len(f) if f is not None else 0,
+                                  int(max_steps)), "temf_run")
+        rows = C.c_int(0)
+        self._ck(self._L.temf_result_rows(self._h, C.byref(rows)), "temf_result_rows")
+        R = rows.value
+        steps = np.zeros(R, dtype=np.int32)
+        times = np.zeros(R)
+        dts = np.zeros(R)
+        fields = np.zeros(R * max(self.nrec, 1) * 9)
+        self._ck(self._L.temf_result_get(self._h, iptr(steps), dptr(times), dptr(dts), dptr(fields)),
+                 "temf_result_get")
+        nt = C.c_int(0)
+        self._ck(self._L.temf_result_trials(self._h, C.byref(nt), None, None), "temf_result_trials")
+        errs = np.zeros(max(nt.value, 1))
+        acc = np.zeros(max(nt.value, 1), dtype=np.int32)
+        self._ck(self._L.temf_result_trials(self._h, C.byref(nt), dptr(errs), iptr(acc)), "temf_result_trials")
+        t = [C.c_double(0), C.c_double(0), C.c_double(0)]
+        nf, ns, nl = C.c_int(0), C.c_int(0), C.c_longlong(0)
+        self._ck(self._L.temf_result_timing(self._h, C.byref(t[0]), C.byref(t[1]), C.byref(t[2]), C.byref(nf),
+                                            C.byref(ns), C.byref(nl)), "temf_result_timing")
+        return RunOutput(steps, times, dts, fields.reshape(R, max(self.nrec, 1), 9), errs[:nt.value],
+                         acc[:nt.value].astype(bool), t[0].value, t[1].value, t[2].value, nf.value, ns.value,
+                         int(nl.value))
+
+    def gates(self, gate_times: Sequence[float]):
+        g = as_f64(gate_times)
+        out = np.zeros(len(g) * max(self.nrec, 1) * 9)
+        done = np.zeros(len(g), dtype=np.int32)
+        self._ck(self._L.temf_result_gates(self._h, len(g), dptr(g), dptr(out), iptr(done)), "temf_result_gates")
+        return out.reshape(len(g), max(self.nrec, 1), 9), done.astype(bool)
+
+    # -- PARDISO-compatible shim ------------------------------------------------------
+    def pardiso_alloc(self, max_matrix: int) -> None:
+        self._ck(self._L.temf_pardiso_alloc(self._h, max_matrix), "temf_pardiso_alloc")
+
+    def pardiso_direct_1(self, num_m: int, ia, ja, va) -> int:
+        ia, ja, va = as_i32(ia), as_i32(ja), as_f64(va)
+        return self._ck(self._L.temf_pardiso_direct_1(self._h, num_m, 1, len(ia) - 1, len(ja), iptr(ia), iptr(ja),
+                                                      dptr(va)), "temf_pardiso_direct_1")
+
+    def pardiso_direct_2(self, num_m: int, b: np.ndarray) -> np.ndarray:
+        b = as_f64(b)
+        x = np.zeros_like(b)
+        self._ck(self._L.temf_pardiso_direct_2(self._h, num_m, dptr(b), dptr(x)), "temf_pardiso_direct_2")
+        return x
+
+    def pardiso_direct_3(self, num_m: int) -> None:
+        self._ck(self._L.temf_pardiso_direct_3(self._h, num_m), "temf_pardiso_direct_3")
+
+    def pardiso_dealloc(self) -> None:
+        self._ck(self._L.temf_pardiso_dealloc(self._h), "temf_pardiso_dealloc")
+
+
+def load_case(gpu: FetdGPU, mesh: meshio.Mesh, ctl: meshio.Control, rec_tet: Optional[np.ndarray] = None):
+    """model_mesh + model_ctl + mesh_process for one ``.mesh``/``.cntl`` pair."""
+    if ctl.bound_cond != 0:
+        raise NotImplementedError("only the PEC boundary (boundary condition: 0) is on the GPU path")
+    edg_vex, tet_edg, tet_drc = mesh_topology(mesh.tet_vex)
+    gpu.set_mesh(mesh.nod_cor, mesh.tet_vex, edg_vex, tet_edg, tet_drc)
+    sig, mu = meshio.media_per_tet(mesh.tet_phy, ctl)
+    gpu.set_media(sig, mu)
+    gpu.analyse()
+    gpu.assemble()
+    src_edg, src_drc = source_edges(edg_vex, mesh.src_vex)
+    gpu.set_sources([(src_edg, src_drc)], ctl.source_type, ctl.pulse_type, ctl.t0, ctl.current)
+    if rec_tet is None:
+        rec_tet = gpu.locate(ctl.rec_cor, ctl.rec_charac)
+        if (rec_tet == 0).any():
+            raise ValueError("no rec tet No. %d" % (int(np.argmin(rec_tet)) + 1))
+    gpu.set_receivers(rec_tet, ctl.rec_cor)
+    return dict(edg_vex=edg_vex, tet_edg=tet_edg, tet_drc=tet_drc, sig=sig, mu=mu, src_edg=src_edg,
+                src_drc=src_drc, rec_tet=np.asarray(rec_tet))
+
+
+def run_case(root: str, device: int = 0, legacy_time_column: bool = False, write: bool = True) -> RunOutput:
+    """``./FETD -f ROOT``: read ROOT.mesh/.cntl, run on the GPU, write ROOT.field(2)."""
+    mesh = meshio.read_mesh(root + ".mesh")
+    ctl = meshio.read_cntl(root + ".cntl")
+    with FetdGPU(device) as gpu:
+        load_case(gpu, mesh, ctl)
+        out = gpu.run(ctl.sp_division, ctl.sp_double, ctl.sp_dblesize, ctl.time_maximum,
+                      legacy_time_column=legacy_time_column)
+        if write:
+            meshio.write_field(root + ".field", out.steps, out.times, out.fields, ctl.output)
+            if ctl.time_points is not None:
+                g, _done = gpu.gates(ctl.time_points)
+                meshio.write_field(root + ".field2", np.arange(1, len(g) + 1), ctl.time_points, g, ctl.output)
+        return out
