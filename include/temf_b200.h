@@ -125,9 +125,10 @@ int temf_locate_points(temf_ctx* ctx, int npts, const double* pts, double rec_ch
 /* ---- the time loop ----------------------------------------------------------
  * Runs time_solver/adap_euler (src/FETD_FWD.f90:1174-1464) on the GPU:
  * sp_division, sp_double, sp_dblesize and time_maximum as in the .cntl file.
- * flags: bit 0 = legacy time column (the shipped LINUX/*.field files advance
- * an accepted trial's time by one extra old step), bit 1 = disable CUDA
- * graphs.  forced (may be NULL): per trial 1 = accept, 0 = reject, -1 = the
+ * flags: bit 0 = reproduce the build that wrote the shipped LINUX/*.field
+ * files (after an accepted dt-doubling trial it restarted BDF2 from
+ * all_e(idx - sp_dblesize) instead of all_e(idx), src/FETD_FWD.f90:1405, and
+ * advanced the time by one more old step); bit 1 = disable CUDA graphs.  forced (may be NULL): per trial 1 = accept, 0 = reject, -1 = the
  * reference's own test (used to replay a given schedule).  max_steps 0 = no
  * limit.  Results are kept in the context; see temf_result_*. */
 int temf_run(temf_ctx* ctx, int sp_division, int sp_double, int sp_dblesize, double time_maximum, int flags,
@@ -158,8 +159,9 @@ int temf_analysis_stats(temf_ctx* ctx, double* stats);
 /* Host-only ordering + symbolic analysis of a symmetric pattern (no GPU
  * needed): 0-based adjacency without the diagonal (xadj[n+1], adj), one point
  * per unknown in xyz(3,n) (x,y,z of each unknown contiguous).  perm_out[new]
- * = old (0-based).  stats[0..7] = n, supernodes, levels, nnz(L), stored
- * doubles, factor flops, seconds ordering, seconds symbolic. */
+ * = old (0-based).  stats[0..8] = n, supernodes, levels, nnz(L) held by the
+ * supernodes, stored doubles, factor flops, seconds ordering, seconds
+ * symbolic, structural nnz(L) (sum of column counts). */
 int temf_symbolic_host(int n, const long long* xadj, const int* adj, const double* xyz, int* perm_out,
                        double* stats);
 

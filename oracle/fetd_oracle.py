@@ -572,15 +572,15 @@ class _Output:
 def adap_euler(model: OracleModel, slots: SuperLUSlots, out: Optional[_Output],
                pulse_sign: float = 1.0, res_e: Optional[np.ndarray] = None,
                max_steps: Optional[int] = None, time_maximum: Optional[float] = None,
-               legacy_time_column: bool = False):
+               legacy_linux: bool = False):
     """Adaptive BDF2 time loop, src/FETD_FWD.f90:1229-1464.
 
     ``pulse_sign`` = -1 reproduces the ``r_h = -r_h`` of the DC pass of pulse
-    type 3 (:1322,1364,1426).  ``legacy_time_column`` reproduces the time
-    column of the shipped ``LINUX/*.field`` files, which advance the time of an
-    accepted doubling trial by one extra old step compared with the source's
-    ``tmp_time_cur = time_cur - step_cur + tmp_step_cur`` (:1350); the field
-    values themselves do not depend on it once the source is off.
+    type 3 (:1322,1364,1426).  ``legacy_linux`` reproduces the build that wrote
+    the shipped ``LINUX/*.field`` files: after an accepted doubling trial it
+    restarted from ``e3 = all_e(idx - sp_dblesize)`` instead of
+    ``all_e(idx)`` (:1405) and advanced the time by one more old step than
+    ``tmp_time_cur = time_cur - step_cur + tmp_step_cur`` (:1350).
     """
     ctl = model.ctl
     n = model.n
@@ -656,9 +656,9 @@ def adap_euler(model: OracleModel, slots: SuperLUSlots, out: Optional[_Output],
                 accepted.append(True)
                 slots.release(ind)
                 ind = other
-                e3 = all_e[-1]
+                e3 = all_e[-1 - dsz] if legacy_linux else all_e[-1]
                 e2 = e_veri_1
-                time_cur = tmp_time_cur + (step_cur if legacy_time_column else 0.0)
+                time_cur = tmp_time_cur + (step_cur if legacy_linux else 0.0)
                 step_cur = tmp_step_cur
                 if out is not None:
                     out(step, time_cur, step_cur, e2)
@@ -676,7 +676,7 @@ def adap_euler(model: OracleModel, slots: SuperLUSlots, out: Optional[_Output],
 
 
 def run_fetd(model: OracleModel, max_steps: Optional[int] = None, time_maximum: Optional[float] = None,
-             legacy_time_column: bool = False) -> FetdResult:
+             legacy_linux: bool = False) -> FetdResult:
     """``time_solver`` (src/FETD_FWD.f90:1174-1227) with MKL replaced by SuperLU."""
     slots = SuperLUSlots(model)
     out = _Output(model)
@@ -688,10 +688,10 @@ def run_fetd(model: OracleModel, max_steps: Optional[int] = None, time_maximum: 
         res_e, _, _ = adap_euler(model, slots, None, pulse_sign=-1.0, max_steps=None,
                                  time_maximum=time_maximum)
         e_last, errs, acc = adap_euler(model, slots, out, res_e=res_e, max_steps=max_steps,
-                                       time_maximum=time_maximum, legacy_time_column=legacy_time_column)
+                                       time_maximum=time_maximum, legacy_linux=legacy_linux)
     else:
         e_last, errs, acc = adap_euler(model, slots, out, max_steps=max_steps, time_maximum=time_maximum,
-                                       legacy_time_column=legacy_time_column)
+                                       legacy_linux=legacy_linux)
     return FetdResult(out.steps, out.times, out.dts, np.array(out.rows), out.chan_val, errs, acc, e_last)
 
 

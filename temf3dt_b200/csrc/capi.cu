@@ -222,6 +222,7 @@ int temf_create(int device, temf_ctx** out) {
     TEMF_CUDA(cudaSetDevice(device));
     TEMF_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     c->d_status.alloc(4);
+    TEMF_CUDA(cudaMemset(c->d_status.p, 0, 4 * sizeof(int)));
     return TEMF_OK;
   });
   if (rc != TEMF_OK) {
@@ -474,6 +475,10 @@ static void host_solve(temf_ctx* c, int slot0, int nrhs, const double* b, double
   for (int q = 0; q < nrhs; ++q)
     TEMF_CUDA(cudaMemcpyAsync(x + (size_t)q * ld, dcol + (size_t)q * n, n * sizeof(double), cudaMemcpyDeviceToHost, st));
   TEMF_CUDA(cudaStreamSynchronize(st));
+  if (const int fl = solve_error_flag(*c)) {
+    clear_solve_error_flag(*c);
+    throw StateError("a triangular-solve wait timed out (code " + std::to_string(fl) + ")");
+  }
 }
 
 int temf_solve(temf_ctx* c, int slot, int nrhs, const double* b, double* x, int ld) {
@@ -646,7 +651,7 @@ int temf_run(temf_ctx* c, int sp_division, int sp_double, int sp_dblesize, doubl
     o.step_dble = sp_double;
     o.step_dblesize = sp_dblesize;
     o.time_maximum = time_maximum;
-    o.legacy_time_column = flags & 1;
+    o.legacy_linux = flags & 1;
     o.use_graphs = (flags & 2) ? 0 : 1;
     o.forced = forced;
     o.n_forced = forced ? n_forced : 0;
@@ -801,6 +806,7 @@ int temf_symbolic_host(int n, const long long* xadj, const int* adj, const doubl
       stats[0] = S.n; stats[1] = S.nsn; stats[2] = S.nlevels; stats[3] = (double)S.nnzL;
       stats[4] = (double)S.stored; stats[5] = S.flops; stats[6] = S.t_order;
       stats[7] = S.t_etree + S.t_colcount + S.t_super;
+      stats[8] = (double)S.nnzL_exact;
     }
     return TEMF_OK;
   } catch (...) {

@@ -45,8 +45,20 @@ struct FactorPlan {
   DBuf<int> relind;
   DBuf<UpdTile> tiles;
   std::vector<int64_t> tile_level_ptr;  // host, nlevels+1
+  DBuf<int2> trsm;             // (supernode, first row) chunks of the row solves
+  std::vector<int64_t> trsm_level_ptr;
+  int64_t n_trsm = 0;
   int64_t n_relind = 0;
   int64_t n_tiles = 0;
+};
+
+// A task of the persistent triangular-solve kernels: the diagonal block of
+// supernode s (kind 0) or rows [r0, r1) of its below-diagonal panel (kind 1).
+struct SolveTask {
+  int s;
+  int kind;
+  int r0;
+  int r1;
 };
 
 struct SolvePlan {
@@ -54,6 +66,17 @@ struct SolvePlan {
   DBuf<int64_t> in_ptr;        // n+1: incoming update entries per column
   DBuf<int64_t> in_idx;        // positions in the update buffer
   int64_t u_len = 0;
+  // persistent schedules (tasks in an order where every wait targets an earlier task)
+  DBuf<SolveTask> ftask, btask;
+  int n_ftask = 0, n_btask = 0;
+  DBuf<int> ftgt_ptr, ftgt;    // per forward task: supernodes whose columns its rows feed
+  DBuf<int> fexpect;           // per supernode: forward chunk tasks feeding it
+  DBuf<int> btgt_ptr, btgt;    // per backward task: supernodes owning its rows (solved first)
+  DBuf<int> nchunk;            // per supernode: row chunks of its panel
+  DBuf<int64_t> part_off;      // per supernode: offset of its backward partial sums
+  int64_t part_len = 0;
+  DBuf<int> sync;              // ready | ydone | cdone | xdone (nsn each) | counters
+  int nsn = 0;
 };
 
 struct FactorSlot {
@@ -121,5 +144,6 @@ struct temf_ctx {
   temf::Receivers rec;
   // scratch vectors
   temf::DBuf<double> d_u;        // solve update buffer (u_len * nrhs)
+  temf::DBuf<double> d_part;     // backward partial sums (part_len * nrhs)
   int u_nrhs = 0;
 };

@@ -6,15 +6,19 @@
 // directly into the supernodal panels (the pattern is dt-independent).
 //
 // Schedule: bottom-up levels of the supernodal elimination tree.  Per level:
-//   k_potrf_trsm : one CTA per supernode: dense Cholesky of the (<=64 x 64)
-//                  diagonal block in shared memory, then the below-diagonal
-//                  rows solved against it (one row per thread, in registers).
+//   k_potrf      : one CTA per supernode: dense Cholesky of the (<=64 x 64)
+//                  diagonal block in shared memory;
+//   k_trsm       : the below-diagonal rows solved against it, 128 rows per
+//                  CTA (one row per thread, in registers);
 //   k_update     : the Schur update L21 L21^T of every supernode of the level,
 //                  in 64x64 tiles on the FP64 tensor cores (DMMA
 //                  mma.sync.m8n8k4.f64), scattered into the ancestor panels
 //                  through precomputed relative indices.  Several supernodes
 //                  of one level may update the same ancestor entry, so the
-//                  scatter uses FP64 atomics (red.global.add.f64).
+//                  scatter of such levels uses FP64 atomics
+//                  (red.global.add.f64); a level holding a single supernode
+//                  (the dense top of the tree, where most flops are) writes
+//                  with plain read-modify-write.
 // Pivot failures are reported through a status word (first failing column),
 // never by trapping.
 #include <algorithm>
@@ -38,7 +42,8 @@ __global__ void k_load_A(int64_t n, const int* __restrict__ src, const int64_t* 
 
 constexpr int kFacThreads = 128;
 
-__global__ void __launch_bounds__(kFacThreads) k_potrf_trsm(
+// Dense Cholesky of the (<= 64 x 64) diagonal block of each supernode of a level.
+__global__ void __launch_bounds__(kFacThreads) k_potrf(
     const int* __restrict__ level_sn, const int* __restrict__ sn_first,
     const int64_t* __restrict__ rows_ptr, const int64_t* __restrict__ Lptr, double* __restrict__ L,
     int* __restrict__ status) {
@@ -80,24 +85,54 @@ __global__ void __launch_bounds__(kFacThreads) k_potrf_trsm(
     const int j = idx / c, i = idx % c;
     if (i >= j) P[(int64_t)j * ld + i] = D[i][j];
   }
-  // below-diagonal rows: x L11^T = a  (forward substitution per row)
-  for (int64_t i = tid; i < r; i += blockDim.x) {
-    double x[CB];
-#pragma unroll
-    for (int j = 0; j < CB; ++j) x[j] = (j < c) ? P[(int64_t)j * ld + c + i] : 0.0;
-#pragma unroll
-    for (int j = 0; j < CB; ++j) {
-      if (j < c) {
-        double v = x[j];
-#pragma unroll
-        for (int k = 0; k < j; ++k) v -= x[k] * D[j][k];
-        x[j] = v / D[j][j];
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < CB; ++j)
-      if (j < c) P[(int64_t)j * ld + c + i] = x[j];
+}
+
+// Below-diagonal rows of the level's supernodes, kTrsmRows rows per CTA:
+// x L11^T = a, forward substitution per row in registers.
+struct TrsmChunk {
+  int s;
+  int r0;
+};
+constexpr int kTrsmRows = kFacThreads;
+
+__global__ void __launch_bounds__(kFacThreads) k_trsm(const TrsmChunk* __restrict__ chunks,
+                                                      const int* __restrict__ sn_first,
+                                                      const int64_t* __restrict__ rows_ptr,
+                                                      const int64_t* __restrict__ Lptr, double* __restrict__ L) {
+  constexpr int CB = kSnCols;
+  __shared__ double D[CB][CB + 1];
+  __shared__ double inv[CB];
+  const TrsmChunk ch = chunks[blockIdx.x];
+  const int s = ch.s;
+  const int f = sn_first[s];
+  const int c = sn_first[s + 1] - f;
+  const int64_t r = rows_ptr[s + 1] - rows_ptr[s];
+  const int64_t ld = c + r;
+  double* P = L + Lptr[s];
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < c * c; idx += blockDim.x) {
+    const int j = idx / c, i = idx % c;
+    if (i >= j) D[i][j] = P[(int64_t)j * ld + i];
   }
+  __syncthreads();
+  const int64_t i = ch.r0 + tid;
+  if (i >= r) return;
+  double x[CB];
+#pragma unroll
+  for (int j = 0; j < CB; ++j) x[j] = (j < c) ? P[(int64_t)j * ld + c + i] : 0.0;
+#pragma unroll
+  for (int j = 0; j < CB; ++j) {
+    if (j < c) {
+      double v = x[j];
+#pragma unroll
+      for (int k = 0; k < j; ++k) v -= x[k] * D[j][k];
+      x[j] = v / D[j][j];
+    }
+  }
+  (void)inv;
+#pragma unroll
+  for (int j = 0; j < CB; ++j)
+    if (j < c) P[(int64_t)j * ld + c + i] = x[j];
 }
 
 __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
@@ -113,7 +148,8 @@ __global__ void __launch_bounds__(128) k_update(
     const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows,
     const int64_t* __restrict__ Lptr, const int* __restrict__ row_grp,
     const int* __restrict__ grp_target, const int* __restrict__ grp_jfirst,
-    const int64_t* __restrict__ grp_relind, const int* __restrict__ relind, double* __restrict__ L) {
+    const int64_t* __restrict__ grp_relind, const int* __restrict__ relind, double* __restrict__ L,
+    int use_atomics) {
   extern __shared__ double sm[];
   double* As = sm;                       // [kSnCols][kLdsU]
   double* Bs = sm + kSnCols * kLdsU;     // [kSnCols][kLdsU]
@@ -170,7 +206,11 @@ __global__ void __launch_bounds__(128) k_update(
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
         const int i = tile.i0 + wr + a * 8 + g;
-        if (i < r && i >= j) atomicAdd(dstcol + rel[i], -acc[a][b][e]);
+        if (i < r && i >= j) {
+          // one supernode per level: every target entry has a single writer
+          if (use_atomics) atomicAdd(dstcol + rel[i], -acc[a][b][e]);
+          else dstcol[rel[i]] -= acc[a][b][e];
+        }
       }
     }
   }
@@ -265,6 +305,22 @@ void build_factor_plan(temf_ctx& c) {
     F.grp_relind.upload(gr.data(), gr.size(), st);
     F.relind.upload(rel.data(), rel.size(), st);
   }
+  // row chunks of the triangular solves per level
+  {
+    std::vector<TrsmChunk> ch;
+    std::vector<int64_t> lp(S.nlevels + 1, 0);
+    for (int l = 0; l < S.nlevels; ++l) {
+      for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+        const int s = S.level_sn[q];
+        const int r = (int)nrows(s);
+        for (int r0 = 0; r0 < r; r0 += kTrsmRows) ch.push_back({s, r0});
+      }
+      lp[l + 1] = (int64_t)ch.size();
+    }
+    F.trsm_level_ptr = lp;
+    F.n_trsm = (int64_t)ch.size();
+    F.trsm.upload(reinterpret_cast<const int2*>(ch.data()), ch.size(), st);
+  }
   // tiles per level
   {
     std::vector<UpdTile> tiles;
@@ -308,8 +364,14 @@ int numeric_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
   for (int l = 0; l < S.nlevels; ++l) {
     const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
     if (cnt > 0) {
-      k_potrf_trsm<<<cnt, kFacThreads, 0, st>>>(F.level_sn.p + S.level_ptr[l], F.sn_first.p, F.sn_rows_ptr.p,
-                                                F.sn_Lptr.p, fs.L.p, c.d_status.p);
+      k_potrf<<<cnt, kFacThreads, 0, st>>>(F.level_sn.p + S.level_ptr[l], F.sn_first.p, F.sn_rows_ptr.p,
+                                           F.sn_Lptr.p, fs.L.p, c.d_status.p);
+      TEMF_CHECK_LAUNCH();
+    }
+    const int64_t c0 = F.trsm_level_ptr[l], c1 = F.trsm_level_ptr[l + 1];
+    if (c1 > c0) {
+      k_trsm<<<(unsigned)(c1 - c0), kFacThreads, 0, st>>>(reinterpret_cast<const TrsmChunk*>(F.trsm.p) + c0,
+                                                          F.sn_first.p, F.sn_rows_ptr.p, F.sn_Lptr.p, fs.L.p);
       TEMF_CHECK_LAUNCH();
     }
     const int64_t t0 = F.tile_level_ptr[l], t1 = F.tile_level_ptr[l + 1];
@@ -317,7 +379,8 @@ int numeric_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
       if (t1 - t0 > INT_MAX) throw StateError("too many update tiles in one level");
       k_update<<<(unsigned)(t1 - t0), 128, upd_smem, st>>>(F.tiles.p + t0, F.sn_first.p, F.sn_rows_ptr.p,
                                                           F.sn_rows.p, F.sn_Lptr.p, F.row_grp.p, F.grp_target.p,
-                                                          F.grp_jfirst.p, F.grp_relind.p, F.relind.p, fs.L.p);
+                                                          F.grp_jfirst.p, F.grp_relind.p, F.relind.p, fs.L.p,
+                                                          cnt > 1 ? 1 : 0);
       TEMF_CHECK_LAUNCH();
     }
   }

@@ -136,7 +136,7 @@ struct Engine {
     return ms;
   }
 
-  int64_t solve_launches() const { return 2 * (int64_t)c.sym.nlevels; }
+  int64_t solve_launches() const { return 2; }  // persistent forward + backward kernels
 
   // one BDF2 step: out = A^{-1} (M (4 e2 - e3) - coef * s)
   void step(const double* e2, const double* e3, double* out, const double* coefp, double* const* Lb) {
@@ -307,6 +307,8 @@ struct Engine {
         TEMF_CUDA(cudaEventSynchronize(ev1));
         TEMF_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
         res.ms_steps += ms;
+        if (const int fl = solve_error_flag(c))
+          throw StateError("a triangular-solve wait timed out (code " + std::to_string(fl) + ")");
         double error = 0.0;
         for (int q = 0; q < nrhs; ++q) {
           const double e = std::sqrt(err_h[2 * q]) / std::sqrt(err_h[2 * q + 1]);
@@ -329,11 +331,13 @@ struct Engine {
           not_changed += 1;
         } else {
           sample(T(dsz - 1), 0);
-          copy_vec(E(0), E(last));
+          // e3 = all_e(idx) (src/FETD_FWD.f90:1405); the build that wrote the
+          // shipped LINUX/*.field files restarted from all_e(idx - sp_dblesize)
+          copy_vec(E(0), opt.legacy_linux ? E(last - dsz) : E(last));
           copy_vec(E(1), T(dsz - 1));
           e1 = E(0);
           set_current(other);
-          time_cur = tmp_time_cur + (opt.legacy_time_column ? step_cur : 0.0);
+          time_cur = tmp_time_cur + (opt.legacy_linux ? step_cur : 0.0);
           step_cur = tmp_step_cur;
           out_row(step, time_cur, step_cur);
           not_changed = 0;
@@ -354,6 +358,8 @@ struct Engine {
     N = flush_steps();
     if (N) e1 = E(N + 1);
     flush_trace();
+    if (const int fl = solve_error_flag(c))
+      throw StateError("a triangular-solve wait timed out (code " + std::to_string(fl) + ")");
     return e1;
   }
 
@@ -400,6 +406,7 @@ void run_fetd(temf_ctx& c, const RunOptions& opt, RunResult& res) {
   if (opt.step_dble < opt.step_dblesize + 2)
     throw ArgError("sp_double must be at least sp_dblesize + 2 (the coarse trial step reads the history)");
   res = RunResult();
+  clear_solve_error_flag(c);
   Engine eng(c, opt, res);
   eng.run();
 }

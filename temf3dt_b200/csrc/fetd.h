@@ -10,7 +10,10 @@ struct RunOptions {
   int step_dble = 0;            // sp_double
   int step_dblesize = 2;        // sp_dblesize
   double time_maximum = 0.0;    // time_maximum
-  int legacy_time_column = 0;   // time column of the shipped LINUX/*.field files
+  // Reproduce the build that wrote the shipped LINUX/*.field files: after an
+  // accepted dt-doubling trial it restarted BDF2 from all_e(idx - sp_dblesize)
+  // and advanced the time by one more old step than src/FETD_FWD.f90:1350,1405.
+  int legacy_linux = 0;
   int use_graphs = 1;           // capture full dt segments as CUDA graphs
   const int* forced = nullptr;  // per trial: 1 accept, 0 reject, <0 own decision (test hook)
   int n_forced = 0;

@@ -9,6 +9,10 @@ void ensure_update_buffer(temf_ctx& c, int nrhs);
 // `Lbase` points at a device word holding the panel base of the factor to use
 // (an indirection so captured graphs can follow the factor slot).
 void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st);
+// Timeout flag of the persistent solve kernels (0 = fine; 1..4 = which wait
+// gave up).  Reading it synchronises the stream.
+int solve_error_flag(temf_ctx& c);
+void clear_solve_error_flag(temf_ctx& c);
 
 // y = M (4 e2 - e3) for nrhs columns (row-major), permuted order.
 void launch_bdf_rhs(temf_ctx& c, const double* e2, const double* e3, double* y, int nrhs, cudaStream_t st);

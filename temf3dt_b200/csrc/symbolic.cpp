@@ -220,6 +220,8 @@ void analyse(int n, const int64_t* xadj, const int* adj, const double* xyz,
   }
   double t3 = now_s();
   out.t_colcount = t3 - t2;
+  out.nnzL_exact = 0;
+  for (int j = 0; j < n; ++j) out.nnzL_exact += cc[j];
 
   // --- fundamental supernodes ---
   std::vector<int> nchild(n, 0);

@@ -37,7 +37,8 @@ struct Symbolic {
   std::vector<int> level_ptr;       // nlevels+1
   std::vector<int> level_sn;        // supernodes grouped by level
   // statistics
-  int64_t nnzL = 0;                 // structural nonzeros of L (lower triangle incl. diagonal)
+  int64_t nnzL = 0;                 // nonzeros of L held by the supernodes (incl. amalgamation zeros)
+  int64_t nnzL_exact = 0;           // structural nonzeros of L (sum of column counts)
   int64_t stored = 0;               // doubles stored in the panels
   double flops = 0.0;               // factor flops (mul+add counted as 2)
   double t_order = 0, t_etree = 0, t_colcount = 0, t_super = 0;

@@ -207,9 +207,9 @@ class FetdGPU:
 
     # -- time loop ------------------------------------------------------------------
     def run(self, sp_division: int, sp_double: int, sp_dblesize: int, time_maximum: float,
-            legacy_time_column: bool = False, graphs: bool = True, forced: Optional[Sequence[int]] = None,
+            legacy_linux: bool = False, graphs: bool = True, forced: Optional[Sequence[int]] = None,
             max_steps: int = 0) -> RunOutput:
-        flags = (1 if legacy_time_column else 0) | (0 if graphs else 2)
+        flags = (1 if legacy_linux else 0) | (0 if graphs else 2)
         f = as_i32(forced) if forced is not None else None
         self._ck(self._L.temf_run(self._h, int(sp_division), int(sp_double), int(sp_dblesize), float(time_maximum),
                                   flags, iptr(f) if f is not None else None, len(f) if f is not None else 0,
@@ -286,14 +286,14 @@ def load_case(gpu: FetdGPU, mesh: meshio.Mesh, ctl: meshio.Control, rec_tet: Opt
                 src_drc=src_drc, rec_tet=np.asarray(rec_tet))
 
 
-def run_case(root: str, device: int = 0, legacy_time_column: bool = False, write: bool = True) -> RunOutput:
+def run_case(root: str, device: int = 0, legacy_linux: bool = False, write: bool = True) -> RunOutput:
     """``./FETD -f ROOT``: read ROOT.mesh/.cntl, run on the GPU, write ROOT.field(2)."""
     mesh = meshio.read_mesh(root + ".mesh")
     ctl = meshio.read_cntl(root + ".cntl")
     with FetdGPU(device) as gpu:
         load_case(gpu, mesh, ctl)
         out = gpu.run(ctl.sp_division, ctl.sp_double, ctl.sp_dblesize, ctl.time_maximum,
-                      legacy_time_column=legacy_time_column)
+                      legacy_linux=legacy_linux)
         if write:
             meshio.write_field(root + ".field", out.steps, out.times, out.fields, ctl.output)
             if ctl.time_points is not None:

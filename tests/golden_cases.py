@@ -1,0 +1,122 @@
+"""Helpers shared by the tests: load golden fixtures, build oracle models and
+GPU models for the same inputs."""
+from __future__ import annotations
+
+import io
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from oracle import fetd_oracle as O  # noqa: E402
+from temf3dt_b200 import meshio  # noqa: E402
+
+GOLDEN = os.path.join(HERE, "golden")
+
+
+def load_fixture(name: str) -> dict:
+    with np.load(os.path.join(GOLDEN, name + ".npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+def _cntl_file(text: str) -> str:
+    fd, path = tempfile.mkstemp(suffix=".cntl")
+    with os.fdopen(fd, "w") as fh:
+        fh.write(str(text))
+    return path
+
+
+def oracle_control(fx: dict) -> O.Control:
+    path = _cntl_file(fx["cntl"])
+    try:
+        return O.read_cntl(path)
+    finally:
+        os.unlink(path)
+
+
+def host_control(fx: dict) -> meshio.Control:
+    path = _cntl_file(fx["cntl"])
+    try:
+        return meshio.read_cntl(path)
+    finally:
+        os.unlink(path)
+
+
+def fixture_mesh_dict(fx: dict) -> dict:
+    return dict(nod_cor=fx["nod_cor"], tet_vex=fx["tet_vex"].astype(np.int64), tet_phy=fx["tet_phy"].astype(np.int64),
+                src_vex=fx["src_vex"].astype(np.int64), src_phy=fx["src_phy"].astype(np.int64))
+
+
+def fixture_mesh(fx: dict) -> meshio.Mesh:
+    d = fixture_mesh_dict(fx)
+    return meshio.Mesh(d["nod_cor"], d["tet_vex"], d["tet_phy"], d["src_vex"], d["src_phy"])
+
+
+def sigma_rescale_factor(sig_dom) -> float:
+    """src_small's sig_parameter (src_small/FETD_FWD.f90:314-323): 1 / sigma of
+    the last domain read (the earth in the shipped example)."""
+    return 1.0 / float(sig_dom[-1])
+
+
+def output_scale(p: float) -> float:
+    """src_small/FETD_FWD.f90:1526: a_f / p**2 * pi**log10(p)."""
+    return float(np.pi ** np.log10(p) / p ** 2)
+
+
+def oracle_model_from_fixture(fx: dict, sigma_rescale: bool = False):
+    ctl = oracle_control(fx)
+    scale = 1.0
+    if sigma_rescale:
+        p = sigma_rescale_factor(ctl.sig_dom)
+        ctl.sig_dom = ctl.sig_dom.copy()
+        ctl.sig_dom[1:] = ctl.sig_dom[1:] * p
+        scale = output_scale(p)
+    return O.build_model(fixture_mesh_dict(fx), ctl), scale
+
+
+def host_model_from_fixture(fx: dict, sigma_rescale: bool = False):
+    ctl = host_control(fx)
+    scale = 1.0
+    if sigma_rescale:
+        p = sigma_rescale_factor([d[1] for d in ctl.domains])
+        ctl.domains = [ctl.domains[0]] + [(d[0], d[1] * p, d[2], d[3]) for d in ctl.domains[1:]]
+        scale = output_scale(p)
+    return fixture_mesh(fx), ctl, scale
+
+
+def synth_oracle_model(model) -> O.OracleModel:
+    """Oracle model for a temf3dt_b200.synth.Model (same arrays)."""
+    c = model.ctl
+    oc = O.Control(rec_cor=c.rec_cor, rec_charac=c.rec_charac,
+                   dom_ind=np.array([d[0] for d in c.domains]), sig_dom=np.array([d[1] for d in c.domains]),
+                   per_dom=np.array([d[2] for d in c.domains]) * O.EPS0,
+                   mag_dom=np.array([d[3] for d in c.domains]) * O.MU0,
+                   src_num=1, src_sourcetype=c.source_type, src_pulsetype=c.pulse_type, src_pulsewidth=c.t0,
+                   src_current=c.current, step_mthd=2, step_dvsi=c.sp_division, time_maxm=c.time_maximum,
+                   step_dble=c.sp_double, step_dblesize=c.sp_dblesize, o_f=c.output, time_channels=c.time_points)
+    mesh = dict(nod_cor=model.mesh.nod_cor, tet_vex=model.mesh.tet_vex, tet_phy=model.mesh.tet_phy,
+                src_vex=model.mesh.src_vex, src_phy=model.mesh.src_phy)
+    return O.build_model(mesh, oc)
+
+
+def small_synth(**kw):
+    """A small synthetic half-space model (~37k edges) used by the parity tests."""
+    from temf3dt_b200 import synth
+    args = dict(h_core=250, ratio=2.5, h_z=50, z_core=150, sp_double=20, time_maximum=2e-4)
+    args.update(kw)
+    return synth.build_model("halfspace", **args)
+
+
+def tiny_synth(**kw):
+    """A tiny synthetic model (~5k edges) for quick oracle runs."""
+    from temf3dt_b200 import synth
+    args = dict(radius=200.0, h_core=200, ratio=3.0, h_z=100, z_core=100, half=20000.0, sp_double=8,
+                sp_division=4, time_maximum=2e-5)
+    args.update(kw)
+    return synth.build_model("halfspace", **args)

@@ -1,0 +1,180 @@
+"""Host-side logic of the package and the C ABI that runs without a GPU:
+exported symbols, mesh topology, ordering/symbolic analysis, file formats and
+the synthetic model generator."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import fetd_oracle as O
+from temf3dt_b200 import _lib, fetd, meshio, synth
+from tests.golden_cases import ROOT, fixture_mesh, host_control, load_fixture, tiny_synth
+
+
+def _header_functions():
+    with open(os.path.join(ROOT, "include", "temf_b200.h")) as fh:
+        txt = fh.read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(temf_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_header_symbol():
+    lib = _lib.lib()
+    names = _header_functions()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in _lib.SIGNATURES, "no ctypes signature for %s" % n
+    assert b"sm_100a" in lib.temf_version()
+
+
+def test_topology_matches_oracle():
+    fx = load_fixture("src_small_mod_small")
+    tv = fx["tet_vex"].astype(np.int64)
+    ev, te, td = fetd.mesh_topology(tv)
+    e2, t2, d2 = O.build_topology(tv)
+    assert np.array_equal(ev, e2) and np.array_equal(te, t2) and np.array_equal(td, d2)
+
+
+def test_source_edges_follow_reference_convention():
+    fx = load_fixture("linux_mod_big")
+    ev, _, _ = fetd.mesh_topology(fx["tet_vex"])
+    se, sd = fetd.source_edges(ev, fx["src_vex"])
+    oe, od = O.source_edges(ev, fx["src_vex"].astype(np.int64))
+    assert np.array_equal(se, oe) and np.array_equal(sd, od)
+    assert sd[-1] == -1 and (sd[:-1] == 1).all()
+
+
+def _grid_pattern(nx, ny, nz):
+    """7-point pattern of an nx*ny*nz grid with coordinates."""
+    idx = np.arange(nx * ny * nz).reshape(nz, ny, nx)
+    rows, cols = [], []
+    for ax, sh in ((2, 1), (1, 1), (0, 1)):
+        a = np.take(idx, np.arange(idx.shape[ax] - 1), axis=ax).ravel()
+        b = np.take(idx, np.arange(1, idx.shape[ax]), axis=ax).ravel()
+        rows += [a, b]; cols += [b, a]
+    rows = np.concatenate(rows); cols = np.concatenate(cols)
+    n = nx * ny * nz
+    order = np.lexsort((cols, rows))
+    rows, cols = rows[order], cols[order]
+    xadj = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(xadj, rows + 1, 1)
+    xadj = np.cumsum(xadj)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    xyz = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1).astype(np.float64)
+    return n, xadj, cols.astype(np.int32), xyz
+
+
+def _symbolic(n, xadj, adj, xyz):
+    perm = np.zeros(n, dtype=np.int32)
+    st = np.zeros(9)
+    xa = np.ascontiguousarray(xadj, dtype=np.int64)
+    rc = _lib.lib().temf_symbolic_host(n, xa.ctypes.data_as(C.POINTER(C.c_longlong)), _lib.iptr(adj),
+                                       _lib.dptr(np.ascontiguousarray(xyz)), _lib.iptr(perm), _lib.dptr(st))
+    assert rc == 0
+    return perm, st
+
+
+def test_symbolic_nnz_matches_dense_cholesky():
+    """The column counts of the symbolic factorisation equal the nonzero count
+    of a dense Cholesky of a random SPD matrix with the same pattern in the
+    computed order (no numerical cancellation in practice); the supernodes
+    (with amalgamation zeros) hold at least that many."""
+    n, xadj, adj, xyz = _grid_pattern(9, 8, 7)
+    perm, st = _symbolic(n, xadj, adj, xyz)
+    assert np.array_equal(np.sort(perm), np.arange(n))
+    rng = np.random.default_rng(3)
+    A = np.zeros((n, n))
+    for i in range(n):
+        for p in range(xadj[i], xadj[i + 1]):
+            A[i, adj[p]] = -rng.uniform(0.1, 1.0)
+    A = A + A.T
+    A[np.arange(n), np.arange(n)] = np.abs(A).sum(axis=1) + 1.0
+    L = np.linalg.cholesky(A[np.ix_(perm, perm)])
+    assert int((np.abs(L) > 0).sum()) == int(st[8])
+    assert st[3] >= st[8]
+    assert st[1] >= 1 and st[2] >= 1
+    # flops are at least the dense-column count lower bound
+    assert st[5] > st[3]
+
+
+def test_symbolic_on_reference_mesh():
+    fx = load_fixture("src_small_mod_small")
+    ev, te, _ = fetd.mesh_topology(fx["tet_vex"])
+    n = len(ev)
+    import scipy.sparse as sp
+    r = np.repeat(te - 1, 6, axis=1).ravel(); c = np.tile(te - 1, (1, 6)).ravel()
+    G = sp.coo_matrix((np.ones(len(r)), (r, c)), shape=(n, n)).tocsr()
+    G.setdiag(0); G.eliminate_zeros(); G.sort_indices()
+    xyz = 0.5 * (fx["nod_cor"][ev[:, 0] - 1] + fx["nod_cor"][ev[:, 1] - 1])
+    perm, st = _symbolic(n, G.indptr.astype(np.int64), G.indices.astype(np.int32), xyz)
+    assert np.array_equal(np.sort(perm), np.arange(n))
+    assert st[3] < 0.05 * n * n       # far from dense
+    assert st[3] >= (G.nnz // 2 + n)  # at least the lower triangle of A
+
+
+def test_meshio_roundtrip(tmp_path):
+    m = tiny_synth()
+    p = str(tmp_path / "m.mesh")
+    meshio.write_mesh(p, m.mesh)
+    r = meshio.read_mesh(p)
+    assert np.array_equal(r.tet_vex, m.mesh.tet_vex) and np.allclose(r.nod_cor, m.mesh.nod_cor, rtol=0, atol=0)
+    assert np.array_equal(r.src_vex, m.mesh.src_vex)
+    # the oracle's own reader agrees
+    o = O.read_mesh(p)
+    assert np.array_equal(o["tet_vex"], m.mesh.tet_vex) and np.array_equal(o["src_vex"], m.mesh.src_vex)
+    pc = str(tmp_path / "m.cntl")
+    meshio.write_cntl(pc, m.ctl)
+    c2 = meshio.read_cntl(pc)
+    oc = O.read_cntl(pc)
+    assert c2.sp_double == m.ctl.sp_double and np.allclose(c2.rec_cor, m.ctl.rec_cor)
+    assert oc.step_dble == m.ctl.sp_double and np.allclose(oc.time_channels, m.ctl.time_points)
+
+
+def test_read_reference_cntl():
+    for name in ("linux_mod_big", "src_small_mod_small"):
+        c = host_control(load_fixture(name))
+        assert c.sp_mthd == 2 and c.sp_dblesize == 2 and c.output[5] and c.output.sum() == 1
+        assert c.domains[0][0] == 11 and c.domains[0][1] > 0
+
+
+def test_field_roundtrip(tmp_path):
+    steps = np.arange(4)
+    times = np.array([0.0, 1e-8, 2e-8, 3.5e-8])
+    f = np.random.default_rng(0).standard_normal((4, 2, 9))
+    mask = np.zeros(9, dtype=bool); mask[[3, 5]] = True
+    p = str(tmp_path / "x.field")
+    meshio.write_field(p, steps, times, f, mask)
+    r = meshio.read_field(p)
+    assert r.shape == (4, 2 + 2 * 2)
+    assert np.allclose(r[:, 2:].reshape(4, 2, 2), f[:, :, [3, 5]], rtol=1e-5)
+
+
+@pytest.mark.parametrize("kind", ["halfspace", "multiloop"])
+def test_synth_models(kind):
+    kw = dict(h_core=250, ratio=2.5, h_z=50, z_core=150) if kind == "halfspace" else \
+        dict(n_loops=3, h_core=60, ratio=2.2, h_z=60, scale=1.0)
+    m = synth.build_model(kind, **kw)
+    P = m.mesh.nod_cor[m.mesh.tet_vex - 1]
+    d = np.einsum("ti,ti->t", P[:, 1] - P[:, 0], np.cross(P[:, 2] - P[:, 0], P[:, 3] - P[:, 0]))
+    assert (d > 0).all()
+    ev, _, _ = fetd.mesh_topology(m.mesh.tet_vex)
+    cols = m.source_columns(ev)
+    se, sd = fetd.source_edges(ev, m.mesh.src_vex)
+    assert np.array_equal(cols[0][0], se) and np.array_equal(cols[0][1], sd)
+    for lp in m.loops:   # closed loop: consecutive vertices are mesh edges
+        assert len(lp) >= 4
+    # every receiver lies strictly inside exactly one tet
+    for p in m.receivers:
+        X = m.mesh.nod_cor[m.mesh.tet_vex - 1]
+        mid = X.mean(axis=1)
+        near = np.nonzero(np.linalg.norm(mid - p, axis=1) < 5000)[0]
+        inside = 0
+        for t in near:
+            T = np.concatenate([X[t], np.ones((4, 1))], axis=1)
+            lam = np.linalg.solve(T.T, np.append(p, 1.0))
+            if (lam > 1e-9).all():
+                inside += 1
+        assert inside == 1
