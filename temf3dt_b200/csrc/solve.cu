@@ -41,7 +41,7 @@ __device__ __forceinline__ void wait_geq(const int* flag, int target, int* err, 
       atomicExch(err, code);
       break;
     }
-    if (it > 64) __nanosleep(64);
+    if (it > 256) __nanosleep(32);
   }
   __threadfence();
 }
@@ -49,7 +49,8 @@ __device__ __forceinline__ void wait_geq(const int* flag, int target, int* err, 
 // Dense lower-triangular solve of the c x c diagonal block held in D (shared)
 // for nrhs columns of ys (row-major c x nrhs), forward (L y = b) or backward
 // (L^T x = z).  nrhs == 1 runs in one warp with shuffles.
-__device__ void diag_solve(const double (*D)[kSnCols + 1], double* ys, int c, int nrhs, bool forward) {
+__device__ void diag_solve(const double (*D)[kSnCols + 1], const double* rinv, double* ys, int c, int nrhs,
+                           bool forward) {
   const int tid = threadIdx.x;
   if (nrhs == 1) {
     if (tid < 32) {
@@ -59,7 +60,7 @@ __device__ void diag_solve(const double (*D)[kSnCols + 1], double* ys, int c, in
       if (forward) {
         for (int j = 0; j < c; ++j) {
           const double v = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-          const double yj = v / D[j][j];
+          const double yj = v * rinv[j];
           if (lane == (j & 31)) { if (j < 32) v0 = yj; else v1 = yj; }
           if (lane > j && lane < c) v0 -= D[lane][j] * yj;
           if (lane + 32 > j && lane + 32 < c) v1 -= D[lane + 32][j] * yj;
@@ -67,7 +68,7 @@ __device__ void diag_solve(const double (*D)[kSnCols + 1], double* ys, int c, in
       } else {
         for (int j = c - 1; j >= 0; --j) {
           const double v = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-          const double xj = v / D[j][j];
+          const double xj = v * rinv[j];
           if (lane == (j & 31)) { if (j < 32) v0 = xj; else v1 = xj; }
           if (lane < j) v0 -= D[j][lane] * xj;
           if (lane + 32 < j) v1 -= D[j][lane + 32] * xj;
@@ -81,7 +82,7 @@ __device__ void diag_solve(const double (*D)[kSnCols + 1], double* ys, int c, in
   }
   if (forward) {
     for (int j = 0; j < c; ++j) {
-      for (int col = tid; col < nrhs; col += blockDim.x) ys[j * nrhs + col] /= D[j][j];
+      for (int col = tid; col < nrhs; col += blockDim.x) ys[j * nrhs + col] *= rinv[j];
       __syncthreads();
       for (int idx = tid; idx < (c - j - 1) * nrhs; idx += blockDim.x) {
         const int k = j + 1 + idx / nrhs, col = idx % nrhs;
@@ -91,7 +92,7 @@ __device__ void diag_solve(const double (*D)[kSnCols + 1], double* ys, int c, in
     }
   } else {
     for (int j = c - 1; j >= 0; --j) {
-      for (int col = tid; col < nrhs; col += blockDim.x) ys[j * nrhs + col] /= D[j][j];
+      for (int col = tid; col < nrhs; col += blockDim.x) ys[j * nrhs + col] *= rinv[j];
       __syncthreads();
       for (int idx = tid; idx < j * nrhs; idx += blockDim.x) {
         const int k = idx / nrhs, col = idx % nrhs;
@@ -102,10 +103,18 @@ __device__ void diag_solve(const double (*D)[kSnCols + 1], double* ys, int c, in
   }
 }
 
-__device__ __forceinline__ void load_diag(double (*D)[kSnCols + 1], const double* P, int c, int64_t ld) {
-  for (int idx = threadIdx.x; idx < c * c; idx += blockDim.x) {
-    const int j = idx / c, i = idx % c;
-    if (i >= j) D[i][j] = __ldg(P + (int64_t)j * ld + i);
+// Lower triangle of the diagonal block (one warp per column, coalesced) and
+// the reciprocals of its diagonal.
+__device__ __forceinline__ void load_diag(double (*D)[kSnCols + 1], double* rinv, const double* P, int c,
+                                          int64_t ld) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = warp; j < c; j += nw) {
+    const double* col = P + (int64_t)j * ld;
+    for (int i = j + lane; i < c; i += 32) {
+      const double v = __ldg(col + i);
+      D[i][j] = v;
+      if (i == j) rinv[j] = 1.0 / v;
+    }
   }
 }
 
@@ -181,6 +190,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_persistent(
     double* const* Lbase, double* x, int nrhs, const int* __restrict__ tgt_ptr, const int* __restrict__ tgt,
     const int* __restrict__ expect, int* sync, int nsn, int* err) {
   __shared__ double D[kSnCols][kSnCols + 1];
+  __shared__ double rinv[kSnCols];
   extern __shared__ double ys[];  // c x nrhs
   __shared__ int task_id;
   int* ready = sync;
@@ -208,12 +218,12 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_persistent(
     FwdRegs R;
     if (nrhs == 1) pre_fwd(R, Pc, c, ld, i, row_on);
     if (T.kind == 0) {
-      load_diag(D, P, c, ld);
+      load_diag(D, rinv, P, c, ld);
       if (tid == 0) wait_geq(ready + s, expect[s], err, 1);
       __syncthreads();
       for (int idx = tid; idx < c * nrhs; idx += blockDim.x) ys[idx] = __ldcg(x + (int64_t)f * nrhs + idx);
       __syncthreads();
-      diag_solve(D, ys, c, nrhs, true);
+      diag_solve(D, rinv, ys, c, nrhs, true);
       for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = ys[idx];
       __threadfence();
       __syncthreads();
@@ -259,6 +269,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_persistent(
     const int* __restrict__ nchunk, const int64_t* __restrict__ part_off, double* part, int* sync, int nsn,
     int* err) {
   __shared__ double D[kSnCols][kSnCols + 1];
+  __shared__ double rinv[kSnCols];
   __shared__ double seg[4][kSnCols];
   extern __shared__ double zs[];  // max(c, chunk rows) x nrhs
   __shared__ int task_id;
@@ -284,7 +295,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_persistent(
     const int nr = T.r1 - T.r0;
     BwdRegs R;
     if (nrhs == 1 && nr > 0) pre_bwd(R, P, c, ld, T.r0, nr);
-    if (T.kind == 0) load_diag(D, P, c, ld);
+    if (T.kind == 0) load_diag(D, rinv, P, c, ld);
     // the chunk's rows need their owners' x; the diagonal task also its other chunks
     if (tid == 0) {
       for (int q = own_ptr[t]; q < own_ptr[t + 1]; ++q) wait_geq(xdone + own[q], 1, err, 3);
@@ -348,7 +359,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_persistent(
         }
       }
       __syncthreads();
-      diag_solve(D, zs, c, nrhs, false);
+      diag_solve(D, rinv, zs, c, nrhs, false);
       for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = zs[idx];
       __threadfence();
       __syncthreads();

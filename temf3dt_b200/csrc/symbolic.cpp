@@ -20,10 +20,15 @@ double now_s() {
 // ---------------------------------------------------------------------------
 // Nested dissection by recursive coordinate bisection.
 //
-// A subset is split at the median of one coordinate axis; the vertex
-// separator is the boundary of the smaller-boundary side.  The axis with the
-// smallest separator is kept.  Each subset is ordered: left part, right part,
-// separator (so separators are eliminated last, forming the top of the tree).
+// For a subset, each coordinate axis is sorted once and the vertex separator
+// of EVERY split position k (left = the k lowest along the axis) is counted in
+// one pass: a left vertex is on the left boundary for the splits
+// rank < k <= max neighbour rank, a right vertex on the right boundary for
+// min neighbour rank < k <= rank; difference arrays turn those intervals into
+// counts for all k.  The split with the smallest boundary among balanced ones
+// (35-65 %) wins; the smaller-side boundary becomes the separator.  Each
+// subset is ordered: left part, right part, separator (separators are
+// eliminated last, forming the top of the elimination tree).
 // ---------------------------------------------------------------------------
 struct NDState {
   int n;
@@ -32,85 +37,183 @@ struct NDState {
   const double* xyz;
   int leaf;
   std::vector<int> stamp;   // subset id a vertex currently belongs to
-  std::vector<signed char> side;
+  std::vector<int> rank;    // rank along the axis being evaluated
   std::vector<int> order;   // output: new -> old
-  std::vector<double> key;
   int next_id = 1;
 };
 
-// Separator size when the subset v[0..m) is split at the median along `axis`.
-// On return side[] holds 0/1 for the chosen split and `use_left` says which
-// boundary is smaller.
-int try_split(NDState& S, int* v, int m, int axis, int id, bool& use_left) {
-  const int half = m / 2;
-  std::nth_element(v, v + half, v + m, [&](int a, int b) {
+struct Split {
+  int axis = -1;
+  int k = 0;          // left = the k lowest
+  int sep = -1;
+  bool left = true;   // separator taken from the left boundary
+  double cost = 0;
+};
+
+// Evaluate all split positions along `axis`; leaves v sorted along the axis.
+void eval_axis(NDState& S, int* v, int m, int axis, int id, Split& best) {
+  std::sort(v, v + m, [&](int a, int b) {
     double ka = S.xyz[3 * (int64_t)a + axis], kb = S.xyz[3 * (int64_t)b + axis];
     return ka < kb || (ka == kb && a < b);
   });
-  for (int i = 0; i < half; ++i) { S.side[v[i]] = 0; S.stamp[v[i]] = id; }
-  for (int i = half; i < m; ++i) { S.side[v[i]] = 1; S.stamp[v[i]] = id; }
-  int bl = 0, br = 0;
+  for (int i = 0; i < m; ++i) { S.rank[v[i]] = i; S.stamp[v[i]] = id; }
+  std::vector<int> dl(m + 2, 0), dr(m + 2, 0);
   for (int i = 0; i < m; ++i) {
-    int u = v[i];
-    int su = S.side[u];
+    const int u = v[i];
+    int mx = -1, mn = m;
     for (int64_t p = S.xadj[u]; p < S.xadj[u + 1]; ++p) {
-      int w = S.adj[p];
-      if (S.stamp[w] == id && S.side[w] != su) {
-        if (su == 0) ++bl; else ++br;
-        break;
-      }
+      const int w = S.adj[p];
+      if (S.stamp[w] != id) continue;
+      const int rw = S.rank[w];
+      mx = std::max(mx, rw);
+      mn = std::min(mn, rw);
+    }
+    if (mx > i) { dl[i + 1] += 1; dl[mx + 1] -= 1; }   // left boundary for k in (i, mx]
+    if (mn < i) { dr[mn + 1] += 1; dr[i + 1] -= 1; }   // right boundary for k in (mn, i]
+  }
+  const int lo = std::max(1, (int)(0.35 * m)), hi = std::min(m - 1, (int)(0.65 * m));
+  int bl = 0, br = 0;
+  for (int k = 0; k <= hi; ++k) {
+    bl += dl[k];
+    br += dr[k];
+    if (k < lo) continue;
+    const int sep = std::min(bl, br);
+    const double cost = sep + 1e-3 * m * std::fabs((double)k / m - 0.5);
+    if (best.sep < 0 || cost < best.cost) {
+      best.axis = axis; best.k = k; best.sep = sep; best.left = bl <= br; best.cost = cost;
     }
   }
-  use_left = bl <= br;
-  return use_left ? bl : br;
 }
 
 void nd_rec(NDState& S, int* v, int m) {
   if (m <= S.leaf) {
-    // leaf: order by a coordinate sweep (keeps the leaf block banded)
     for (int i = 0; i < m; ++i) S.order.push_back(v[i]);
     return;
   }
-  int best_axis = 0, best_sep = -1;
-  bool best_left = true;
-  // extent per axis
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   for (int i = 0; i < m; ++i)
     for (int a = 0; a < 3; ++a) {
       double x = S.xyz[3 * (int64_t)v[i] + a];
       lo[a] = std::min(lo[a], x); hi[a] = std::max(hi[a], x);
     }
+  Split best;
   for (int axis = 0; axis < 3; ++axis) {
     if (hi[axis] <= lo[axis]) continue;
-    bool ul;
-    int id = S.next_id++;
-    int sep = try_split(S, v, m, axis, id, ul);
-    if (best_sep < 0 || sep < best_sep) { best_sep = sep; best_axis = axis; best_left = ul; }
+    eval_axis(S, v, m, axis, S.next_id++, best);
   }
-  if (best_sep < 0) {  // all points coincide: give up splitting
+  if (best.axis < 0) {  // all points coincide: give up splitting
     for (int i = 0; i < m; ++i) S.order.push_back(v[i]);
     return;
   }
-  bool ul;
-  int id = S.next_id++;
-  try_split(S, v, m, best_axis, id, ul);
-  (void)ul;
-  const int sep_side = best_left ? 0 : 1;
-  // classify: separator = vertices on sep_side with a neighbour on the other side
-  std::vector<int> L, R, Sp;
-  L.reserve(m / 2 + 1); R.reserve(m / 2 + 1);
+  // re-sort along the chosen axis (v holds the order of the last axis tried)
+  const int id = S.next_id++;
+  std::sort(v, v + m, [&](int a, int b) {
+    double ka = S.xyz[3 * (int64_t)a + best.axis], kb = S.xyz[3 * (int64_t)b + best.axis];
+    return ka < kb || (ka == kb && a < b);
+  });
+  for (int i = 0; i < m; ++i) { S.rank[v[i]] = i; S.stamp[v[i]] = id; }
+  // Minimum vertex cover of the bipartite graph of cut edges (Koenig): maximum
+  // matching between the left boundary BL and the right boundary BR, then the
+  // alternating search from unmatched BL vertices; cover = (BL \ Z) u (BR n Z).
+  // It is never larger than either boundary.
+  std::vector<int> BL, BR;
   for (int i = 0; i < m; ++i) {
-    int u = v[i];
-    int su = S.side[u];
-    bool is_sep = false;
-    if (su == sep_side) {
-      for (int64_t p = S.xadj[u]; p < S.xadj[u + 1]; ++p) {
-        int w = S.adj[p];
-        if (S.stamp[w] == id && S.side[w] != su) { is_sep = true; break; }
+    const int u = v[i];
+    const bool on_left = i < best.k;
+    for (int64_t p = S.xadj[u]; p < S.xadj[u + 1]; ++p) {
+      const int w = S.adj[p];
+      if (S.stamp[w] == id && ((S.rank[w] < best.k) != on_left)) {
+        (on_left ? BL : BR).push_back(u);
+        break;
       }
     }
-    if (is_sep) Sp.push_back(u);
-    else if (su == 0) L.push_back(u);
+  }
+  // local indices: BL -> [0, nbl), BR -> [0, nbr) via `pos` (reuse rank storage after the cut is fixed)
+  std::vector<int> pos_of(BL.size() + BR.size());
+  std::vector<char> in_cover;
+  {
+    const int nbl = (int)BL.size(), nbr = (int)BR.size();
+    std::vector<int> lidx(m, -1);  // by rank
+    for (int q = 0; q < nbl; ++q) lidx[S.rank[BL[q]]] = q;
+    for (int q = 0; q < nbr; ++q) lidx[S.rank[BR[q]]] = q;
+    std::vector<int> gptr(nbl + 1, 0), gadj;
+    for (int q = 0; q < nbl; ++q) {
+      const int u = BL[q];
+      for (int64_t p = S.xadj[u]; p < S.xadj[u + 1]; ++p) {
+        const int w = S.adj[p];
+        if (S.stamp[w] == id && S.rank[w] >= best.k) gadj.push_back(lidx[S.rank[w]]);
+      }
+      gptr[q + 1] = (int)gadj.size();
+    }
+    std::vector<int> mL(nbl, -1), mR(nbr, -1);
+    for (int q = 0; q < nbl; ++q)  // greedy start
+      for (int e = gptr[q]; e < gptr[q + 1]; ++e)
+        if (mR[gadj[e]] < 0) { mL[q] = gadj[e]; mR[gadj[e]] = q; break; }
+    std::vector<int> seen(nbl, -1), stackv, stacke, parentR(nbr, -1);
+    int budget = 200 * (nbl + nbr) + 100000;  // bounded work; fall back to the greedy matching
+    for (int q0 = 0; q0 < nbl && budget > 0; ++q0) {
+      if (mL[q0] >= 0) continue;
+      // iterative DFS for an augmenting path from q0
+      stackv.assign(1, q0); stacke.assign(1, gptr[q0]);
+      seen[q0] = q0;
+      int found = -1;
+      while (!stackv.empty() && found < 0 && budget-- > 0) {
+        const int q = stackv.back();
+        int& e = stacke.back();
+        if (e >= gptr[q + 1]) { stackv.pop_back(); stacke.pop_back(); continue; }
+        const int rr = gadj[e++];
+        const int nq = mR[rr];
+        if (nq < 0) { parentR[rr] = q; found = rr; break; }
+        if (seen[nq] == q0) continue;
+        seen[nq] = q0;
+        parentR[rr] = q;
+        stackv.push_back(nq);
+        stacke.push_back(gptr[nq]);
+      }
+      if (found >= 0) {  // flip the path
+        int rr = found;
+        while (true) {
+          const int q = parentR[rr];
+          const int prev = mL[q];
+          mL[q] = rr; mR[rr] = q;
+          if (q == q0) break;
+          rr = prev;
+        }
+      }
+    }
+    // Koenig: Z = vertices reachable from unmatched BL by alternating paths
+    std::vector<char> zl(nbl, 0), zr(nbr, 0);
+    std::vector<int> queue;
+    for (int q = 0; q < nbl; ++q)
+      if (mL[q] < 0) { zl[q] = 1; queue.push_back(q); }
+    for (size_t h = 0; h < queue.size(); ++h) {
+      const int q = queue[h];
+      for (int e = gptr[q]; e < gptr[q + 1]; ++e) {
+        const int rr = gadj[e];
+        if (zr[rr] || mL[q] == rr) continue;
+        zr[rr] = 1;
+        const int nq = mR[rr];
+        if (nq >= 0 && !zl[nq]) { zl[nq] = 1; queue.push_back(nq); }
+      }
+    }
+    in_cover.assign(m, 0);  // by rank
+    int cover = 0;
+    for (int q = 0; q < nbl; ++q) if (!zl[q]) { in_cover[S.rank[BL[q]]] = 1; ++cover; }
+    for (int q = 0; q < nbr; ++q) if (zr[q]) { in_cover[S.rank[BR[q]]] = 1; ++cover; }
+    // keep the plain boundary if the cover is not smaller (e.g. budget ran out)
+    const int plain = std::min(nbl, nbr);
+    if (cover >= plain) {
+      std::fill(in_cover.begin(), in_cover.end(), 0);
+      const bool use_left = nbl <= nbr;
+      for (int u : (use_left ? BL : BR)) in_cover[S.rank[u]] = 1;
+    }
+  }
+  std::vector<int> L, R, Sp;
+  L.reserve(best.k + 1); R.reserve(m - best.k + 1);
+  for (int i = 0; i < m; ++i) {
+    const int u = v[i];
+    if (in_cover[i]) Sp.push_back(u);
+    else if (i < best.k) L.push_back(u);
     else R.push_back(u);
   }
   std::copy(L.begin(), L.end(), v);
@@ -130,7 +233,7 @@ std::vector<int> nested_dissection(int n, const int64_t* xadj, const int* adj,
   NDState S;
   S.n = n; S.xadj = xadj; S.adj = adj; S.xyz = xyz; S.leaf = std::max(leaf_size, 4);
   S.stamp.assign(n, 0);
-  S.side.assign(n, 0);
+  S.rank.assign(n, 0);
   S.order.reserve(n);
   std::vector<int> v(n);
   std::iota(v.begin(), v.end(), 0);
