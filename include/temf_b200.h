@@ -93,6 +93,27 @@ int temf_factor(temf_ctx* ctx, int slot, double dt);
  * column-major with leading dimension ld >= n_edges (original numbering).
  * b and x may alias. */
 int temf_solve(temf_ctx* ctx, int slot, int nrhs, const double* b, double* x, int ld);
+/* Allocation-free solve.  It has no counterpart in the reference.  Some
+ * callers cannot let a library call cudaMalloc where they solve.  Examples
+ * are an application that reserves all device memory for its own pool up
+ * front, a driver that must not call into the allocator while another thread
+ * is capturing CUDA work, and a time loop that runs on a fixed memory budget.
+ * temf_solve allocates staging and scratch buffers on first use; this call
+ * allocates nothing.
+ * - x_dev = A^{-1} b_dev for one right-hand side, with the factor in `slot`.
+ * - b_dev and x_dev are DEVICE arrays of n_edges doubles in the original edge
+ *   numbering; they may alias.  They are the caller's memory.
+ * - Scratch lives in one static device array of 32 MiB that every GPU loading
+ *   the library holds until the process exits.  A factor whose solve needs
+ *   more returns TEMF_EARG with the byte count; use temf_solve then.
+ * - The first call on a device looks the array's address up (set-up), so make
+ *   that first call before any stream capture.
+ * - Every call shares the array, so calls whose GPU work overlaps (two
+ *   contexts, two threads, two devices' calls are separate arrays) race.
+ *   Serialise them.
+ * - The call runs on the context's stream and returns after the solve
+ *   finished. */
+int temf_solve_noalloc(temf_ctx* ctx, int slot, const double* b_dev, double* x_dev);
 /* Forget the factor in `slot` (pardiso_direct_3, src/FETD_UTILITY.f90:959-975).
  * Device memory is kept for reuse until temf_destroy. */
 int temf_release(temf_ctx* ctx, int slot);

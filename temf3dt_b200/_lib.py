@@ -36,6 +36,7 @@ SIGNATURES = {
     "temf_factor": (_i, [_p, _i, _d]),
     "temf_solve": (_i, [_p, _i, _i, _dp, _dp, _i]),
     "temf_release": (_i, [_p, _i]),
+    "temf_solve_noalloc": (_i, [_p, _i, _p, _p]),
     "temf_spmv": (_i, [_p, _i, _i, _dp, _dp, _i]),
     "temf_set_sources": (_i, [_p, _i, _ip, _ip, _ip, _i, _i, _d, _d]),
     "temf_set_receivers": (_i, [_p, _i, _ip, _dp, _ip]),

@@ -203,6 +203,15 @@ DBuf<int>& perm_dev(temf_ctx* c) {
   return *m.back().second;
 }
 
+}  // namespace
+
+namespace temf {
+// Device copy of the fill-reducing permutation (perm[new] = old) of a context.
+const int* ctx_perm_device(temf_ctx* c) { return perm_dev(c).p; }
+}  // namespace temf
+
+namespace {
+
 void need(bool cond, const char* msg) {
   if (!cond) throw StateError(msg);
 }

@@ -608,6 +608,24 @@ void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaSt
   TEMF_CHECK_LAUNCH();
 }
 
+void launch_solve_scratch(temf_ctx& c, double* const* Lbase, double* x, int* sync, double* part, int* err,
+                          cudaStream_t st) {
+  FactorPlan& F = c.fplan;
+  SolvePlan& P = c.splan;
+  const size_t smem = (size_t)(kSnCols + kChunkRows) * sizeof(double);
+  TEMF_CUDA(cudaMemsetAsync(sync, 0, (4 * (size_t)P.nsn + 4) * sizeof(int), st));
+  const int grid = std::min(persistent_grid(k_fwd_persistent, smem), std::max(P.n_ftask, 1));
+  k_fwd_persistent<<<grid, kSolveThreads, smem, st>>>(P.n_ftask, P.ftask.p, F.sn_first.p, F.sn_rows_ptr.p,
+                                                      F.sn_rows.p, F.sn_Lptr.p, Lbase, x, 1, P.ftgt_ptr.p, P.ftgt.p,
+                                                      P.fexpect.p, sync, P.nsn, err);
+  TEMF_CHECK_LAUNCH();
+  const int gridb = std::min(persistent_grid(k_bwd_persistent, smem), std::max(P.n_btask, 1));
+  k_bwd_persistent<<<gridb, kSolveThreads, smem, st>>>(P.n_btask, P.btask.p, F.sn_first.p, F.sn_rows_ptr.p,
+                                                       F.sn_rows.p, F.sn_Lptr.p, Lbase, x, 1, P.btgt_ptr.p, P.btgt.p,
+                                                       P.nchunk.p, P.part_off.p, part, sync, P.nsn, err);
+  TEMF_CHECK_LAUNCH();
+}
+
 int solve_error_flag(temf_ctx& c) {
   int v = 0;
   TEMF_CUDA(cudaMemcpyAsync(&v, c.d_status.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
