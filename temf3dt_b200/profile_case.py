@@ -1,0 +1,45 @@
+"""Run the first N time steps of a benchmark model, for profiler captures.
+
+    python -m temf3dt_b200.profile_case --config 0 --max-steps 150
+
+Builds the same seeded synthetic model as ``bench.py --config K``, assembles
+and analyses it, and runs the FETD time loop for the first ``max-steps``
+steps (the factorisations and trials those steps contain included).  It prints
+the phase timings; it is not a benchmark (no warm-up, not the whole run).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+from . import fetd, synth
+
+CONFIG_KW = {
+    0: ("halfspace", dict(h_core=125, ratio=2.0, h_z=25)),
+    1: ("block", dict()),
+    2: ("multiloop", dict()),
+}
+COMMON = dict(t0=1e-6, sp_division=10, sp_double=100, time_maximum=1e-2)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--config", type=int, default=0, choices=sorted(CONFIG_KW))
+    ap.add_argument("--max-steps", type=int, default=150)
+    a = ap.parse_args()
+    kind, kw = CONFIG_KW[a.config]
+    kw = dict(kw)
+    kw.update(COMMON)
+    m = synth.build_model(kind, seed=a.config, **kw)
+    with fetd.FetdGPU(0) as g:
+        fetd.load_case(g, m.mesh, m.ctl)
+        st = g.stats()
+        out = g.run(m.ctl.sp_division, m.ctl.sp_double, m.ctl.sp_dblesize, m.ctl.time_maximum,
+                    max_steps=a.max_steps)
+        print(json.dumps({"config": a.config, "stats": st, "rows": len(out.steps), "ms_factor": out.ms_factor,
+                          "n_factor": out.n_factor, "ms_steps": out.ms_steps, "n_solve": out.n_solve,
+                          "ms_per_solve": out.ms_steps / max(out.n_solve, 1), "ms_total": out.ms_total}))
+
+
+if __name__ == "__main__":
+    main()
