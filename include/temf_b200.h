@@ -172,6 +172,34 @@ int temf_result_gates(temf_ctx* ctx, int n_gates, const double* gates, double* f
 int temf_result_timing(temf_ctx* ctx, double* ms_factor, double* ms_steps, double* ms_total, int* n_factor,
                        int* n_solve, long long* n_launch);
 
+/* ---- adjoint gradient --------------------------------------------------------
+ * No reference counterpart: the reference's inversion module (inv_modeling)
+ * ships only as compiled objects.  These entries give the gradient of a
+ * misfit of the receiver output with respect to the conductivities.
+ *
+ * temf_adjoint_record: the following temf_run calls record their solve graph
+ * and keep, every checkpoint_every solves and wherever dt changes, a
+ * checkpoint of the BDF2 history (2*sp_dblesize+2 state vectors of n doubles
+ * each).  A recording run launches its kernels one by one (no CUDA graphs),
+ * needs one RHS column and pulse type 1 or 2.  0 turns recording off and
+ * frees the checkpoints.
+ *
+ * temf_adjoint: reverse sweep over the recorded run.  dJ_dfields(9, nrec,
+ * rows) is dJ/d(fields) in the layout temf_result_get returns (the b columns
+ * are chained back onto dB/dt).  tet_cell(n_tets): 1-based inversion cell of
+ * each tet, 0 = not in the grid.  Writes grad_logsigma(ncell) = dJ/dlog sigma_c
+ * = sum over the cell's tets of sigma_t dJ/dsigma_t, and, if grad_sigma is
+ * not NULL, grad_sigma(n_tets) = dJ/dsigma_t.  Uses factor slot 1 (the
+ * factor held there is released).  tet_cell and grad_logsigma may be NULL
+ * together.  Changing the media (temf_set_media) discards the recording. */
+int temf_adjoint_record(temf_ctx* ctx, int checkpoint_every);
+int temf_adjoint(temf_ctx* ctx, const double* dJ_dfields, int ncell, const int* tet_cell, double* grad_logsigma,
+                 double* grad_sigma);
+/* Timing of the last adjoint sweep: ms[0] whole sweep, ms[1] factorisations;
+ * counts[0] solve-graph nodes, counts[1] checkpoint blocks, counts[2]
+ * factorisations, counts[3] kernel launches.  Either pointer may be NULL. */
+int temf_adjoint_timing(temf_ctx* ctx, double* ms, long long* counts);
+
 /* ---- statistics of the symbolic analysis ----------------------------------
  * stats[0..9] = n, nnz(A full), supernodes, levels, nnz(L), stored doubles,
  * factor flops, update tiles, seconds ordering, seconds symbolic. */

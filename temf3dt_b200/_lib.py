@@ -50,6 +50,9 @@ SIGNATURES = {
     "temf_result_timing": (_i, [_p, _dp, _dp, _dp, _ip, _ip, C.POINTER(C.c_longlong)]),
     "temf_analysis_stats": (_i, [_p, _dp]),
     "temf_symbolic_host": (_i, [_i, C.POINTER(C.c_longlong), _ip, _dp, _ip, _dp]),
+    "temf_adjoint_record": (_i, [_p, _i]),
+    "temf_adjoint": (_i, [_p, _dp, _i, _ip, _dp, _dp]),
+    "temf_adjoint_timing": (_i, [_p, _dp, C.POINTER(C.c_longlong)]),
     "temf_pardiso_alloc": (_i, [_p, _i]),
     "temf_pardiso_direct_1": (_i, [_p, _i, _i, _i, _i, _ip, _ip, _dp]),
     "temf_pardiso_direct_2": (_i, [_p, _i, _dp, _dp]),

@@ -17,38 +17,9 @@
 #include <numeric>
 
 #include "assemble.h"
+#include "element.cuh"
 
 namespace temf {
-
-// local edge j joins local vertices IND_TET[j][0] -> IND_TET[j][1] (src/FETD_FWD.f90:23)
-__constant__ int c_ind_tet[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {3, 1}, {2, 3}};
-
-__host__ __device__ inline int packed_upper(int i, int j) {  // i <= j < 6
-  return i * 6 - (i * (i - 1)) / 2 + (j - i);
-}
-
-// Gradients g_k = (b_k, c_k, d_k) and V, written as differences from the first
-// vertex (the cofactor expansion of the reference's 3x3 determinants after
-// subtracting one row from the others; same values up to rounding).
-__device__ inline void tet_gradients(const double X[4][3], double g[4][3], double& vol) {
-  // D(u,w; p,q,r) = det [[1,u_p,w_p],[1,u_q,w_q],[1,u_r,w_r]]
-  auto D = [&](int u, int w, int p, int q, int r) {
-    return (X[q][u] - X[p][u]) * (X[r][w] - X[p][w]) - (X[r][u] - X[p][u]) * (X[q][w] - X[p][w]);
-  };
-  const int rest[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
-  const double sa[4] = {1.0, -1.0, 1.0, -1.0};
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int p = rest[k][0], q = rest[k][1], r = rest[k][2];
-    g[k][0] = -sa[k] * D(1, 2, p, q, r);  // b_k
-    g[k][1] = sa[k] * D(0, 2, p, q, r);   // c_k
-    g[k][2] = -sa[k] * D(0, 1, p, q, r);  // d_k
-  }
-  const double ax = X[1][0] - X[0][0], ay = X[1][1] - X[0][1], az = X[1][2] - X[0][2];
-  const double bx = X[2][0] - X[0][0], by = X[2][1] - X[0][1], bz = X[2][2] - X[0][2];
-  const double cx = X[3][0] - X[0][0], cy = X[3][1] - X[0][1], cz = X[3][2] - X[0][2];
-  vol = (ax * (by * cz - bz * cy) - ay * (bx * cz - bz * cx) + az * (bx * cy - by * cx)) / 6.0;
-}
 
 __global__ void __launch_bounds__(128) k_element_matrices(
     int n_tets, const double* __restrict__ xyz, const int* __restrict__ tet_vex,
@@ -63,43 +34,20 @@ __global__ void __launch_bounds__(128) k_element_matrices(
 #pragma unroll
     for (int a = 0; a < 3; ++a) X[k][a] = xyz[3 * (int64_t)v + a];
   }
-  double g[4][3], vol;
-  tet_gradients(X, g, vol);
-  double len[6], cr[6][3], s[6];
+  double M21[21], K21[21];
+  unit_elements(X, M21, K21);
+  double s[6];
 #pragma unroll
-  for (int j = 0; j < 6; ++j) {
-    const int p = c_ind_tet[j][0], q = c_ind_tet[j][1];
-    const double dx = X[p][0] - X[q][0], dy = X[p][1] - X[q][1], dz = X[p][2] - X[q][2];
-    len[j] = sqrt(dx * dx + dy * dy + dz * dz);
-    cr[j][0] = g[p][1] * g[q][2] - g[q][1] * g[p][2];
-    cr[j][1] = g[q][0] * g[p][2] - g[p][0] * g[q][2];
-    cr[j][2] = g[p][0] * g[q][1] - g[q][0] * g[p][1];
-    s[j] = (double)tet_drc[6 * (int64_t)t + j];
-  }
-  double gram[4][4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-#pragma unroll
-    for (int l = 0; l < 4; ++l) gram[k][l] = g[k][0] * g[l][0] + g[k][1] * g[l][1] + g[k][2] * g[l][2];
+  for (int j = 0; j < 6; ++j) s[j] = (double)tet_drc[6 * (int64_t)t + j];
   const double sv = sig[t], inv_mu = 1.0 / mu[t];
-  const double v6 = 6.0 * vol;
-  const double fM = sv / (720.0 * vol);
-  const double fK = inv_mu * 4.0 * vol / (v6 * v6 * v6 * v6);
 #pragma unroll
   for (int i = 0; i < 6; ++i) {
 #pragma unroll
     for (int j = i; j < 6; ++j) {
-      const int pi = c_ind_tet[i][0], qi = c_ind_tet[i][1];
-      const int pj = c_ind_tet[j][0], qj = c_ind_tet[j][1];
-      // f_kind_iso bracket (src/FETD_FWD.f90:843-844)
-      const double br = gram[qi][qj] * (1.0 + (pi == pj)) - gram[pi][qj] * (1.0 + (qi == pj)) -
-                        gram[qi][pj] * (1.0 + (pi == qj)) + gram[pi][pj] * (1.0 + (qi == qj));
-      const double ll = len[i] * len[j];
-      const double sgn = s[i] * s[j];
-      const double dots = cr[i][0] * cr[j][0] + cr[i][1] * cr[j][1] + cr[i][2] * cr[j][2];
       const int k = packed_upper(i, j);
-      elemM[(int64_t)k * n_tets + t] = sgn * (ll * fM * br);
-      elemK[(int64_t)k * n_tets + t] = sgn * (ll * fK * dots);
+      const double sgn = s[i] * s[j];
+      elemM[(int64_t)k * n_tets + t] = sgn * (sv * M21[k]);
+      elemK[(int64_t)k * n_tets + t] = sgn * (inv_mu * K21[k]);
     }
   }
 }

@@ -6,6 +6,7 @@
 #include <numeric>
 
 #include "../../include/temf_b200.h"
+#include "adjoint.h"
 #include "assemble.h"
 #include "factor.h"
 #include "fetd.h"
@@ -23,6 +24,8 @@ namespace {
 // per-context extras that do not belong in the core context header
 struct CtxExtra {
   temf_run_state run;
+  AdjointResult adj;
+  bool adj_valid = false;
   // PARDISO shim: user upper-CSR position -> CSR position of the permuted full pattern
   std::vector<int> shim_map;  // nnz_user (index into pattern) or -1
   int shim_n = 0, shim_nnz = 0;
@@ -358,6 +361,7 @@ int temf_set_media(temf_ctx* c, const double* sig, const double* mu) {
       if (!(c->sig[t] >= 0.0) || !(c->mu[t] > 0.0)) throw ArgError("sigma must be >= 0 and mu > 0 in every tet");
     c->have_media = true;
     c->assembled = false;
+    c->adj.valid = false;
     c->slots[0].valid = c->slots[1].valid = false;
     upload_media(*c);
     TEMF_CUDA(cudaStreamSynchronize(c->stream));
@@ -665,8 +669,10 @@ int temf_run(temf_ctx* c, int sp_division, int sp_double, int sp_dblesize, doubl
     o.forced = forced;
     o.n_forced = forced ? n_forced : 0;
     o.max_steps = max_steps;
+    o.record_every = c->adj.every;
     CtxExtra& X = extra(c);
     X.run.valid = false;
+    c->adj.valid = false;
     run_fetd(*c, o, X.run.res);
     X.run.valid = true;
     c->slots[0].valid = c->slots[1].valid = false;  // the run reused both slots
@@ -779,6 +785,71 @@ int temf_result_timing(temf_ctx* c, double* ms_factor, double* ms_steps, double*
     if (n_factor) *n_factor = R.n_factor;
     if (n_solve) *n_solve = R.n_solve;
     if (n_launch) *n_launch = (long long)R.launches;
+    return TEMF_OK;
+  });
+}
+
+int temf_adjoint_record(temf_ctx* c, int checkpoint_every) {
+  return guarded(c, [&] {
+    if (checkpoint_every < 0) throw ArgError("checkpoint_every must be >= 0");
+    c->adj.every = checkpoint_every;
+    if (!checkpoint_every) {
+      c->adj.valid = false;
+      c->adj.ck.clear();
+    }
+    return TEMF_OK;
+  });
+}
+
+int temf_adjoint(temf_ctx* c, const double* dJ_dfields, int ncell, const int* tet_cell, double* grad_logsigma,
+                 double* grad_sigma) {
+  return guarded(c, [&] {
+    CtxExtra& X = extra(c);
+    need(X.run.valid && c->adj.valid, "temf_adjoint: no recorded run (temf_adjoint_record, then temf_run)");
+    if (!dJ_dfields) throw ArgError("temf_adjoint: NULL dJ_dfields");
+    if (ncell < 0 || (ncell > 0 && grad_logsigma && !tet_cell)) throw ArgError("temf_adjoint: bad cell map");
+    const RunResult& R = X.run.res;
+    const int rows = (int)R.steps.size(), nrec = c->rec.nrec;
+    // fields -> samples: b_i = sum_{m <= i} dB/dt_m dt_m, with dB/dt reported as 0 on step-0 rows
+    std::vector<double> g((size_t)rows * nrec * 6, 0.0);
+    for (int r = 0; r < nrec; ++r) {
+      double tail[3] = {0.0, 0.0, 0.0};
+      for (int i = rows - 1; i >= 0; --i) {
+        const double* f = dJ_dfields + ((size_t)i * nrec + r) * 9;
+        double* o = g.data() + ((size_t)i * nrec + r) * 6;
+        for (int a = 0; a < 3; ++a) {
+          tail[a] += f[6 + a];
+          o[a] = f[a];
+          o[3 + a] = (R.steps[i] == 0) ? 0.0 : f[3 + a] + tail[a] * R.dts[i];
+        }
+      }
+    }
+    std::vector<int> cell0;
+    if (tet_cell) {
+      cell0.resize(c->n_tets);
+      for (int t = 0; t < c->n_tets; ++t) {
+        if (tet_cell[t] < 0 || tet_cell[t] > ncell) throw ArgError("temf_adjoint: tet_cell out of range");
+        cell0[t] = tet_cell[t] - 1;
+      }
+    }
+    X.adj_valid = false;
+    run_adjoint(*c, g.data(), rows, tet_cell ? cell0.data() : nullptr, ncell, grad_logsigma, grad_sigma, X.adj);
+    X.adj_valid = true;
+    return TEMF_OK;
+  });
+}
+
+int temf_adjoint_timing(temf_ctx* c, double* ms, long long* counts) {
+  return guarded(c, [&] {
+    CtxExtra& X = extra(c);
+    need(X.adj_valid, "no completed adjoint sweep");
+    if (ms) { ms[0] = X.adj.ms_total; ms[1] = X.adj.ms_factor; }
+    if (counts) {
+      counts[0] = X.adj.n_nodes;
+      counts[1] = X.adj.n_blocks;
+      counts[2] = X.adj.n_factor;
+      counts[3] = X.adj.launches;
+    }
     return TEMF_OK;
   });
 }

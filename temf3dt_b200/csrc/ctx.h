@@ -110,6 +110,21 @@ struct Receivers {
   std::vector<double> w_host;  // same, copied back (n_arr/d_arr for checks)
 };
 
+// Record of a forward run for the adjoint: the solve graph (each node:
+// dt, source scalar, the two history nodes it reads), the node each output row
+// reports, and checkpoints of the last W node states taken before the first
+// node of every block (every `every` nodes and wherever dt changes).
+struct AdjointRecord {
+  int every = 0;                 // 0: recording off
+  bool valid = false;
+  int W = 0;                     // history window (states a node may read, counted back)
+  std::vector<double> dt, coef;  // per node k = 1..N at index k-1
+  std::vector<int> a, b;
+  std::vector<int> row_node;
+  std::vector<int> ck_first;     // first node of each block
+  std::vector<std::unique_ptr<DBuf<double>>> ck;  // W states: nodes ck_first-W .. ck_first-1
+};
+
 }  // namespace temf
 
 struct temf_ctx {
@@ -145,5 +160,6 @@ struct temf_ctx {
   // scratch vectors
   temf::DBuf<double> d_u;        // solve update buffer (u_len * nrhs)
   temf::DBuf<double> d_part;     // backward partial sums (part_len * nrhs)
+  temf::AdjointRecord adj;
   int u_nrhs = 0;
 };

@@ -73,6 +73,12 @@ struct Engine {
   // bookkeeping of one pass
   int pass_sign = 1;
   bool pass_output = true;
+  // adjoint recording (eager launches only)
+  bool rec = false;
+  int W = 0;
+  std::vector<int> slot_node, tnode;
+  DBuf<double> recent;  // W most recent node states, node id % W
+  int last_node = 0;
 
   Engine(temf_ctx& c_, const RunOptions& o, RunResult& r) : c(c_), opt(o), res(r) {
     st = c.stream;
@@ -102,7 +108,53 @@ struct Engine {
     k_set_ptr<<<1, 1, 0, st>>>(lptr.p + 0, c.slots[0].L.p);
     k_set_ptr<<<1, 1, 0, st>>>(lptr.p + 1, c.slots[1].L.p);
     TEMF_CHECK_LAUNCH();
+    rec = opt.record_every > 0;
+    if (rec) {
+      if (nrhs != 1) throw ArgError("adjoint recording supports one right-hand side");
+      if (c.src.pulse_type == 3) throw ArgError("adjoint recording covers runs from rest (pulse types 1 and 2)");
+      // a node reads states at most 2*dsz+1 nodes back (the restart after an
+      // accepted trial in the legacy schedule); the window covers that
+      W = 2 * dsz + 2;
+      recent.alloc(vec * W);
+      slot_node.assign(RS, 0);
+      tnode.assign(dsz, 0);
+      AdjointRecord& A = c.adj;
+      A.every = opt.record_every;
+      A.valid = false;
+      A.W = W;
+      A.dt.clear(); A.coef.clear(); A.a.clear(); A.b.clear(); A.row_node.clear();
+      A.ck_first.clear(); A.ck.clear();
+    }
   }
+
+  // --- recording helpers ---------------------------------------------------
+  double* recent_slot(int node) { return recent.p + (size_t)(node % W) * n; }
+  // called before node `k` (= last_node + 1) is computed
+  void maybe_checkpoint(double dt) {
+    AdjointRecord& A = c.adj;
+    const int k = last_node + 1;
+    if (!(k == 1 || (k - 1) % A.every == 0 || dt != A.dt.back())) return;
+    auto buf = std::make_unique<DBuf<double>>();
+    buf->alloc((size_t)W * n);
+    for (int w = 0; w < W; ++w) {
+      const int node = k - W + w;
+      double* dst = buf->p + (size_t)w * n;
+      if (node <= 0) TEMF_CUDA(cudaMemsetAsync(dst, 0, (size_t)n * sizeof(double), st));
+      else TEMF_CUDA(cudaMemcpyAsync(dst, recent_slot(node), (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    A.ck_first.push_back(k);
+    A.ck.push_back(std::move(buf));
+  }
+  // record node (dt, coef, a, b) whose state is now in `x`
+  int record_node(double dt, double cf, int na, int nb, const double* x) {
+    AdjointRecord& A = c.adj;
+    const int k = ++last_node;
+    A.dt.push_back(dt); A.coef.push_back(cf); A.a.push_back(na); A.b.push_back(nb);
+    TEMF_CUDA(cudaMemcpyAsync(recent_slot(k), x, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    return k;
+  }
+  int sn(int k) const { return slot_node[((k % RS) + RS) % RS]; }
+  void set_sn(int k, int node) { slot_node[((k % RS) + RS) % RS] = node; }
   ~Engine() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
     if (coef_h) cudaFreeHost(coef_h);
@@ -190,7 +242,7 @@ struct Engine {
     k_set_int<<<1, 1, 0, st>>>(row_base.p, trace_rows);
     TEMF_CHECK_LAUNCH();
     TEMF_CUDA(cudaEventRecord(ev0, st));
-    if (opt.use_graphs && !any_src) {
+    if (opt.use_graphs && !any_src && !rec) {
       auto it = graphs.find(N);
       if (it == graphs.end()) {
         const int64_t l0 = res.launches;
@@ -218,8 +270,14 @@ struct Engine {
       if (any_src)
         TEMF_CUDA(cudaMemcpyAsync(coef.p, coef_h, N * sizeof(double), cudaMemcpyHostToDevice, st));
       for (int k = 1; k <= N; ++k) {
+        if (rec) maybe_checkpoint(pending[k - 1].dt);
         step(E(k), E(k - 1), E(k + 1), any_src ? coef.p + (k - 1) : nullptr, lptr.p + 2);
         sample(E(k + 1), k - 1);
+        if (rec) {
+          const int id = record_node(pending[k - 1].dt, pending[k - 1].coef, sn(k), sn(k - 1), E(k + 1));
+          set_sn(k + 1, id);
+          c.adj.row_node.push_back(id);
+        }
       }
     }
     TEMF_CUDA(cudaEventRecord(ev1, st));
@@ -261,6 +319,12 @@ struct Engine {
         trace_rows = 0;
         sample(E(1), 0);
         out_row(0, time_cur - step_cur, step_cur);
+        if (rec) {
+          set_sn(1, 0); set_sn(0, 0);
+          last_node = 0;
+          TEMF_CUDA(cudaMemsetAsync(recent.p, 0, recent.bytes(), st));
+          c.adj.row_node.push_back(0);
+        }
         trace_rows = 1;
         cur = 0;
         factor(0, step_cur);
@@ -281,8 +345,15 @@ struct Engine {
           tt += step_cur;
         }
         TEMF_CUDA(cudaMemcpyAsync(coef.p, coef_h, dsz * sizeof(double), cudaMemcpyHostToDevice, st));
+        int a2n = rec ? sn(last) : 0, a3n = rec ? sn(prev) : 0;
         for (int i = 0; i < dsz; ++i) {
+          if (rec) maybe_checkpoint(step_cur);
           step_fn(a2, a3, T(i), coef_h[i] != 0.0 ? coef.p + i : nullptr, lptr.p + 2);
+          if (rec) {
+            tnode[i] = record_node(step_cur, coef_h[i], a2n, a3n, T(i));
+            a3n = a2n;
+            a2n = tnode[i];
+          }
           a3 = a2;
           a2 = T(i);
         }
@@ -325,6 +396,12 @@ struct Engine {
         if (reject) {
           sample(T(0), 0);
           out_row(step, time_cur, step_cur);
+          if (rec) {
+            c.adj.row_node.push_back(tnode[0]);
+            const int n0 = sn(last);
+            set_sn(0, n0);
+            set_sn(1, tnode[0]);
+          }
           copy_vec(E(0), E(last));
           copy_vec(E(1), T(0));
           e1 = E(1);
@@ -333,6 +410,12 @@ struct Engine {
           sample(T(dsz - 1), 0);
           // e3 = all_e(idx) (src/FETD_FWD.f90:1405); the build that wrote the
           // shipped LINUX/*.field files restarted from all_e(idx - sp_dblesize)
+          if (rec) {
+            c.adj.row_node.push_back(tnode[dsz - 1]);
+            const int n0 = opt.legacy_linux ? sn(last - dsz) : sn(last);
+            set_sn(0, n0);
+            set_sn(1, tnode[dsz - 1]);
+          }
           copy_vec(E(0), opt.legacy_linux ? E(last - dsz) : E(last));
           copy_vec(E(1), T(dsz - 1));
           e1 = E(0);
@@ -392,6 +475,7 @@ struct Engine {
     float ms = 0;
     TEMF_CUDA(cudaEventElapsedTime(&ms, a, b));
     res.ms_total = ms;
+    if (rec) c.adj.valid = true;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
   }

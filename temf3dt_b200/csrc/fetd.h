@@ -18,6 +18,7 @@ struct RunOptions {
   const int* forced = nullptr;  // per trial: 1 accept, 0 reject, <0 own decision (test hook)
   int n_forced = 0;
   int max_steps = 0;            // 0: run to time_maximum
+  int record_every = 0;         // >0: record the solve graph + checkpoints for the adjoint
 };
 
 struct RunResult {

@@ -243,6 +243,33 @@ class FetdGPU:
         self._ck(self._L.temf_result_gates(self._h, len(g), dptr(g), dptr(out), iptr(done)), "temf_result_gates")
         return out.reshape(len(g), max(self.nrec, 1), 9), done.astype(bool)
 
+    # -- adjoint gradient ---------------------------------------------------------------
+    def adjoint_record(self, checkpoint_every: int = 50) -> None:
+        """Record the next runs' solve graph for :meth:`adjoint` (0 = off)."""
+        self._ck(self._L.temf_adjoint_record(self._h, int(checkpoint_every)), "temf_adjoint_record")
+
+    def adjoint(self, dJ_dfields: np.ndarray, tet_cell: Optional[np.ndarray] = None, ncell: int = 0):
+        """Gradient of a misfit J of the last recorded run's output.
+
+        dJ_dfields: (rows, nrec, 9) = dJ/d(fields of :meth:`run`).  tet_cell:
+        0-based inversion cell per tet, -1 outside (None: no cells).  Returns
+        (dJ/dlog sigma per cell, dJ/dsigma per tet, timing dict).
+        """
+        g = as_f64(np.asarray(dJ_dfields, dtype=np.float64).reshape(-1))
+        grad_t = np.zeros(self.n_tets)
+        grad_c = np.zeros(max(int(ncell), 1))
+        cell = None
+        if tet_cell is not None:
+            cell = as_i32(np.asarray(tet_cell, dtype=np.int64) + 1)
+        self._ck(self._L.temf_adjoint(self._h, dptr(g), int(ncell), iptr(cell) if cell is not None else None,
+                                      dptr(grad_c) if cell is not None else None, dptr(grad_t)), "temf_adjoint")
+        ms = np.zeros(2)
+        cnt = (C.c_longlong * 4)()
+        self._ck(self._L.temf_adjoint_timing(self._h, dptr(ms), cnt), "temf_adjoint_timing")
+        timing = dict(ms_total=float(ms[0]), ms_factor=float(ms[1]), nodes=int(cnt[0]), blocks=int(cnt[1]),
+                      factors=int(cnt[2]), launches=int(cnt[3]))
+        return grad_c[:int(ncell)], grad_t, timing
+
     # -- PARDISO-compatible shim ------------------------------------------------------
     def pardiso_alloc(self, max_matrix: int) -> None:
         self._ck(self._L.temf_pardiso_alloc(self._h, max_matrix), "temf_pardiso_alloc")

@@ -120,3 +120,26 @@ def tiny_synth(**kw):
                 sp_division=4, time_maximum=2e-5)
     args.update(kw)
     return synth.build_model("halfspace", **args)
+
+
+def cell_grid_2x2x2(om) -> "np.ndarray":
+    """Inversion cells for the adjoint tests: a 2 x 2 x 2 grid of 400 x 400 x
+    150 m cells under the loop; 0-based cell per tet, -1 outside."""
+    X = om.nod_cor[om.tet_vex - 1].mean(axis=1)
+    cell = -np.ones(len(X), dtype=np.int64)
+    ins = (np.abs(X[:, 0]) < 400) & (np.abs(X[:, 1]) < 400) & (X[:, 2] > 0) & (X[:, 2] < 300)
+    ix = ((X[:, 0] + 400) // 400).astype(int)
+    iy = ((X[:, 1] + 400) // 400).astype(int)
+    iz = (X[:, 2] // 150).astype(int)
+    cell[ins] = (ix * 4 + iy * 2 + iz)[ins]
+    return cell
+
+
+def adjoint_misfit_case(rows, seed: int = 0):
+    """Observed data = the run's own output with 5 % multiplicative noise, and
+    weights 1/max|.|^2 on the dB/dt and b columns (9 output columns)."""
+    rng = np.random.default_rng(seed)
+    d_obs = rows * (1 + 0.05 * rng.standard_normal(rows.shape))
+    mask = np.zeros_like(d_obs)
+    mask[:, :, 3:9] = 1.0 / np.maximum(np.abs(rows[:, :, 3:9]).max(axis=0), 1e-300) ** 2
+    return d_obs, mask
