@@ -10,6 +10,10 @@ air 1e-12 S/m, 1000 m square loop, 64 receivers on a 20 m line, ~1.2M edges),
 synthetic and seeded.  Its factors (GBs) exceed the 126 MB L2 many times over,
 so no L2 flush is needed between steps.
 
+adjoint: one gradient of a dB/dt misfit with respect to log sigma on a
+32 x 32 x 16 inversion grid (recorded forward run + reverse sweep), reported
+beside the metric with its ratio to one forward run.
+
 e2e: the same metric through the public API with host buffers: per step the
 conductivity/permeability per tet and the source/receiver arrays are copied
 host->device, the matrices re-assembled, the loop run and the receiver
@@ -129,6 +133,43 @@ def cpu_sample(cfg: int, max_steps: int):
     return steps * nrhs / dt, dict(n_edges=om.n, steps=steps, seconds=dt)
 
 
+def inversion_cells(m, shape=(32, 32, 16), box=((-640.0, 640.0), (-640.0, 640.0), (0.0, 400.0))):
+    """Tet -> cell map of a regular inversion grid under the loop (0-based, -1
+    outside): 32 x 32 x 16 cells of 40 x 40 x 25 m by default."""
+    X = m.mesh.nod_cor[m.mesh.tet_vex - 1].mean(axis=1)
+    idx = []
+    inside = np.ones(len(X), dtype=bool)
+    for a in range(3):
+        lo, hi = box[a]
+        k = np.floor((X[:, a] - lo) / (hi - lo) * shape[a]).astype(np.int64)
+        inside &= (k >= 0) & (k < shape[a])
+        idx.append(np.clip(k, 0, shape[a] - 1))
+    cell = (idx[0] * shape[1] + idx[1]) * shape[2] + idx[2]
+    return np.where(inside, cell, -1), int(np.prod(shape))
+
+
+def adjoint_measure(g, m, one_run, forward_ms):
+    """Gradient of J = 1/2 sum (d - d_obs)^2 over the receivers' dB/dt with
+    respect to log sigma of a 32 x 32 x 16 grid: a recorded forward run
+    (eager launches, checkpoints every 50 solves) and the reverse sweep, both
+    timed with CUDA events inside the library."""
+    cell, ncell = inversion_cells(m)
+    g.adjoint_record(50)
+    o = one_run()
+    rng = np.random.default_rng(7)
+    d_obs = o.fields * (1 + 0.05 * rng.standard_normal(o.fields.shape))
+    mask = np.zeros_like(d_obs)
+    mask[:, :, 3:6] = 1.0
+    dJ = mask * (o.fields - d_obs)
+    grad, _, tm = g.adjoint(dJ, cell, ncell)
+    g.adjoint_record(0)
+    return {"ms": tm["ms_total"], "recorded_forward_ms": o.ms_total, "forward_ms": forward_ms,
+            "ratio_to_forward": tm["ms_total"] / forward_ms, "factor_ms": tm["ms_factor"], "nodes": tm["nodes"],
+            "blocks": tm["blocks"], "factorisations": tm["factors"], "launches": tm["launches"],
+            "checkpoint_every": 50, "cells": ncell, "cells_in_mesh": int(len(np.unique(cell[cell >= 0]))),
+            "grad_finite": bool(np.isfinite(grad).all())}
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -189,6 +230,16 @@ def ours(args):
     t_setup = time.perf_counter() - t_setup
     st = g.stats()
     c = m.ctl
+    plain = None
+    if cfg == 2:
+        # the plain single-RHS path on the same mesh (first loop, its receiver)
+        g2 = fetd.FetdGPU(local)
+        fetd.load_case(g2, m.mesh, m.ctl)
+        g2.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum)
+        o2 = g2.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum)
+        plain = {"value": (len(o2.steps) - 1) / (o2.ms_total / 1e3), "unit": "steps*RHS/s", "rhs": 1,
+                 "ms_per_run": o2.ms_total, "solve_ms_per_step": o2.ms_steps / max(o2.n_solve, 1)}
+        g2.close()
 
     def one_run():
         return g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum)
@@ -230,6 +281,10 @@ def ours(args):
         e2e_times.append(time.perf_counter() - t0)
     e2e_steps = len(o.steps) - 1
     e2e_val = e2e_steps * ncols * world / float(np.mean(e2e_times))
+    # --- adjoint gradient (single-RHS workloads): one recorded run + one reverse sweep ---
+    adj = None
+    if cfg != 2 and args.adjoint:
+        adj = adjoint_measure(g, m, one_run, outs[-1].ms_total)
     # --- roofline of the dominant phase ---
     o = outs[-1]
     ms_fac = o.ms_factor / max(o.n_factor, 1)
@@ -279,6 +334,9 @@ def ours(args):
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": int(sum(x.n_launch for x in outs)),
+        "plain_same_mesh": plain,
+        "batched_over_plain": (value / world / plain["value"]) if plain else None,
+        "adjoint": adj,
         "phases_ms_per_run": {"factor": o.ms_factor, "steps": o.ms_steps, "total": o.ms_total,
                               "factor_each": ms_fac, "solve_step_each": ms_step, "setup_s": t_setup},
     }
@@ -299,6 +357,7 @@ def main():
     ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2])
     ap.add_argument("--sample-steps", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--adjoint", type=int, default=1, help="1: also time one adjoint gradient (single-RHS configs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

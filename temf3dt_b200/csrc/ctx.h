@@ -62,10 +62,7 @@ struct SolveTask {
 };
 
 struct SolvePlan {
-  DBuf<int64_t> uoff;          // nsn+1: offsets of the per-supernode update vectors
-  DBuf<int64_t> in_ptr;        // n+1: incoming update entries per column
-  DBuf<int64_t> in_idx;        // positions in the update buffer
-  int64_t u_len = 0;
+  int64_t u_len = 0;           // sum over supernodes of the rows below the diagonal block
   // persistent schedules (tasks in an order where every wait targets an earlier task)
   DBuf<SolveTask> ftask, btask;
   int n_ftask = 0, n_btask = 0;
@@ -75,6 +72,12 @@ struct SolvePlan {
   DBuf<int> nchunk;            // per supernode: row chunks of its panel
   DBuf<int64_t> part_off;      // per supernode: offset of its backward partial sums
   int64_t part_len = 0;
+  // the same schedules with 64-row chunks for blocks of up to 64 right-hand sides
+  DBuf<SolveTask> mftask, mbtask;
+  int n_mftask = 0, n_mbtask = 0;
+  DBuf<int> mftgt_ptr, mftgt, mfexpect, mbtgt_ptr, mbtgt, mnchunk;
+  DBuf<int64_t> mpart_off;
+  int64_t mpart_len = 0;
   DBuf<int> sync;              // ready | ydone | cdone | xdone (nsn each) | counters
   int nsn = 0;
 };
@@ -158,8 +161,7 @@ struct temf_ctx {
   temf::Source src;
   temf::Receivers rec;
   // scratch vectors
-  temf::DBuf<double> d_u;        // solve update buffer (u_len * nrhs)
-  temf::DBuf<double> d_part;     // backward partial sums (part_len * nrhs)
+  temf::DBuf<double> d_part;     // backward partial sums (part_len, or mpart_len * 64 for blocks)
   temf::AdjointRecord adj;
   int u_nrhs = 0;
 };

@@ -188,7 +188,7 @@ struct Engine {
     return ms;
   }
 
-  int64_t solve_launches() const { return 2; }  // persistent forward + backward kernels
+  int64_t solve_launches() const { return solve_launch_count(nrhs); }  // persistent forward + backward kernels
 
   // one BDF2 step: out = A^{-1} (M (4 e2 - e3) - coef * s)
   void step(const double* e2, const double* e3, double* out, const double* coefp, double* const* Lb) {

@@ -27,6 +27,8 @@ namespace temf {
 
 constexpr int kSolveThreads = 128;
 constexpr int kChunkRows = 128;        // rows of a panel handled by one task (= threads per CTA)
+constexpr int kChunkRowsMulti = 64;    // rows per task when solving blocks of right-hand sides
+constexpr int kMultiCols = 64;         // right-hand sides per block
 constexpr int kSpinLimit = 1 << 22;    // bounded waits: ~seconds, then the error flag
 
 // Bounded wait until *flag >= target (written by other CTAs of the same
@@ -369,6 +371,247 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_persistent(
 }
 
 // ---------------------------------------------------------------------------
+// Blocks of up to 64 right-hand sides (many sources on one mesh): the same
+// persistent task graph with 64-row chunks; the chunk products are 64 x 64 x c
+// FP64 tensor-core (DMMA) tiles staged in shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kLdm = 72;  // padded leading dimension of the 64-wide shared tiles
+
+__device__ __forceinline__ void dmma8(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+struct MultiSmem {
+  double D[kSnCols][kSnCols + 1];
+  double rinv[kSnCols];
+  double A[kSnCols * kLdm];  // panel block, [j][i] (column j of L21, rows of the chunk)
+  double Y[kSnCols * kLdm];  // right-hand-side block, [row][col]
+};
+
+// C[m][n] += sum_k A(m,k) B(k,n) for a 64 x 64 tile; warps 2x2 of 32x32.
+// A(m,k) = Am[m * sam + k * sak], B(k,n) = Bk[k * kLdm + n].
+__device__ __forceinline__ void mma_tile64(double acc[4][4][2], const double* Am, int sam, int sak,
+                                           const double* Bk, int kdim) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  const int g = lane >> 2, q = lane & 3;
+  for (int k0 = 0; k0 < kdim; k0 += 4) {
+    double fa[4], fb[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) fa[a] = Am[(wr + a * 8 + g) * sam + (k0 + q) * sak];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) fb[b] = Bk[(k0 + q) * kLdm + wc + b * 8 + g];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) dmma8(acc[a][b][0], acc[a][b][1], fa[a], fb[b]);
+  }
+}
+
+// store the accumulators of mma_tile64 to a [m][n] tile with leading dimension kLdm
+__device__ __forceinline__ void store_tile64(const double acc[4][4][2], double* C) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
+  const int g = lane >> 2, q = lane & 3;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) C[(wr + a * 8 + g) * kLdm + wc + b * 8 + 2 * q + e] = acc[a][b][e];
+}
+
+__device__ __forceinline__ void zero_acc(double acc[4][4][2]) {
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+}
+
+// panel rows [r0, r0+nr) x columns [0, c) of L21 into A[j][i] (zero padded to 64 x 64)
+__device__ __forceinline__ void load_panel_block(double* A, const double* P, int c, int64_t ld, int r0, int nr) {
+  for (int idx = threadIdx.x; idx < kSnCols * kSnCols; idx += blockDim.x) {
+    const int j = idx / kSnCols, i = idx % kSnCols;
+    A[j * kLdm + i] = (j < c && i < nr) ? __ldg(P + (int64_t)j * ld + c + r0 + i) : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(kSolveThreads) k_fwd_multi(
+    int ntask, const SolveTask* __restrict__ tasks, const int* __restrict__ sn_first,
+    const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows, const int64_t* __restrict__ Lptr,
+    double* const* Lbase, double* x, int ldx, int k, const int* __restrict__ tgt_ptr, const int* __restrict__ tgt,
+    const int* __restrict__ expect, int* sync, int nsn, int* err) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  MultiSmem& M = *reinterpret_cast<MultiSmem*>(smraw);
+  __shared__ int task_id;
+  int* ready = sync;
+  int* ydone = sync + nsn;
+  int* counter = sync + 4 * nsn;
+  const int tid = threadIdx.x;
+  const double* Lb = *Lbase;
+  for (;;) {
+    if (tid == 0) task_id = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = task_id;
+    __syncthreads();
+    if (t >= ntask) break;
+    const SolveTask T = tasks[t];
+    const int s = T.s;
+    const int f = sn_first[s];
+    const int c = sn_first[s + 1] - f;
+    const int64_t rp = rows_ptr[s];
+    const int64_t r = rows_ptr[s + 1] - rp;
+    const int64_t ld = c + r;
+    const double* P = Lb + Lptr[s];
+    const int nr = T.r1 - T.r0;
+    if (nr > 0) load_panel_block(M.A, P, c, ld, T.r0, nr);  // independent of the waits
+    if (T.kind == 0) {
+      load_diag(M.D, M.rinv, P, c, ld);
+      if (tid == 0) wait_geq(ready + s, expect[s], err, 1);
+    } else {
+      if (tid == 0) wait_geq(ydone + s, 1, err, 2);
+    }
+    __syncthreads();
+    for (int idx = tid; idx < kSnCols * kSnCols; idx += blockDim.x) {
+      const int j = idx / kSnCols, col = idx % kSnCols;
+      M.Y[j * kLdm + col] = (j < c && col < k) ? __ldcg(x + (int64_t)(f + j) * ldx + col) : 0.0;
+    }
+    __syncthreads();
+    if (T.kind == 0) {
+      // Y_s = L11^{-1} B_s, one thread per right-hand side
+      if (tid < k) {
+        for (int j = 0; j < c; ++j) {
+          const double v = M.Y[j * kLdm + tid] * M.rinv[j];
+          M.Y[j * kLdm + tid] = v;
+          for (int i = j + 1; i < c; ++i) M.Y[i * kLdm + tid] -= M.D[i][j] * v;
+        }
+      }
+      __syncthreads();
+      for (int idx = tid; idx < c * k; idx += blockDim.x) {
+        const int j = idx / k, col = idx % k;
+        x[(int64_t)(f + j) * ldx + col] = M.Y[j * kLdm + col];
+      }
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) atomicExch(ydone + s, 1);
+    }
+    if (nr > 0) {
+      // U = L21[rows] Y_s (64 x 64 x c), then push -U into the rows' right-hand sides
+      double acc[4][4][2];
+      zero_acc(acc);
+      mma_tile64(acc, M.A, 1, kLdm, M.Y, (c + 3) & ~3);
+      __syncthreads();
+      store_tile64(acc, M.A);  // reuse A as [row][col]
+      __syncthreads();
+      const int warp = tid >> 5, lane = tid & 31;
+      for (int i = warp; i < nr; i += kSolveThreads / 32) {
+        double* dst = x + (int64_t)sn_rows[rp + T.r0 + i] * ldx;
+        for (int col = lane; col < k; col += 32) atomicAdd(dst + col, -M.A[i * kLdm + col]);
+      }
+      __threadfence();
+      __syncthreads();
+      if (tid == 0)
+        for (int q = tgt_ptr[t]; q < tgt_ptr[t + 1]; ++q) atomicAdd(ready + tgt[q], 1);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(
+    int ntask, const SolveTask* __restrict__ tasks, const int* __restrict__ sn_first,
+    const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows, const int64_t* __restrict__ Lptr,
+    double* const* Lbase, double* x, int ldx, int k, const int* __restrict__ own_ptr, const int* __restrict__ own,
+    const int* __restrict__ nchunk, const int64_t* __restrict__ part_off, double* part, int* sync, int nsn,
+    int* err) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  MultiSmem& M = *reinterpret_cast<MultiSmem*>(smraw);
+  __shared__ int task_id;
+  int* cdone = sync + 2 * nsn;
+  int* xdone = sync + 3 * nsn;
+  int* counter = sync + 4 * nsn + 1;
+  const int tid = threadIdx.x;
+  const double* Lb = *Lbase;
+  for (;;) {
+    if (tid == 0) task_id = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = task_id;
+    __syncthreads();
+    if (t >= ntask) break;
+    const SolveTask T = tasks[t];
+    const int s = T.s;
+    const int f = sn_first[s];
+    const int c = sn_first[s + 1] - f;
+    const int64_t rp = rows_ptr[s];
+    const int64_t r = rows_ptr[s + 1] - rp;
+    const int64_t ld = c + r;
+    const double* P = Lb + Lptr[s];
+    const int nr = T.r1 - T.r0;
+    if (nr > 0) load_panel_block(M.A, P, c, ld, T.r0, nr);
+    if (T.kind == 0) load_diag(M.D, M.rinv, P, c, ld);
+    if (tid == 0) {
+      for (int q = own_ptr[t]; q < own_ptr[t + 1]; ++q) wait_geq(xdone + own[q], 1, err, 3);
+      if (T.kind == 0) wait_geq(cdone + s, nchunk[s] - (nr > 0 ? 1 : 0), err, 4);
+    }
+    __syncthreads();
+    double acc[4][4][2];
+    zero_acc(acc);
+    if (nr > 0) {
+      // Xr = x[rows] (64 x k), then C = L21[rows]^T Xr (c x k)
+      for (int idx = tid; idx < kSnCols * kSnCols; idx += blockDim.x) {
+        const int i = idx / kSnCols, col = idx % kSnCols;
+        M.Y[i * kLdm + col] = (i < nr && col < k) ? __ldcg(x + (int64_t)sn_rows[rp + T.r0 + i] * ldx + col) : 0.0;
+      }
+      __syncthreads();
+      mma_tile64(acc, M.A, kLdm, 1, M.Y, 64);
+      __syncthreads();
+    }
+    if (T.kind == 1) {
+      const int chunk = T.r0 / kChunkRowsMulti;
+      double* pp = part + (part_off[s] + (int64_t)chunk * c) * kMultiCols;
+      store_tile64(acc, M.Y);
+      __syncthreads();
+      for (int idx = tid; idx < c * kMultiCols; idx += blockDim.x) {
+        const int j = idx / kMultiCols, col = idx % kMultiCols;
+        pp[idx] = M.Y[j * kLdm + col];
+      }
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) atomicAdd(cdone + s, 1);
+    } else {
+      // Z = Y_s - (first chunk, here) - (other chunks, in order); back-substitute
+      store_tile64(acc, M.A);  // first-chunk products as [j][col]
+      __syncthreads();
+      const int nch = nchunk[s];
+      const double* pp = part + part_off[s] * kMultiCols;
+      for (int idx = tid; idx < c * k; idx += blockDim.x) {
+        const int j = idx / k, col = idx % k;
+        double v = __ldcg(x + (int64_t)(f + j) * ldx + col);
+        if (nr > 0) v -= M.A[j * kLdm + col];
+        for (int q = 1; q < nch; ++q) v -= __ldcg(pp + ((int64_t)q * c + j) * kMultiCols + col);
+        M.Y[j * kLdm + col] = v;
+      }
+      __syncthreads();
+      if (tid < k) {
+        for (int j = c - 1; j >= 0; --j) {
+          const double v = M.Y[j * kLdm + tid] * M.rinv[j];
+          M.Y[j * kLdm + tid] = v;
+          for (int i = 0; i < j; ++i) M.Y[i * kLdm + tid] -= M.D[j][i] * v;
+        }
+      }
+      __syncthreads();
+      for (int idx = tid; idx < c * k; idx += blockDim.x) {
+        const int j = idx / k, col = idx % k;
+        x[(int64_t)(f + j) * ldx + col] = M.Y[j * kLdm + col];
+      }
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) atomicExch(xdone + s, 1);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // SpMV-type kernels
 // ---------------------------------------------------------------------------
 // y = M (4 e2 - e3), eight lanes per row
@@ -481,43 +724,35 @@ __global__ void k_err_final(int nblocks, int nrhs, const double* __restrict__ pa
 // ---------------------------------------------------------------------------
 // host
 // ---------------------------------------------------------------------------
-void build_solve_plan(temf_ctx& c) {
-  const Symbolic& S = c.sym;
-  SolvePlan& P = c.splan;
-  const int n = S.n, nsn = S.nsn;
-  P.nsn = nsn;
-  std::vector<int64_t> uoff(nsn + 1, 0);
-  for (int s = 0; s < nsn; ++s) uoff[s + 1] = uoff[s] + (S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]);
-  P.u_len = uoff[nsn];
-  std::vector<int64_t> in_ptr(n + 1, 0);
-  for (size_t q = 0; q < S.sn_rows.size(); ++q) in_ptr[S.sn_rows[q] + 1]++;
-  for (int i = 0; i < n; ++i) in_ptr[i + 1] += in_ptr[i];
-  std::vector<int64_t> in_idx(S.sn_rows.size());
-  std::vector<int64_t> fill(in_ptr.begin(), in_ptr.end() - 1);
-  for (int s = 0; s < nsn; ++s)
-    for (int64_t q = S.sn_rows_ptr[s]; q < S.sn_rows_ptr[s + 1]; ++q)
-      in_idx[fill[S.sn_rows[q]]++] = uoff[s] + (q - S.sn_rows_ptr[s]);
-  P.uoff.upload(uoff.data(), uoff.size(), c.stream);
-  P.in_ptr.upload(in_ptr.data(), in_ptr.size(), c.stream);
-  P.in_idx.upload(in_idx.data(), in_idx.size(), c.stream);
+namespace {
+// Task lists of the persistent sweeps for a given chunk height (see the
+// kernels): per task its owner/target supernodes, per supernode the forward
+// chunk count it waits for, its row-chunk count and partial-sum offset.
+struct Sched {
+  std::vector<SolveTask> ft, bt;
+  std::vector<int> ftp{0}, ftg, btp{0}, btg, expect, nch;
+  std::vector<int64_t> poff;
+};
 
+void build_sched(const Symbolic& S, int CH, Sched& o) {
+  const int nsn = S.nsn;
   // distinct owner supernodes of rows [r0, r1) of s (rows ascending -> owners ascending)
-  auto owners = [&](int s, int r0, int r1, std::vector<int>& out) {
-    out.clear();
+  std::vector<int> tmp;
+  auto owners = [&](int s, int r0, int r1) {
+    tmp.clear();
     const int* rows = S.sn_rows.data() + S.sn_rows_ptr[s];
     for (int i = r0; i < r1; ++i) {
-      const int o = S.col2sn[rows[i]];
-      if (out.empty() || out.back() != o) out.push_back(o);
+      const int ow = S.col2sn[rows[i]];
+      if (tmp.empty() || tmp.back() != ow) tmp.push_back(ow);
     }
   };
-  std::vector<SolveTask> ft, bt;
-  std::vector<int> ftp(1, 0), ftg, btp(1, 0), btg, expect(nsn, 0), nch(nsn, 0);
-  std::vector<int64_t> poff(nsn + 1, 0);
-  std::vector<int> tmp;
+  o.expect.assign(nsn, 0);
+  o.nch.assign(nsn, 0);
+  o.poff.assign(nsn + 1, 0);
   for (int s = 0; s < nsn; ++s) {
     const int r = (int)(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]);
-    nch[s] = ceil_div(r, kChunkRows);
-    poff[s + 1] = poff[s] + (int64_t)nch[s] * (S.sn_first[s + 1] - S.sn_first[s]);
+    o.nch[s] = ceil_div(r, CH);
+    o.poff[s + 1] = o.poff[s] + (int64_t)o.nch[s] * (S.sn_first[s + 1] - S.sn_first[s]);
   }
   // forward: bottom-up levels; per supernode its diagonal task (with the first
   // row chunk), then the other chunks
@@ -525,12 +760,12 @@ void build_solve_plan(temf_ctx& c) {
     for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
       const int s = S.level_sn[q];
       const int r = (int)(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]);
-      for (int r0 = 0; r0 < std::max(r, 1); r0 += kChunkRows) {
-        const int r1 = std::min(r, r0 + kChunkRows);
-        ft.push_back({s, r0 == 0 ? 0 : 1, r0, r1});
-        owners(s, r0, r1, tmp);
-        for (int o : tmp) { ftg.push_back(o); expect[o]++; }
-        ftp.push_back((int)ftg.size());
+      for (int r0 = 0; r0 < std::max(r, 1); r0 += CH) {
+        const int r1 = std::min(r, r0 + CH);
+        o.ft.push_back({s, r0 == 0 ? 0 : 1, r0, r1});
+        owners(s, r0, r1);
+        for (int ow : tmp) { o.ftg.push_back(ow); o.expect[ow]++; }
+        o.ftp.push_back((int)o.ftg.size());
       }
     }
   // backward: top-down levels; per supernode its other chunks, then the
@@ -539,40 +774,67 @@ void build_solve_plan(temf_ctx& c) {
     for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
       const int s = S.level_sn[q];
       const int r = (int)(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]);
-      for (int r0 = kChunkRows; r0 < r; r0 += kChunkRows) {
-        const int r1 = std::min(r, r0 + kChunkRows);
-        bt.push_back({s, 1, r0, r1});
-        owners(s, r0, r1, tmp);
-        btg.insert(btg.end(), tmp.begin(), tmp.end());
-        btp.push_back((int)btg.size());
+      for (int r0 = CH; r0 < r; r0 += CH) {
+        const int r1 = std::min(r, r0 + CH);
+        o.bt.push_back({s, 1, r0, r1});
+        owners(s, r0, r1);
+        o.btg.insert(o.btg.end(), tmp.begin(), tmp.end());
+        o.btp.push_back((int)o.btg.size());
       }
-      const int r1 = std::min(r, kChunkRows);
-      bt.push_back({s, 0, 0, r1});
-      owners(s, 0, r1, tmp);
-      btg.insert(btg.end(), tmp.begin(), tmp.end());
-      btp.push_back((int)btg.size());
+      const int r1 = std::min(r, CH);
+      o.bt.push_back({s, 0, 0, r1});
+      owners(s, 0, r1);
+      o.btg.insert(o.btg.end(), tmp.begin(), tmp.end());
+      o.btp.push_back((int)o.btg.size());
     }
-  P.n_ftask = (int)ft.size();
-  P.n_btask = (int)bt.size();
-  P.ftask.upload(ft.data(), ft.size(), c.stream);
-  P.btask.upload(bt.data(), bt.size(), c.stream);
-  P.ftgt_ptr.upload(ftp.data(), ftp.size(), c.stream);
-  P.ftgt.upload(ftg.data(), std::max<size_t>(ftg.size(), 1), c.stream);
-  P.fexpect.upload(expect.data(), expect.size(), c.stream);
-  P.btgt_ptr.upload(btp.data(), btp.size(), c.stream);
-  P.btgt.upload(btg.data(), std::max<size_t>(btg.size(), 1), c.stream);
-  P.nchunk.upload(nch.data(), nch.size(), c.stream);
-  P.part_len = poff[nsn];
-  P.part_off.upload(poff.data(), poff.size(), c.stream);
+}
+}  // namespace
+
+void build_solve_plan(temf_ctx& c) {
+  const Symbolic& S = c.sym;
+  SolvePlan& P = c.splan;
+  const int nsn = S.nsn;
+  P.nsn = nsn;
+  P.u_len = (int64_t)S.sn_rows.size();
+  cudaStream_t st = c.stream;
+  Sched a;
+  build_sched(S, kChunkRows, a);
+  P.n_ftask = (int)a.ft.size();
+  P.n_btask = (int)a.bt.size();
+  P.ftask.upload(a.ft.data(), a.ft.size(), st);
+  P.btask.upload(a.bt.data(), a.bt.size(), st);
+  P.ftgt_ptr.upload(a.ftp.data(), a.ftp.size(), st);
+  P.ftgt.upload(a.ftg.data(), std::max<size_t>(a.ftg.size(), 1), st);
+  P.fexpect.upload(a.expect.data(), a.expect.size(), st);
+  P.btgt_ptr.upload(a.btp.data(), a.btp.size(), st);
+  P.btgt.upload(a.btg.data(), std::max<size_t>(a.btg.size(), 1), st);
+  P.nchunk.upload(a.nch.data(), a.nch.size(), st);
+  P.part_len = a.poff[nsn];
+  P.part_off.upload(a.poff.data(), a.poff.size(), st);
+  TEMF_CUDA(cudaStreamSynchronize(st));  // the host vectors of `a` go out of scope
+  Sched b;
+  build_sched(S, kChunkRowsMulti, b);
+  P.n_mftask = (int)b.ft.size();
+  P.n_mbtask = (int)b.bt.size();
+  P.mftask.upload(b.ft.data(), b.ft.size(), st);
+  P.mbtask.upload(b.bt.data(), b.bt.size(), st);
+  P.mftgt_ptr.upload(b.ftp.data(), b.ftp.size(), st);
+  P.mftgt.upload(b.ftg.data(), std::max<size_t>(b.ftg.size(), 1), st);
+  P.mfexpect.upload(b.expect.data(), b.expect.size(), st);
+  P.mbtgt_ptr.upload(b.btp.data(), b.btp.size(), st);
+  P.mbtgt.upload(b.btg.data(), std::max<size_t>(b.btg.size(), 1), st);
+  P.mnchunk.upload(b.nch.data(), b.nch.size(), st);
+  P.mpart_len = b.poff[nsn];
+  P.mpart_off.upload(b.poff.data(), b.poff.size(), st);
   P.sync.alloc(4 * (size_t)nsn + 4);
-  TEMF_CUDA(cudaStreamSynchronize(c.stream));
+  TEMF_CUDA(cudaStreamSynchronize(st));
 }
 
 void ensure_update_buffer(temf_ctx& c, int nrhs) {
-  const size_t need = (size_t)std::max<int64_t>(c.splan.u_len, 1) * nrhs;
-  if (c.d_u.n < need) c.d_u.alloc(need);
-  const size_t needp = (size_t)std::max<int64_t>(c.splan.part_len, 1) * nrhs;
-  if (c.d_part.n < needp) c.d_part.alloc(needp);
+  const SolvePlan& P = c.splan;
+  const size_t need = nrhs == 1 ? (size_t)std::max<int64_t>(P.part_len, 1)
+                                : (size_t)std::max<int64_t>(P.mpart_len, 1) * kMultiCols;
+  if (c.d_part.n < need) c.d_part.alloc(need);
 }
 
 // CTAs of a persistent kernel: all that fit on the device at once.
@@ -585,10 +847,39 @@ static int persistent_grid(K kernel, size_t smem) {
   return std::max(1, sms) * std::max(1, per);
 }
 
+static void launch_solve_multi(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st) {
+  FactorPlan& F = c.fplan;
+  SolvePlan& P = c.splan;
+  const size_t smem = sizeof(MultiSmem);
+  TEMF_CUDA(cudaFuncSetAttribute(k_fwd_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  TEMF_CUDA(cudaFuncSetAttribute(k_bwd_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int gridf = std::min(persistent_grid(k_fwd_multi, smem), std::max(P.n_mftask, 1));
+  const int gridb = std::min(persistent_grid(k_bwd_multi, smem), std::max(P.n_mbtask, 1));
+  for (int c0 = 0; c0 < nrhs; c0 += kMultiCols) {
+    const int k = std::min(kMultiCols, nrhs - c0);
+    TEMF_CUDA(cudaMemsetAsync(P.sync.p, 0, P.sync.bytes(), st));
+    k_fwd_multi<<<gridf, kSolveThreads, smem, st>>>(P.n_mftask, P.mftask.p, F.sn_first.p, F.sn_rows_ptr.p,
+                                                   F.sn_rows.p, F.sn_Lptr.p, Lbase, x + c0, nrhs, k, P.mftgt_ptr.p,
+                                                   P.mftgt.p, P.mfexpect.p, P.sync.p, P.nsn, c.d_status.p + 1);
+    TEMF_CHECK_LAUNCH();
+    k_bwd_multi<<<gridb, kSolveThreads, smem, st>>>(P.n_mbtask, P.mbtask.p, F.sn_first.p, F.sn_rows_ptr.p,
+                                                   F.sn_rows.p, F.sn_Lptr.p, Lbase, x + c0, nrhs, k, P.mbtgt_ptr.p,
+                                                   P.mbtgt.p, P.mnchunk.p, P.mpart_off.p, c.d_part.p, P.sync.p,
+                                                   P.nsn, c.d_status.p + 1);
+    TEMF_CHECK_LAUNCH();
+  }
+}
+
+int solve_launch_count(int nrhs) { return nrhs == 1 ? 2 : 2 * ceil_div(nrhs, kMultiCols); }
+
 void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st) {
   FactorPlan& F = c.fplan;
   SolvePlan& P = c.splan;
   ensure_update_buffer(c, nrhs);
+  if (nrhs > 1) {
+    launch_solve_multi(c, Lbase, x, nrhs, st);
+    return;
+  }
   const size_t smem = (size_t)(kSnCols + kChunkRows) * nrhs * sizeof(double);
   if (smem > 12 * 1024) {
     TEMF_CUDA(cudaFuncSetAttribute(k_fwd_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

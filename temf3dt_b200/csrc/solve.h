@@ -9,6 +9,8 @@ void ensure_update_buffer(temf_ctx& c, int nrhs);
 // `Lbase` points at a device word holding the panel base of the factor to use
 // (an indirection so captured graphs can follow the factor slot).
 void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st);
+// kernels launch_solve issues for nrhs columns
+int solve_launch_count(int nrhs);
 // Single right-hand side, every scratch word supplied by the caller: `sync`
 // (4*nsn+4 ints, cleared here), `part` (part_len doubles), `err` (one int).
 void launch_solve_scratch(temf_ctx& c, double* const* Lbase, double* x, int* sync, double* part, int* err,

@@ -1,6 +1,7 @@
 """Run the first N time steps of a benchmark model, for profiler captures.
 
     python -m temf3dt_b200.profile_case --config 0 --max-steps 150
+    python -m temf3dt_b200.profile_case --config 2 --max-steps 150   # 64 loops = 64 RHS columns
 
 Builds the same seeded synthetic model as ``bench.py --config K``, assembles
 and analyses it, and runs the FETD time loop for the first ``max-steps``
@@ -26,13 +27,21 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", type=int, default=0, choices=sorted(CONFIG_KW))
     ap.add_argument("--max-steps", type=int, default=150)
+    ap.add_argument("--rhs", type=int, default=0, help="multiloop: use the first RHS loops only (0 = all)")
     a = ap.parse_args()
     kind, kw = CONFIG_KW[a.config]
     kw = dict(kw)
     kw.update(COMMON)
     m = synth.build_model(kind, seed=a.config, **kw)
     with fetd.FetdGPU(0) as g:
-        fetd.load_case(g, m.mesh, m.ctl)
+        info = fetd.load_case(g, m.mesh, m.ctl)
+        if kind == "multiloop":
+            # every loop is a right-hand-side column with its own receiver
+            cols = m.source_columns(info["edg_vex"])
+            k = len(cols) if a.rhs <= 0 else min(a.rhs, len(cols))
+            g.set_sources(cols[:k], 1, m.ctl.pulse_type, m.ctl.t0, 1.0)
+            sel = [i for i in range(len(m.receivers)) if m.rec_rhs[i] < k]
+            g.set_receivers(g.locate(m.receivers[sel], m.ctl.rec_charac), m.receivers[sel], rec_rhs=m.rec_rhs[sel])
         st = g.stats()
         out = g.run(m.ctl.sp_division, m.ctl.sp_double, m.ctl.sp_dblesize, m.ctl.time_maximum,
                     max_steps=a.max_steps)
