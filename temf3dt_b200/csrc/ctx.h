@@ -76,8 +76,8 @@ struct SolvePlan {
   DBuf<SolveTask> mftask, mbtask;
   int n_mftask = 0, n_mbtask = 0;
   DBuf<int> mftgt_ptr, mftgt, mfexpect, mbtgt_ptr, mbtgt, mnchunk;
-  DBuf<int64_t> mpart_off;
-  int64_t mpart_len = 0;
+  DBuf<int64_t> macc_off;      // per supernode with >= 2 chunks: row offset of its c x 64 accumulator
+  int64_t macc_len = 0;
   DBuf<int> sync;              // ready | ydone | cdone | xdone (nsn each) | counters
   int nsn = 0;
 };
@@ -161,7 +161,7 @@ struct temf_ctx {
   temf::Source src;
   temf::Receivers rec;
   // scratch vectors
-  temf::DBuf<double> d_part;     // backward partial sums (part_len, or mpart_len * 64 for blocks)
+  temf::DBuf<double> d_part;     // backward partial sums (part_len), or block accumulators (macc_len * 64)
   temf::AdjointRecord adj;
   int u_nrhs = 0;
 };

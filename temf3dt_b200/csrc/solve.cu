@@ -372,8 +372,18 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_persistent(
 
 // ---------------------------------------------------------------------------
 // Blocks of up to 64 right-hand sides (many sources on one mesh): the same
-// persistent task graph with 64-row chunks; the chunk products are 64 x 64 x c
-// FP64 tensor-core (DMMA) tiles staged in shared memory.
+// persistent task graph with 64-row chunks.  Per task:
+//  * the panel block (64 rows x c columns) and the diagonal block are copied
+//    to shared memory with cp.async before any dependency wait, so their
+//    latency overlaps the wait;
+//  * right-hand-side rows are read with all of a thread's loads in flight at
+//    once (register staging; L2-coherent loads, since other CTAs write them);
+//  * the 64 x 64 x c chunk products run on the FP64 tensor cores (DMMA);
+//  * the c x 64 diagonal solves use two threads per column;
+//  * forward chunk updates are pushed into the ancestors' rows with FP64
+//    atomics; backward chunk partial sums are accumulated with FP64 atomics
+//    into one c x 64 block per supernode (zeroed before each sweep), so the
+//    diagonal task reads one block however many chunks the supernode has.
 // ---------------------------------------------------------------------------
 constexpr int kLdm = 72;  // padded leading dimension of the 64-wide shared tiles
 
@@ -382,6 +392,14 @@ __device__ __forceinline__ void dmma8(double& d0, double& d1, double a, double b
                : "+d"(d0), "+d"(d1)
                : "d"(a), "d"(b));
 }
+
+// 8-byte asynchronous global -> shared copy (L1-allocating: only for data
+// no CTA writes during the sweep, i.e. the factor panels)
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 struct MultiSmem {
   double D[kSnCols][kSnCols + 1];
@@ -430,12 +448,70 @@ __device__ __forceinline__ void zero_acc(double acc[4][4][2]) {
     for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
 }
 
-// panel rows [r0, r0+nr) x columns [0, c) of L21 into A[j][i] (zero padded to 64 x 64)
-__device__ __forceinline__ void load_panel_block(double* A, const double* P, int c, int64_t ld, int r0, int nr) {
+// panel rows [r0, r0+nr) x columns [0, c) of L21 into A[j][i] (zero padded to 64 x 64), asynchronously
+__device__ __forceinline__ void load_panel_block_async(double* A, const double* P, int c, int64_t ld, int r0,
+                                                       int nr) {
   for (int idx = threadIdx.x; idx < kSnCols * kSnCols; idx += blockDim.x) {
     const int j = idx / kSnCols, i = idx % kSnCols;
-    A[j * kLdm + i] = (j < c && i < nr) ? __ldg(P + (int64_t)j * ld + c + r0 + i) : 0.0;
+    if (j < c && i < nr) cp_async8(A + j * kLdm + i, P + (int64_t)j * ld + c + r0 + i);
+    else A[j * kLdm + i] = 0.0;
   }
+}
+// lower triangle of the diagonal block into D[i][j], asynchronously (rinv after the wait)
+__device__ __forceinline__ void load_diag_async(double (*D)[kSnCols + 1], const double* P, int c, int64_t ld) {
+  for (int idx = threadIdx.x; idx < c * c; idx += blockDim.x) {
+    const int j = idx / c, i = idx % c;
+    if (i >= j) cp_async8(&D[i][j], P + (int64_t)j * ld + i);
+  }
+}
+__device__ __forceinline__ void finish_diag(MultiSmem& M, int c) {
+  if ((int)threadIdx.x < c) M.rinv[threadIdx.x] = 1.0 / M.D[threadIdx.x][threadIdx.x];
+}
+
+// Y[j][col] = x[rows[j]][col] for j < nr, col < k (zero elsewhere); every
+// load of a thread is issued before the first store.
+template <bool kContiguous>
+__device__ __forceinline__ void load_rows(double* Y, const double* x, int64_t ldx, int k, int nr, int f,
+                                          const int* __restrict__ rows) {
+  constexpr int kPer = kSnCols * kSnCols / kSolveThreads;
+  double v[kPer];
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int idx = threadIdx.x + u * kSolveThreads;
+    const int j = idx / kSnCols, col = idx % kSnCols;
+    const int64_t row = kContiguous ? (int64_t)(f + j) : (j < nr ? (int64_t)rows[j] : 0);
+    v[u] = (j < nr && col < k) ? __ldcg(x + row * ldx + col) : 0.0;
+  }
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int idx = threadIdx.x + u * kSolveThreads;
+    Y[(idx / kSnCols) * kLdm + idx % kSnCols] = v[u];
+  }
+}
+
+// Y = L11^{-1} Y (forward) or L11^{-T} Y (backward) for 64 columns; two
+// threads per column (adjacent lanes) split the rows by parity.
+__device__ __forceinline__ void diag_solve_block(MultiSmem& M, int c, bool forward) {
+  const int col = threadIdx.x >> 1, h = threadIdx.x & 1;
+  double* Y = M.Y;
+  if (forward) {
+    for (int j = 0; j < c; ++j) {
+      if ((j & 1) == h) Y[j * kLdm + col] *= M.rinv[j];
+      __syncwarp();
+      const double yj = Y[j * kLdm + col];
+      int i = j + 1;
+      if ((i & 1) != h) ++i;
+      for (; i < c; i += 2) Y[i * kLdm + col] -= M.D[i][j] * yj;
+    }
+  } else {
+    for (int j = c - 1; j >= 0; --j) {
+      if ((j & 1) == h) Y[j * kLdm + col] *= M.rinv[j];
+      __syncwarp();
+      const double xj = Y[j * kLdm + col];
+      for (int i = h; i < j; i += 2) Y[i * kLdm + col] -= M.D[j][i] * xj;
+    }
+  }
+  __syncthreads();
 }
 
 __global__ void __launch_bounds__(kSolveThreads) k_fwd_multi(
@@ -466,29 +542,21 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_multi(
     const int64_t ld = c + r;
     const double* P = Lb + Lptr[s];
     const int nr = T.r1 - T.r0;
-    if (nr > 0) load_panel_block(M.A, P, c, ld, T.r0, nr);  // independent of the waits
-    if (T.kind == 0) {
-      load_diag(M.D, M.rinv, P, c, ld);
-      if (tid == 0) wait_geq(ready + s, expect[s], err, 1);
-    } else {
-      if (tid == 0) wait_geq(ydone + s, 1, err, 2);
+    // the factor does not depend on the sweep: start its copies before the waits
+    if (nr > 0) load_panel_block_async(M.A, P, c, ld, T.r0, nr);
+    if (T.kind == 0) load_diag_async(M.D, P, c, ld);
+    if (tid == 0) {
+      if (T.kind == 0) wait_geq(ready + s, expect[s], err, 1);
+      else wait_geq(ydone + s, 1, err, 2);
     }
     __syncthreads();
-    for (int idx = tid; idx < kSnCols * kSnCols; idx += blockDim.x) {
-      const int j = idx / kSnCols, col = idx % kSnCols;
-      M.Y[j * kLdm + col] = (j < c && col < k) ? __ldcg(x + (int64_t)(f + j) * ldx + col) : 0.0;
-    }
+    load_rows<true>(M.Y, x, ldx, k, c, f, nullptr);
+    cp_async_wait_all();
     __syncthreads();
     if (T.kind == 0) {
-      // Y_s = L11^{-1} B_s, one thread per right-hand side
-      if (tid < k) {
-        for (int j = 0; j < c; ++j) {
-          const double v = M.Y[j * kLdm + tid] * M.rinv[j];
-          M.Y[j * kLdm + tid] = v;
-          for (int i = j + 1; i < c; ++i) M.Y[i * kLdm + tid] -= M.D[i][j] * v;
-        }
-      }
+      finish_diag(M, c);
       __syncthreads();
+      diag_solve_block(M, c, true);
       for (int idx = tid; idx < c * k; idx += blockDim.x) {
         const int j = idx / k, col = idx % k;
         x[(int64_t)(f + j) * ldx + col] = M.Y[j * kLdm + col];
@@ -522,7 +590,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(
     int ntask, const SolveTask* __restrict__ tasks, const int* __restrict__ sn_first,
     const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows, const int64_t* __restrict__ Lptr,
     double* const* Lbase, double* x, int ldx, int k, const int* __restrict__ own_ptr, const int* __restrict__ own,
-    const int* __restrict__ nchunk, const int64_t* __restrict__ part_off, double* part, int* sync, int nsn,
+    const int* __restrict__ nchunk, const int64_t* __restrict__ acc_off, double* accum, int* sync, int nsn,
     int* err) {
   extern __shared__ __align__(16) unsigned char smraw[];
   MultiSmem& M = *reinterpret_cast<MultiSmem*>(smraw);
@@ -547,59 +615,51 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(
     const int64_t ld = c + r;
     const double* P = Lb + Lptr[s];
     const int nr = T.r1 - T.r0;
-    if (nr > 0) load_panel_block(M.A, P, c, ld, T.r0, nr);
-    if (T.kind == 0) load_diag(M.D, M.rinv, P, c, ld);
+    if (nr > 0) load_panel_block_async(M.A, P, c, ld, T.r0, nr);
+    if (T.kind == 0) load_diag_async(M.D, P, c, ld);
     if (tid == 0) {
       for (int q = own_ptr[t]; q < own_ptr[t + 1]; ++q) wait_geq(xdone + own[q], 1, err, 3);
       if (T.kind == 0) wait_geq(cdone + s, nchunk[s] - (nr > 0 ? 1 : 0), err, 4);
     }
     __syncthreads();
+    // Xr = x[rows] (64 x k); C = L21[rows]^T Xr (c x k)
+    if (nr > 0) load_rows<false>(M.Y, x, ldx, k, nr, 0, sn_rows + rp + T.r0);
+    cp_async_wait_all();
+    __syncthreads();
     double acc[4][4][2];
     zero_acc(acc);
     if (nr > 0) {
-      // Xr = x[rows] (64 x k), then C = L21[rows]^T Xr (c x k)
-      for (int idx = tid; idx < kSnCols * kSnCols; idx += blockDim.x) {
-        const int i = idx / kSnCols, col = idx % kSnCols;
-        M.Y[i * kLdm + col] = (i < nr && col < k) ? __ldcg(x + (int64_t)sn_rows[rp + T.r0 + i] * ldx + col) : 0.0;
-      }
-      __syncthreads();
       mma_tile64(acc, M.A, kLdm, 1, M.Y, 64);
       __syncthreads();
     }
+    double* as = accum + acc_off[s] * kMultiCols;  // this supernode's c x 64 accumulator
     if (T.kind == 1) {
-      const int chunk = T.r0 / kChunkRowsMulti;
-      double* pp = part + (part_off[s] + (int64_t)chunk * c) * kMultiCols;
       store_tile64(acc, M.Y);
       __syncthreads();
-      for (int idx = tid; idx < c * kMultiCols; idx += blockDim.x) {
-        const int j = idx / kMultiCols, col = idx % kMultiCols;
-        pp[idx] = M.Y[j * kLdm + col];
-      }
+      const int warp = tid >> 5, lane = tid & 31;
+      for (int j = warp; j < c; j += kSolveThreads / 32)
+        for (int col = lane; col < k; col += 32) atomicAdd(as + j * kMultiCols + col, M.Y[j * kLdm + col]);
       __threadfence();
       __syncthreads();
       if (tid == 0) atomicAdd(cdone + s, 1);
     } else {
-      // Z = Y_s - (first chunk, here) - (other chunks, in order); back-substitute
+      // Z = Y_s - (first chunk, here) - (other chunks, accumulated); back-substitute
+      finish_diag(M, c);
       store_tile64(acc, M.A);  // first-chunk products as [j][col]
       __syncthreads();
-      const int nch = nchunk[s];
-      const double* pp = part + part_off[s] * kMultiCols;
-      for (int idx = tid; idx < c * k; idx += blockDim.x) {
-        const int j = idx / k, col = idx % k;
-        double v = __ldcg(x + (int64_t)(f + j) * ldx + col);
-        if (nr > 0) v -= M.A[j * kLdm + col];
-        for (int q = 1; q < nch; ++q) v -= __ldcg(pp + ((int64_t)q * c + j) * kMultiCols + col);
+      const bool more = nchunk[s] > 1;
+      for (int idx = tid; idx < kSnCols * kSnCols; idx += blockDim.x) {
+        const int j = idx / kSnCols, col = idx % kSnCols;
+        double v = 0.0;
+        if (j < c && col < k) {
+          v = __ldcg(x + (int64_t)(f + j) * ldx + col);
+          if (nr > 0) v -= M.A[j * kLdm + col];
+          if (more) v -= __ldcg(as + j * kMultiCols + col);
+        }
         M.Y[j * kLdm + col] = v;
       }
       __syncthreads();
-      if (tid < k) {
-        for (int j = c - 1; j >= 0; --j) {
-          const double v = M.Y[j * kLdm + tid] * M.rinv[j];
-          M.Y[j * kLdm + tid] = v;
-          for (int i = 0; i < j; ++i) M.Y[i * kLdm + tid] -= M.D[j][i] * v;
-        }
-      }
-      __syncthreads();
+      diag_solve_block(M, c, false);
       for (int idx = tid; idx < c * k; idx += blockDim.x) {
         const int j = idx / k, col = idx % k;
         x[(int64_t)(f + j) * ldx + col] = M.Y[j * kLdm + col];
@@ -824,8 +884,10 @@ void build_solve_plan(temf_ctx& c) {
   P.mbtgt_ptr.upload(b.btp.data(), b.btp.size(), st);
   P.mbtgt.upload(b.btg.data(), std::max<size_t>(b.btg.size(), 1), st);
   P.mnchunk.upload(b.nch.data(), b.nch.size(), st);
-  P.mpart_len = b.poff[nsn];
-  P.mpart_off.upload(b.poff.data(), b.poff.size(), st);
+  std::vector<int64_t> aoff(nsn + 1, 0);
+  for (int s = 0; s < nsn; ++s) aoff[s + 1] = aoff[s] + (b.nch[s] > 1 ? S.sn_first[s + 1] - S.sn_first[s] : 0);
+  P.macc_len = aoff[nsn];
+  P.macc_off.upload(aoff.data(), aoff.size(), st);
   P.sync.alloc(4 * (size_t)nsn + 4);
   TEMF_CUDA(cudaStreamSynchronize(st));
 }
@@ -833,7 +895,7 @@ void build_solve_plan(temf_ctx& c) {
 void ensure_update_buffer(temf_ctx& c, int nrhs) {
   const SolvePlan& P = c.splan;
   const size_t need = nrhs == 1 ? (size_t)std::max<int64_t>(P.part_len, 1)
-                                : (size_t)std::max<int64_t>(P.mpart_len, 1) * kMultiCols;
+                                : (size_t)std::max<int64_t>(P.macc_len, 1) * kMultiCols;
   if (c.d_part.n < need) c.d_part.alloc(need);
 }
 
@@ -862,9 +924,10 @@ static void launch_solve_multi(temf_ctx& c, double* const* Lbase, double* x, int
                                                    F.sn_rows.p, F.sn_Lptr.p, Lbase, x + c0, nrhs, k, P.mftgt_ptr.p,
                                                    P.mftgt.p, P.mfexpect.p, P.sync.p, P.nsn, c.d_status.p + 1);
     TEMF_CHECK_LAUNCH();
+    TEMF_CUDA(cudaMemsetAsync(c.d_part.p, 0, (size_t)std::max<int64_t>(P.macc_len, 1) * kMultiCols * sizeof(double), st));
     k_bwd_multi<<<gridb, kSolveThreads, smem, st>>>(P.n_mbtask, P.mbtask.p, F.sn_first.p, F.sn_rows_ptr.p,
                                                    F.sn_rows.p, F.sn_Lptr.p, Lbase, x + c0, nrhs, k, P.mbtgt_ptr.p,
-                                                   P.mbtgt.p, P.mnchunk.p, P.mpart_off.p, c.d_part.p, P.sync.p,
+                                                   P.mbtgt.p, P.mnchunk.p, P.macc_off.p, c.d_part.p, P.sync.p,
                                                    P.nsn, c.d_status.p + 1);
     TEMF_CHECK_LAUNCH();
   }

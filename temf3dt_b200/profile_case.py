@@ -13,6 +13,8 @@ from __future__ import annotations
 import argparse
 import json
 
+import numpy as np
+
 from . import fetd, synth
 
 CONFIG_KW = {
@@ -28,11 +30,17 @@ def main() -> None:
     ap.add_argument("--config", type=int, default=0, choices=sorted(CONFIG_KW))
     ap.add_argument("--max-steps", type=int, default=150)
     ap.add_argument("--rhs", type=int, default=0, help="multiloop: use the first RHS loops only (0 = all)")
+    ap.add_argument("--scale", type=float, default=1.0, help="grid-line density factor (< 1: smaller mesh)")
+    ap.add_argument("--h-core", type=float, default=0.0, help="core cell size override (m)")
+    ap.add_argument("--replicate", type=int, default=1,
+                    help="single-loop models: solve the loop as this many identical RHS columns")
     a = ap.parse_args()
     kind, kw = CONFIG_KW[a.config]
     kw = dict(kw)
     kw.update(COMMON)
-    m = synth.build_model(kind, seed=a.config, **kw)
+    if a.h_core > 0:
+        kw["h_core"] = a.h_core
+    m = synth.build_model(kind, seed=a.config, scale=a.scale, **kw)
     with fetd.FetdGPU(0) as g:
         info = fetd.load_case(g, m.mesh, m.ctl)
         if kind == "multiloop":
@@ -42,6 +50,11 @@ def main() -> None:
             g.set_sources(cols[:k], 1, m.ctl.pulse_type, m.ctl.t0, 1.0)
             sel = [i for i in range(len(m.receivers)) if m.rec_rhs[i] < k]
             g.set_receivers(g.locate(m.receivers[sel], m.ctl.rec_charac), m.receivers[sel], rec_rhs=m.rec_rhs[sel])
+        elif a.replicate > 1:
+            cols = [(info["src_edg"], info["src_drc"])] * a.replicate
+            g.set_sources(cols, m.ctl.source_type, m.ctl.pulse_type, m.ctl.t0, m.ctl.current)
+            g.set_receivers(np.repeat(info["rec_tet"], a.replicate), np.repeat(m.ctl.rec_cor, a.replicate, axis=0),
+                            rec_rhs=np.arange(a.replicate))
         st = g.stats()
         out = g.run(m.ctl.sp_division, m.ctl.sp_double, m.ctl.sp_dblesize, m.ctl.time_maximum,
                     max_steps=a.max_steps)

@@ -211,7 +211,11 @@ def build_model(kind: str = "halfspace", seed: int = 0, scale: float = 1.0, **kw
                      the surface, one central receiver (the plain single-RHS case);
       "block"     -- conductive block in a host, square loop, receivers on a line;
       "multiloop" -- the block model with an nx*ny grid of small square loops,
-                     one RHS column and one central receiver each.
+                     one RHS column and one central receiver each;
+      "layered"   -- a 1-D layered earth (3-6 layers, conductivities
+                     log-uniform in [1e-4, 1e-1] S/m, thicknesses log-uniform
+                     in [10, 300] m, all drawn from the seed) under air, a
+                     square loop on the surface and one central receiver.
     ``scale`` multiplies the number of grid lines in the core (mesh size).
     """
     rng = np.random.default_rng(seed)
@@ -278,6 +282,29 @@ def build_model(kind: str = "halfspace", seed: int = 0, scale: float = 1.0, **kw
                                                  (np.abs(x - cx) < a) & (np.abs(y - cy) < a)))
                     rec.append(_nudge((cx, cy, kw.get("rec_z", 2.5)), g))
                     rec_rhs.append(len(loops0) - 1)
+    elif kind == "layered":
+        nlay = int(kw.get("n_layers", rng.integers(3, 7)))
+        sig_l = 10.0 ** rng.uniform(-4.0, -1.0, nlay)
+        thick = 10.0 ** rng.uniform(1.0, np.log10(300.0), nlay - 1)
+        tops = np.concatenate([[0.0], np.cumsum(thick)])          # top of each layer (z down)
+        a = kw.get("loop_half", 100.0)
+        h = kw.get("h_core", 25.0) / scale
+        xs = graded_axis([-a, a], (-a - 2 * h, a + 2 * h), h, half, kw.get("ratio", 1.5))
+        ys = xs.copy()
+        hz = kw.get("h_z", 10.0) / scale
+        zs = graded_axis(list(tops), (-2 * hz, tops[-1] + 2 * hz), hz, half, kw.get("ratio", 1.5), h_min=2.0)
+        g = Grid(xs, ys, zs)
+
+        def phys(x, y, z):
+            lay = np.clip(np.searchsorted(tops, z, side="right") - 1, 0, nlay - 1)
+            return np.where(z > 0, EARTH + lay, AIR)
+
+        nod, tets, tph = hex_to_tets(g, phys)
+        kz = int(np.searchsorted(zs, 0.0))
+        loops0 = [staircase_loop(g, kz, lambda x, y: (np.abs(x) < a) & (np.abs(y) < a))]
+        rec = [_nudge(kw.get("receiver", (0.0, 0.0, 2.0)), g)]
+        rec_rhs = [0]
+        domains = [(AIR, sig_air, 1.0, 1.0)] + [(EARTH + i, float(sig_l[i]), 1.0, 1.0) for i in range(nlay)]
     else:
         raise ValueError("unknown model kind %r" % kind)
     nod2, tets1, new = _renumber_loop_first(nod, tets, loops0[0])

@@ -1,0 +1,75 @@
+"""The adjoint gradient behind a torch.autograd.Function: the misfit of a
+run's receiver output as a differentiable function of per-cell
+log-conductivity.  torch is the harness here; the forward run and the
+gradient are the library's CUDA path (temf_run with recording, then
+temf_adjoint).  Marked ``gpu``; run on a B200."""
+import numpy as np
+import pytest
+import torch
+
+from temf3dt_b200 import fetd
+from tests.golden_cases import cell_grid_2x2x2, small_synth, synth_oracle_model
+
+pytestmark = pytest.mark.gpu
+
+
+class Misfit(torch.autograd.Function):
+    """J(m) = 1/2 sum w (d(m) - d_obs)^2 over the dB/dt columns, with
+    sigma_t = exp(m_cell(t)) inside the inversion cells and the background
+    conductivity elsewhere."""
+
+    @staticmethod
+    def forward(ctx, m, case):
+        g, model, sig0, mu, cell, d_obs, w = case
+        sig = sig0.copy()
+        inside = cell >= 0
+        sig[inside] = np.exp(m.detach().cpu().numpy()[cell[inside]])
+        g.set_media(sig, mu)
+        g.assemble()
+        g.adjoint_record(50)
+        c = model.ctl
+        out = g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum)
+        r = out.fields - d_obs
+        ctx.case = case
+        ctx.dJ = w * r
+        ctx.ncell = m.numel()
+        return torch.tensor(0.5 * float(np.sum(w * r * r)), dtype=torch.float64)
+
+    @staticmethod
+    def backward(ctx, gJ):
+        g, model, sig0, mu, cell, d_obs, w = ctx.case
+        grad, _, _ = g.adjoint(ctx.dJ, cell, ctx.ncell)
+        g.adjoint_record(0)
+        return gJ * torch.from_numpy(grad), None
+
+
+def test_autograd_gradient_descends_the_misfit():
+    model = small_synth()
+    om = synth_oracle_model(model)
+    cell = cell_grid_2x2x2(om)
+    with fetd.FetdGPU(0) as g:
+        info = fetd.load_case(g, model.mesh, model.ctl)
+        sig0, mu = info["sig"], info["mu"]
+        # observed data: cell 3 twice as conductive; dB/dt columns weighted by 1/max^2
+        sig_true = sig0.copy()
+        sig_true[cell == 3] *= 2.0
+        g.set_media(sig_true, mu)
+        g.assemble()
+        c = model.ctl
+        obs = g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum)
+        d_obs = obs.fields
+        w = np.zeros_like(d_obs)
+        w[:, :, 3:6] = 1.0 / np.maximum(np.abs(d_obs[:, :, 3:6]).max(axis=0), 1e-300) ** 2
+        case = (g, model, sig0, mu, cell, d_obs, w)
+        m = torch.full((8,), float(np.log(sig0[cell >= 0][0])), dtype=torch.float64, requires_grad=True)
+        J0 = Misfit.apply(m, case)
+        J0.backward()
+        grad = m.grad.clone()
+        assert torch.isfinite(grad).all() and grad.abs().max() > 0
+        # raising the perturbed cell's conductivity lowers the misfit
+        assert float(grad[3]) < 0
+        with torch.no_grad():
+            m1 = m - 0.2 * grad / grad.abs().max()
+        J1 = Misfit.apply(m1, case)
+        assert float(J1) < float(J0)
+        g.adjoint_record(0)

@@ -267,11 +267,12 @@ def test_pardiso_shim_and_pivot_status(small):
 
 def test_halfspace_central_loop_matches_analytic_response():
     """dBz/dt at the centre of a 500 m loop on a 0.001 S/m half-space against
-    the closed-form response (Ward & Hohmann eq. 4.98), 2 % over 1e-5..1e-3 s.
-    The staircase loop's enclosed area sets the effective radius."""
+    the closed-form response (Ward & Hohmann eq. 4.98) convolved with the erf
+    step-on waveform: within 2 % over 1e-5..1e-3 s.  The staircase loop's
+    enclosed area sets the effective radius; 10 m cells below the surface."""
     from temf3dt_b200 import synth
-    from tests.halfspace import central_loop_dbzdt
-    m = synth.build_model("halfspace", h_core=50, ratio=1.6, h_z=20, time_maximum=2e-3)
+    from tests.halfspace import erf_step_on_dbzdt
+    m = synth.build_model("halfspace", h_core=50, ratio=1.6, h_z=10, z_core=300, time_maximum=2e-3)
     sv = m.mesh.src_vex - 1
     P = m.mesh.nod_cor[sv[:, 0]]
     area = 0.5 * abs(np.sum(P[:, 0] * np.roll(P[:, 1], -1) - np.roll(P[:, 0], -1) * P[:, 1]))
@@ -282,7 +283,6 @@ def test_halfspace_central_loop_matches_analytic_response():
         gates = np.logspace(-5, -3, 21)
         v, done = g.gates(gates)
     assert done.all()
-    # step-on (pulse type 1) = negated step-off response after the ramp; compare magnitudes
-    ana = np.abs(central_loop_dbzdt(gates, 1e-3, a_eff))
-    rel = np.abs(np.abs(v[:, 0, 5]) - ana) / ana
+    ana = erf_step_on_dbzdt(gates, 1e-3, a_eff, m.ctl.t0)
+    rel = np.abs(v[:, 0, 5] - ana) / np.abs(ana)
     assert rel.max() <= 0.02, rel
