@@ -10,6 +10,9 @@ air 1e-12 S/m, 1000 m square loop, 64 receivers on a 20 m line, ~1.2M edges),
 synthetic and seeded.  Its factors (GBs) exceed the 126 MB L2 many times over,
 so no L2 flush is needed between steps.
 
+batched: 64 sources on the config-2 mesh as one 64-column block per step
+against the plain single-RHS path on that mesh, over the first 300 steps.
+
 adjoint: one gradient of a dB/dt misfit with respect to log sigma on a
 32 x 32 x 16 inversion grid (recorded forward run + reverse sweep), reported
 beside the metric with its ratio to one forward run.
@@ -170,6 +173,35 @@ def adjoint_measure(g, m, one_run, forward_ms):
             "grad_finite": bool(np.isfinite(grad).all())}
 
 
+def batched_measure(local: int, max_steps: int):
+    """64 small loops on the 3-D block mesh as one 64-column block per step
+    against the plain single-RHS path on the same mesh, both over the same
+    leading steps of the run (factorisations included), after one warm-up."""
+    from temf3dt_b200 import fetd
+    m = model_for(2)
+    c = m.ctl
+    out = {}
+    with fetd.FetdGPU(local) as g:
+        info = fetd.load_case(g, m.mesh, m.ctl)
+        out["n_edges"] = int(g.stats()["n"])
+        g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum, max_steps=max_steps)
+        o = g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum, max_steps=max_steps)
+        plain = (len(o.steps) - 1) / (o.ms_total / 1e3)
+        cols = m.source_columns(info["edg_vex"])
+        g.set_sources(cols, 1, c.pulse_type, c.t0, 1.0)
+        g.set_receivers(g.locate(m.receivers, c.rec_charac), m.receivers, rec_rhs=m.rec_rhs)
+        g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum, max_steps=max_steps)
+        ob = g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum, max_steps=max_steps)
+        batched = (len(ob.steps) - 1) * len(cols) / (ob.ms_total / 1e3)
+    out.update({"value": batched, "unit": "steps*RHS/s", "rhs": len(cols), "plain_value": plain,
+                "batched_over_plain": batched / plain, "steps": len(ob.steps) - 1,
+                "ms_per_step_batched": ob.ms_steps / max(ob.n_solve, 1),
+                "ms_per_step_plain": o.ms_steps / max(o.n_solve, 1),
+                "ms_factor_batched": ob.ms_factor, "ms_factor_plain": o.ms_factor,
+                "workload": CONFIGS[2]["label"] + ", first %d steps" % max_steps})
+    return out
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -285,6 +317,9 @@ def ours(args):
     adj = None
     if cfg != 2 and args.adjoint:
         adj = adjoint_measure(g, m, one_run, outs[-1].ms_total)
+    batched = None
+    if cfg == 1 and args.batched_steps > 0 and world == 1:
+        batched = batched_measure(local, args.batched_steps)
     # --- roofline of the dominant phase ---
     o = outs[-1]
     ms_fac = o.ms_factor / max(o.n_factor, 1)
@@ -337,6 +372,7 @@ def ours(args):
         "plain_same_mesh": plain,
         "batched_over_plain": (value / world / plain["value"]) if plain else None,
         "adjoint": adj,
+        "batched": batched,
         "phases_ms_per_run": {"factor": o.ms_factor, "steps": o.ms_steps, "total": o.ms_total,
                               "factor_each": ms_fac, "solve_step_each": ms_step, "setup_s": t_setup},
     }
@@ -358,6 +394,8 @@ def main():
     ap.add_argument("--sample-steps", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--adjoint", type=int, default=1, help="1: also time one adjoint gradient (single-RHS configs)")
+    ap.add_argument("--batched-steps", type=int, default=300,
+                    help="config 1: also compare a 64-RHS block with one RHS on the config-2 mesh over these steps")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

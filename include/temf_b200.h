@@ -36,6 +36,7 @@ extern "C" {
 #define TEMF_EINTERNAL (-4)
 
 typedef struct temf_ctx temf_ctx;
+typedef struct temf_batch temf_batch;
 
 /* ---- context --------------------------------------------------------- */
 /* Create a context on CUDA device `device`. */
@@ -199,6 +200,34 @@ int temf_adjoint(temf_ctx* ctx, const double* dJ_dfields, int ncell, const int* 
  * counts[0] solve-graph nodes, counts[1] checkpoint blocks, counts[2]
  * factorisations, counts[3] kernel launches.  Either pointer may be NULL. */
 int temf_adjoint_timing(temf_ctx* ctx, double* ms, long long* counts);
+
+/* ---- many models at once ------------------------------------------------------
+ * No reference counterpart (the reference runs one model per process).  A
+ * batch steps several independent models -- each a context prepared up to
+ * temf_set_sources/temf_set_receivers, one RHS column, pulse type 1 or 2 --
+ * through the adaptive time loop in lockstep on one GPU: every model keeps
+ * its own dt schedule, factors and accept/reject decisions, while the
+ * triangular solves of all models in a step run as one merged persistent
+ * forward and one backward kernel.  Results land in each model's context
+ * (temf_result_*).  The contexts must share a device and outlive the batch.
+ *
+ * temf_batch_run flags: bit 0 = legacy LINUX schedule (as temf_run), bit 1 =
+ * no CUDA graphs, bit 2 = autotune: before the first step the candidate
+ * merge orders (0 proportional interleave, 1 level-aligned, 2 one model after
+ * another) and resident-CTA fractions (100 %, 67 %) are timed on one merged
+ * solve and the fastest is kept for this and later runs.  max_steps 0 = no
+ * limit.  temf_batch_timing: ms[0..3] = whole run, factorisations, stepping,
+ * tuning; counts[0..2] = lockstep steps, kernel launches, merged solves.
+ * temf_batch_tuning returns 1 if tuned (order, grid_pct and, if not NULL,
+ * the six candidate times in ms), 0 if not. */
+int temf_batch_create(temf_ctx* const* models, int n_models, temf_batch** batch);
+int temf_batch_destroy(temf_batch* batch);
+const char* temf_batch_last_error(const temf_batch* batch);
+int temf_batch_run(temf_batch* batch, int sp_division, int sp_double, int sp_dblesize, double time_maximum,
+                   int flags, int max_steps);
+int temf_batch_timing(temf_batch* batch, double* ms, long long* counts);
+int temf_batch_tuning(temf_batch* batch, int* order, int* grid_pct, double* candidate_ms);
+int temf_batch_set_tuning(temf_batch* batch, int order, int grid_pct);
 
 /* ---- statistics of the symbolic analysis ----------------------------------
  * stats[0..9] = n, nnz(A full), supernodes, levels, nnz(L), stored doubles,

@@ -51,6 +51,13 @@ SIGNATURES = {
     "temf_analysis_stats": (_i, [_p, _dp]),
     "temf_symbolic_host": (_i, [_i, C.POINTER(C.c_longlong), _ip, _dp, _ip, _dp]),
     "temf_adjoint_record": (_i, [_p, _i]),
+    "temf_batch_create": (_i, [C.POINTER(C.c_void_p), _i, C.POINTER(C.c_void_p)]),
+    "temf_batch_destroy": (_i, [_p]),
+    "temf_batch_last_error": (C.c_char_p, [_p]),
+    "temf_batch_run": (_i, [_p, _i, _i, _i, _d, _i, _i]),
+    "temf_batch_timing": (_i, [_p, _dp, C.POINTER(C.c_longlong)]),
+    "temf_batch_tuning": (_i, [_p, _ip, _ip, _dp]),
+    "temf_batch_set_tuning": (_i, [_p, _i, _i]),
     "temf_adjoint": (_i, [_p, _dp, _i, _ip, _dp, _dp]),
     "temf_adjoint_timing": (_i, [_p, _dp, C.POINTER(C.c_longlong)]),
     "temf_pardiso_alloc": (_i, [_p, _i]),

@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libtemf_b200.so")
 BUILD = os.path.join(ROOT, "_build")
 
-SOURCES = ["symbolic.cpp", "assemble.cu", "factor.cu", "solve.cu", "fetd.cu", "capi.cu", "noalloc.cu", "adjoint.cu"]
+SOURCES = ["symbolic.cpp", "assemble.cu", "factor.cu", "solve.cu", "fetd.cu", "capi.cu", "noalloc.cu", "adjoint.cu", "batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
           "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]

@@ -8,6 +8,7 @@
 #include "../../include/temf_b200.h"
 #include "adjoint.h"
 #include "assemble.h"
+#include "batch.h"
 #include "factor.h"
 #include "fetd.h"
 #include "solve.h"
@@ -17,6 +18,11 @@ using namespace temf;
 struct temf_run_state {
   RunResult res;
   bool valid = false;
+};
+
+struct temf_batch {
+  temf::Batch b;
+  std::string err;
 };
 
 namespace {
@@ -76,6 +82,29 @@ int guarded(temf_ctx* c, F&& f) {
     return TEMF_EINTERNAL;
   }
 }
+
+template <typename F>
+int guarded_batch(temf_batch* B, F&& f) {
+  if (!B) return TEMF_EARG;
+  try {
+    TEMF_CUDA(cudaSetDevice(B->b.device));
+    B->err.clear();
+    return f();
+  } catch (const ArgError& e) {
+    B->err = e.what();
+    return TEMF_EARG;
+  } catch (const StateError& e) {
+    B->err = e.what();
+    return TEMF_ESTATE;
+  } catch (const CudaError& e) {
+    B->err = e.what();
+    return TEMF_ECUDA;
+  } catch (const std::exception& e) {
+    B->err = e.what();
+    return TEMF_EINTERNAL;
+  }
+}
+
 
 // K7 set-up: n_arr / d_arr (src/FETD_FWD.f90:712-731) for each receiver.
 // lambda'_k = a_k + b_k x + c_k y + d_k z is evaluated as six times the signed
@@ -785,6 +814,95 @@ int temf_result_timing(temf_ctx* c, double* ms_factor, double* ms_steps, double*
     if (n_factor) *n_factor = R.n_factor;
     if (n_solve) *n_solve = R.n_solve;
     if (n_launch) *n_launch = (long long)R.launches;
+    return TEMF_OK;
+  });
+}
+
+// ---- many models at once ---------------------------------------------------
+int temf_batch_create(temf_ctx* const* models, int n_models, temf_batch** out) {
+  if (!out || !models || n_models < 1) return TEMF_EARG;
+  temf_batch* B = new temf_batch();
+  *out = B;
+  B->b.device = models[0] ? models[0]->device : 0;
+  return guarded_batch(B, [&] {
+    for (int m = 0; m < n_models; ++m) {
+      temf_ctx* c = models[m];
+      if (!c) throw ArgError("temf_batch_create: NULL model");
+      if (c->device != B->b.device) throw ArgError("temf_batch_create: models on different devices");
+      for (int q = 0; q < m; ++q)
+        if (models[q] == c) throw ArgError("temf_batch_create: a model appears twice");
+      B->b.models.push_back(c);
+    }
+    TEMF_CUDA(cudaStreamCreateWithFlags(&B->b.stream, cudaStreamNonBlocking));
+    return TEMF_OK;
+  });
+}
+
+int temf_batch_destroy(temf_batch* B) {
+  if (!B) return TEMF_EARG;
+  cudaSetDevice(B->b.device);
+  if (B->b.stream) {
+    cudaStreamSynchronize(B->b.stream);
+    cudaStreamDestroy(B->b.stream);
+  }
+  delete B;
+  return TEMF_OK;
+}
+
+const char* temf_batch_last_error(const temf_batch* B) { return B ? B->err.c_str() : "null batch"; }
+
+int temf_batch_run(temf_batch* B, int sp_division, int sp_double, int sp_dblesize, double time_maximum, int flags,
+                   int max_steps) {
+  return guarded_batch(B, [&] {
+    for (temf_ctx* c : B->b.models) {
+      need(c->assembled, "temf_batch_run: assemble every model first");
+      need(c->src.nrhs >= 1, "temf_batch_run: set every model's source first");
+      extra(c).run.valid = false;
+      c->adj.valid = false;
+    }
+    RunOptions o;
+    o.step_dvsi = sp_division;
+    o.step_dble = sp_double;
+    o.step_dblesize = sp_dblesize;
+    o.time_maximum = time_maximum;
+    o.legacy_linux = flags & 1;
+    o.use_graphs = (flags & 2) ? 0 : 1;
+    o.max_steps = max_steps;
+    run_batch(B->b, o, (flags & 4) != 0);
+    for (size_t m = 0; m < B->b.models.size(); ++m) {
+      CtxExtra& X = extra(B->b.models[m]);
+      X.run.res = std::move(B->b.results[m]);
+      X.run.valid = true;
+    }
+    return TEMF_OK;
+  });
+}
+
+int temf_batch_timing(temf_batch* B, double* ms, long long* counts) {
+  return guarded_batch(B, [&] {
+    const BatchStats& S = B->b.stats;
+    if (ms) { ms[0] = S.ms_total; ms[1] = S.ms_factor; ms[2] = S.ms_steps; ms[3] = S.ms_tune; }
+    if (counts) { counts[0] = S.steps; counts[1] = S.launches; counts[2] = S.solves; }
+    return TEMF_OK;
+  });
+}
+
+int temf_batch_tuning(temf_batch* B, int* order, int* grid_pct, double* candidate_ms) {
+  return guarded_batch(B, [&] {
+    if (order) *order = B->b.tune.order;
+    if (grid_pct) *grid_pct = B->b.tune.grid_pct;
+    if (candidate_ms)
+      for (size_t i = 0; i < B->b.stats.tune_ms.size(); ++i) candidate_ms[i] = B->b.stats.tune_ms[i];
+    return B->b.tuned ? 1 : 0;
+  });
+}
+
+int temf_batch_set_tuning(temf_batch* B, int order, int grid_pct) {
+  return guarded_batch(B, [&] {
+    if (order < 0 || order > 2 || grid_pct < 1 || grid_pct > 100) throw ArgError("temf_batch_set_tuning: bad value");
+    B->b.tune.order = order;
+    B->b.tune.grid_pct = grid_pct;
+    B->b.tuned = true;
     return TEMF_OK;
   });
 }

@@ -347,6 +347,30 @@ int numeric_factor(temf_ctx& c, int slot, double dt) {
 }
 
 int numeric_factor_values(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b) {
+  launch_factor_values(c, slot, X, a, Y, b);
+  return finish_factor(c, slot);
+}
+
+int finish_factor(temf_ctx& c, int slot) {
+  FactorSlot& fs = c.slots[slot];
+  int status = 0;
+  TEMF_CUDA(cudaMemcpyAsync(&status, c.d_status.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  TEMF_CUDA(cudaStreamSynchronize(c.stream));
+  if (status != INT_MAX) {
+    fs.valid = false;
+    fs.status = c.sym.perm[status - 1] + 1;
+    return fs.status;
+  }
+  fs.valid = true;
+  fs.status = 0;
+  return 0;
+}
+
+void launch_factor(temf_ctx& c, int slot, double dt) {
+  launch_factor_values(c, slot, c.d_M.p, 3.0, c.d_K.p, 2.0 * dt);
+}
+
+void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b) {
   const Symbolic& S = c.sym;
   FactorPlan& F = c.fplan;
   FactorSlot& fs = c.slots[slot];
@@ -384,18 +408,8 @@ int numeric_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
       TEMF_CHECK_LAUNCH();
     }
   }
-  int status = 0;
-  TEMF_CUDA(cudaMemcpyAsync(&status, c.d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-  TEMF_CUDA(cudaStreamSynchronize(st));
   fs.dt = b * 0.5;
-  if (status != INT_MAX) {
-    fs.valid = false;
-    fs.status = c.sym.perm[status - 1] + 1;
-    return fs.status;
-  }
-  fs.valid = true;
-  fs.status = 0;
-  return 0;
+  fs.valid = false;
 }
 
 }  // namespace temf

@@ -12,4 +12,10 @@ int numeric_factor(temf_ctx& c, int slot, double dt);
 // General form: L = LL^T factor of a*X + b*Y where X, Y are values on the
 // permuted full pattern (device arrays).  Same return convention.
 int numeric_factor_values(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b);
+// The same in two halves: enqueue every kernel on the context's stream, then
+// (finish) wait for the stream and read the pivot status.  Factorisations of
+// different contexts can run concurrently between the two calls.
+void launch_factor(temf_ctx& c, int slot, double dt);
+void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b);
+int finish_factor(temf_ctx& c, int slot);
 }  // namespace temf

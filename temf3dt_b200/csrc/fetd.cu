@@ -29,7 +29,7 @@ static double deltafunc1(double t, double t0) {  // :1144-1147
   const double a = t * 5.436563656918091 - t0 * 2.718281828459046;
   return -1.0 / (t0 * t0) * std::exp(-1.0 / (t0 * t0) * a * a) * (t * 59.11244879144521 - t0 * 29.55622439572261);
 }
-static double time_const_p(int source_type, int pulse_type, double t, double t0, double cur) {  // :1050-1078
+double time_const_p(int source_type, int pulse_type, double t, double t0, double cur) {  // :1050-1078
   if (source_type == 1 && pulse_type == 1) return erfstepon1(t, t0) * cur;
   if (source_type == 1 && pulse_type == 2) return deltafunc1(t, t0) * cur;
   if (source_type == 1 && pulse_type == 3) return -erfstepon1(t, t0) * cur;
@@ -49,6 +49,15 @@ __global__ void k_receivers_row(int nrec, const int* __restrict__ edges, const i
 #pragma unroll
   for (int j = 0; j < 6; ++j) acc += w[rec * 36 + q * 6 + j] * x[(int64_t)edges[rec * 6 + j] * nrhs + rrhs[rec]];
   trace[((int64_t)(row_base[0] + k) * nrec + rec) * 6 + q] = acc;
+}
+
+void launch_receivers_row(temf_ctx& c, const double* x, int nrhs, const int* row_base, int k, double* trace,
+                          cudaStream_t st) {
+  const int nrec = c.rec.nrec;
+  if (!nrec) return;
+  k_receivers_row<<<ceil_div(nrec * 6, 128), 128, 0, st>>>(nrec, c.rec.d_edges.p, c.rec.d_rhs.p, c.rec.d_w.p, x, nrhs,
+                                                           row_base, k, trace);
+  TEMF_CHECK_LAUNCH();
 }
 
 namespace {

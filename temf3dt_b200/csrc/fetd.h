@@ -32,6 +32,12 @@ struct RunResult {
   int64_t launches = 0;
 };
 
+// dI/dt of the source waveform (time_const_p, src/FETD_UTILITY.f90:1050-1078)
+double time_const_p(int source_type, int pulse_type, double t, double t0, double cur);
+// receiver samples of x into trace row (row_base[0] + k)
+void launch_receivers_row(temf_ctx& c, const double* x, int nrhs, const int* row_base, int k, double* trace,
+                          cudaStream_t st);
+
 // Adaptive BDF2 time loop (adap_euler, src/FETD_FWD.f90:1229-1464) on the GPU.
 // Pulse type 3 runs the DC pass first (time_solver, :1212-1215).
 void run_fetd(temf_ctx& c, const RunOptions& opt, RunResult& res);

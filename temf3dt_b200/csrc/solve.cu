@@ -186,6 +186,60 @@ __device__ __forceinline__ void fin_bwd(const BwdRegs& R, const double* zs, int 
 //     ready counter of each supernode owning one of the rows;
 //   chunk task (s, r0..r1), r0 >= 128: wait for y_s, push the same way.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double* Lb, int nrhs, int* err,
+                                         double (*D)[kSnCols + 1], double* rinv, double* ys) {
+  int* ready = V.sync;
+  int* ydone = V.sync + V.nsn;
+  double* x = V.x;
+  const int tid = threadIdx.x;
+  const SolveTask T = V.tasks[t];
+  const int s = T.s;
+  const int f = V.sn_first[s];
+  const int c = V.sn_first[s + 1] - f;
+  const int64_t rp = V.rows_ptr[s];
+  const int64_t r = V.rows_ptr[s + 1] - rp;
+  const int64_t ld = c + r;
+  const double* P = Lb + V.Lptr[s];
+  const double* Pc = P + c;
+  const int i = T.r0 + tid;
+  const bool row_on = i < T.r1;
+  FwdRegs R;
+  if (nrhs == 1) pre_fwd(R, Pc, c, ld, i, row_on);
+  if (T.kind == 0) {
+    load_diag(D, rinv, P, c, ld);
+    if (tid == 0) wait_geq(ready + s, V.expect[s], err, 1);
+    __syncthreads();
+    for (int idx = tid; idx < c * nrhs; idx += blockDim.x) ys[idx] = __ldcg(x + (int64_t)f * nrhs + idx);
+    __syncthreads();
+    diag_solve(D, rinv, ys, c, nrhs, true);
+    for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = ys[idx];
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) atomicExch(ydone + s, 1);
+  } else {
+    if (tid == 0) wait_geq(ydone + s, 1, err, 2);
+    __syncthreads();
+    for (int idx = tid; idx < c * nrhs; idx += blockDim.x) ys[idx] = __ldcg(x + (int64_t)f * nrhs + idx);
+    __syncthreads();
+  }
+  if (T.r1 > T.r0) {
+    if (nrhs == 1) {
+      if (row_on) atomicAdd(x + V.sn_rows[rp + i], -fin_fwd(R, ys, c));
+    } else if (row_on) {
+      double* dst = x + (int64_t)V.sn_rows[rp + i] * nrhs;
+      for (int col = 0; col < nrhs; ++col) {
+        double a = 0.0;
+        for (int j = 0; j < c; ++j) a += __ldg(Pc + (int64_t)j * ld + i) * ys[j * nrhs + col];
+        atomicAdd(dst + col, -a);
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0)
+      for (int q = V.tgt_ptr[t]; q < V.tgt_ptr[t + 1]; ++q) atomicAdd(ready + V.tgt[q], 1);
+  }
+}
+
 __global__ void __launch_bounds__(kSolveThreads) k_fwd_persistent(
     int ntask, const SolveTask* __restrict__ tasks, const int* __restrict__ sn_first,
     const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows, const int64_t* __restrict__ Lptr,
@@ -195,63 +249,17 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_persistent(
   __shared__ double rinv[kSnCols];
   extern __shared__ double ys[];  // c x nrhs
   __shared__ int task_id;
-  int* ready = sync;
-  int* ydone = sync + nsn;
   int* counter = sync + 4 * nsn;
-  const int tid = threadIdx.x;
+  const SweepView V{tasks, sn_first, rows_ptr, sn_rows, Lptr, Lbase, x, tgt_ptr, tgt, expect,
+                    nullptr, nullptr, nullptr, sync, nsn, ntask};
   const double* Lb = *Lbase;
   for (;;) {
-    if (tid == 0) task_id = atomicAdd(counter, 1);
+    if (threadIdx.x == 0) task_id = atomicAdd(counter, 1);
     __syncthreads();
     const int t = task_id;
     __syncthreads();
     if (t >= ntask) break;
-    const SolveTask T = tasks[t];
-    const int s = T.s;
-    const int f = sn_first[s];
-    const int c = sn_first[s + 1] - f;
-    const int64_t rp = rows_ptr[s];
-    const int64_t r = rows_ptr[s + 1] - rp;
-    const int64_t ld = c + r;
-    const double* P = Lb + Lptr[s];
-    const double* Pc = P + c;
-    const int i = T.r0 + tid;
-    const bool row_on = i < T.r1;
-    FwdRegs R;
-    if (nrhs == 1) pre_fwd(R, Pc, c, ld, i, row_on);
-    if (T.kind == 0) {
-      load_diag(D, rinv, P, c, ld);
-      if (tid == 0) wait_geq(ready + s, expect[s], err, 1);
-      __syncthreads();
-      for (int idx = tid; idx < c * nrhs; idx += blockDim.x) ys[idx] = __ldcg(x + (int64_t)f * nrhs + idx);
-      __syncthreads();
-      diag_solve(D, rinv, ys, c, nrhs, true);
-      for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = ys[idx];
-      __threadfence();
-      __syncthreads();
-      if (tid == 0) atomicExch(ydone + s, 1);
-    } else {
-      if (tid == 0) wait_geq(ydone + s, 1, err, 2);
-      __syncthreads();
-      for (int idx = tid; idx < c * nrhs; idx += blockDim.x) ys[idx] = __ldcg(x + (int64_t)f * nrhs + idx);
-      __syncthreads();
-    }
-    if (T.r1 > T.r0) {
-      if (nrhs == 1) {
-        if (row_on) atomicAdd(x + sn_rows[rp + i], -fin_fwd(R, ys, c));
-      } else if (row_on) {
-        double* dst = x + (int64_t)sn_rows[rp + i] * nrhs;
-        for (int col = 0; col < nrhs; ++col) {
-          double a = 0.0;
-          for (int j = 0; j < c; ++j) a += __ldg(Pc + (int64_t)j * ld + i) * ys[j * nrhs + col];
-          atomicAdd(dst + col, -a);
-        }
-      }
-      __threadfence();
-      __syncthreads();
-      if (tid == 0)
-        for (int q = tgt_ptr[t]; q < tgt_ptr[t + 1]; ++q) atomicAdd(ready + tgt[q], 1);
-    }
+    fwd_task(V, t, Lb, nrhs, err, D, rinv, ys);
   }
 }
 
@@ -264,6 +272,96 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_persistent(
 //     the owners of the first chunk's rows, z = y_s - partials (fixed order,
 //     so the backward sweep is deterministic), solve with L11^T, publish x_s.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double* Lb, int nrhs, int* err,
+                                         double (*D)[kSnCols + 1], double* rinv, double (*seg)[kSnCols],
+                                         double* zs) {
+  int* cdone = V.sync + 2 * V.nsn;
+  int* xdone = V.sync + 3 * V.nsn;
+  double* x = V.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const SolveTask T = V.tasks[t];
+  const int s = T.s;
+  const int f = V.sn_first[s];
+  const int c = V.sn_first[s + 1] - f;
+  const int64_t rp = V.rows_ptr[s];
+  const int64_t r = V.rows_ptr[s + 1] - rp;
+  const int64_t ld = c + r;
+  const double* P = Lb + V.Lptr[s];
+  const int nr = T.r1 - T.r0;
+  BwdRegs R;
+  if (nrhs == 1 && nr > 0) pre_bwd(R, P, c, ld, T.r0, nr);
+  if (T.kind == 0) load_diag(D, rinv, P, c, ld);
+  // the chunk's rows need their owners' x; the diagonal task also its other chunks
+  if (tid == 0) {
+    for (int q = V.tgt_ptr[t]; q < V.tgt_ptr[t + 1]; ++q) wait_geq(xdone + V.tgt[q], 1, err, 3);
+    if (T.kind == 0) wait_geq(cdone + s, V.nchunk[s] - (nr > 0 ? 1 : 0), err, 4);
+  }
+  __syncthreads();
+  double* zx = zs + (T.kind == 0 ? kSnCols * nrhs : 0);  // chunk rows live after the diagonal block
+  if (nr > 0) {
+    for (int idx = tid; idx < nr * nrhs; idx += blockDim.x) {
+      const int ii = idx / nrhs, col = idx % nrhs;
+      zx[idx] = __ldcg(x + (int64_t)V.sn_rows[rp + T.r0 + ii] * nrhs + col);
+    }
+    __syncthreads();
+    if (nrhs == 1) {
+      fin_bwd(R, zx, c, nr, seg);
+      __syncthreads();
+    }
+  }
+  if (T.kind == 1) {
+    const int chunk = T.r0 / kChunkRows;
+    double* pp = V.part + (V.part_off[s] + (int64_t)chunk * c) * nrhs;
+    if (nrhs == 1) {
+      for (int j = tid; j < c; j += blockDim.x) pp[j] = (seg[0][j] + seg[1][j]) + (seg[2][j] + seg[3][j]);
+    } else {
+      for (int j = warp; j < c; j += nw) {
+        const double* colp = P + (int64_t)j * ld + c + T.r0;
+        for (int col = 0; col < nrhs; ++col) {
+          double acc = 0.0;
+          for (int ii = lane; ii < nr; ii += 32) acc += __ldg(colp + ii) * zx[ii * nrhs + col];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+          if (lane == 0) pp[j * nrhs + col] = acc;
+        }
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) atomicAdd(cdone + s, 1);
+  } else {
+    // z = y_s - (first chunk, computed here) - (other chunks, in order)
+    const int nch = V.nchunk[s];
+    const double* pp = V.part + V.part_off[s] * nrhs;
+    if (nrhs == 1) {
+      for (int j = tid; j < c; j += blockDim.x) {
+        double v = __ldcg(x + f + j);
+        if (nr > 0) v -= (seg[0][j] + seg[1][j]) + (seg[2][j] + seg[3][j]);
+        for (int q = 1; q < nch; ++q) v -= __ldcg(pp + (int64_t)q * c + j);
+        zs[j] = v;
+      }
+    } else {
+      for (int idx = tid; idx < c * nrhs; idx += blockDim.x) {
+        const int j = idx / nrhs, col = idx % nrhs;
+        double v = __ldcg(x + (int64_t)f * nrhs + idx);
+        if (nr > 0) {
+          double a = 0.0;
+          for (int ii = 0; ii < nr; ++ii) a += __ldg(P + (int64_t)j * ld + c + ii) * zx[ii * nrhs + col];
+          v -= a;
+        }
+        for (int q = 1; q < nch; ++q) v -= __ldcg(pp + (int64_t)q * c * nrhs + idx);
+        zs[idx] = v;
+      }
+    }
+    __syncthreads();
+    diag_solve(D, rinv, zs, c, nrhs, false);
+    for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = zs[idx];
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) atomicExch(xdone + s, 1);
+  }
+}
+
 __global__ void __launch_bounds__(kSolveThreads) k_bwd_persistent(
     int ntask, const SolveTask* __restrict__ tasks, const int* __restrict__ sn_first,
     const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows, const int64_t* __restrict__ Lptr,
@@ -275,98 +373,68 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_persistent(
   __shared__ double seg[4][kSnCols];
   extern __shared__ double zs[];  // max(c, chunk rows) x nrhs
   __shared__ int task_id;
-  int* cdone = sync + 2 * nsn;
-  int* xdone = sync + 3 * nsn;
   int* counter = sync + 4 * nsn + 1;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const SweepView V{tasks, sn_first, rows_ptr, sn_rows, Lptr, Lbase, x, own_ptr, own, nullptr,
+                    nchunk, part_off, part, sync, nsn, ntask};
   const double* Lb = *Lbase;
   for (;;) {
-    if (tid == 0) task_id = atomicAdd(counter, 1);
+    if (threadIdx.x == 0) task_id = atomicAdd(counter, 1);
     __syncthreads();
     const int t = task_id;
     __syncthreads();
     if (t >= ntask) break;
-    const SolveTask T = tasks[t];
-    const int s = T.s;
-    const int f = sn_first[s];
-    const int c = sn_first[s + 1] - f;
-    const int64_t rp = rows_ptr[s];
-    const int64_t r = rows_ptr[s + 1] - rp;
-    const int64_t ld = c + r;
-    const double* P = Lb + Lptr[s];
-    const int nr = T.r1 - T.r0;
-    BwdRegs R;
-    if (nrhs == 1 && nr > 0) pre_bwd(R, P, c, ld, T.r0, nr);
-    if (T.kind == 0) load_diag(D, rinv, P, c, ld);
-    // the chunk's rows need their owners' x; the diagonal task also its other chunks
-    if (tid == 0) {
-      for (int q = own_ptr[t]; q < own_ptr[t + 1]; ++q) wait_geq(xdone + own[q], 1, err, 3);
-      if (T.kind == 0) wait_geq(cdone + s, nchunk[s] - (nr > 0 ? 1 : 0), err, 4);
-    }
+    bwd_task(V, t, Lb, nrhs, err, D, rinv, seg, zs);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Many models at once (one right-hand side each): the persistent sweeps over
+// the merged task list of all models.  `order` holds (model, task) pairs,
+// each model's tasks in its own dependency order, so every wait still targets
+// a task claimed earlier; tasks of models whose flag in `active` is 0 are
+// skipped.  The dependency chains of the models overlap, which fills the GPU
+// where one small model alone leaves most SMs waiting.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSolveThreads, 3) k_fwd_models(int ntotal, const int2* __restrict__ order,
+                                                               const SweepView* __restrict__ views,
+                                                               const int* __restrict__ active, int* counter,
+                                                               int* err) {
+  __shared__ double D[kSnCols][kSnCols + 1];
+  __shared__ double rinv[kSnCols];
+  __shared__ double ys[kSnCols];
+  __shared__ int task_id;
+  for (;;) {
+    if (threadIdx.x == 0) task_id = atomicAdd(counter, 1);
     __syncthreads();
-    double* zx = zs + (T.kind == 0 ? kSnCols * nrhs : 0);  // chunk rows live after the diagonal block
-    if (nr > 0) {
-      for (int idx = tid; idx < nr * nrhs; idx += blockDim.x) {
-        const int ii = idx / nrhs, col = idx % nrhs;
-        zx[idx] = __ldcg(x + (int64_t)sn_rows[rp + T.r0 + ii] * nrhs + col);
-      }
-      __syncthreads();
-      if (nrhs == 1) {
-        fin_bwd(R, zx, c, nr, seg);
-        __syncthreads();
-      }
-    }
-    if (T.kind == 1) {
-      const int chunk = T.r0 / kChunkRows;
-      double* pp = part + (part_off[s] + (int64_t)chunk * c) * nrhs;
-      if (nrhs == 1) {
-        for (int j = tid; j < c; j += blockDim.x) pp[j] = (seg[0][j] + seg[1][j]) + (seg[2][j] + seg[3][j]);
-      } else {
-        for (int j = warp; j < c; j += nw) {
-          const double* colp = P + (int64_t)j * ld + c + T.r0;
-          for (int col = 0; col < nrhs; ++col) {
-            double acc = 0.0;
-            for (int ii = lane; ii < nr; ii += 32) acc += __ldg(colp + ii) * zx[ii * nrhs + col];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) pp[j * nrhs + col] = acc;
-          }
-        }
-      }
-      __threadfence();
-      __syncthreads();
-      if (tid == 0) atomicAdd(cdone + s, 1);
-    } else {
-      // z = y_s - (first chunk, computed here) - (other chunks, in order)
-      const int nch = nchunk[s];
-      const double* pp = part + part_off[s] * nrhs;
-      if (nrhs == 1) {
-        for (int j = tid; j < c; j += blockDim.x) {
-          double v = __ldcg(x + f + j);
-          if (nr > 0) v -= (seg[0][j] + seg[1][j]) + (seg[2][j] + seg[3][j]);
-          for (int q = 1; q < nch; ++q) v -= __ldcg(pp + (int64_t)q * c + j);
-          zs[j] = v;
-        }
-      } else {
-        for (int idx = tid; idx < c * nrhs; idx += blockDim.x) {
-          const int j = idx / nrhs, col = idx % nrhs;
-          double v = __ldcg(x + (int64_t)f * nrhs + idx);
-          if (nr > 0) {
-            double a = 0.0;
-            for (int ii = 0; ii < nr; ++ii) a += __ldg(P + (int64_t)j * ld + c + ii) * zx[ii * nrhs + col];
-            v -= a;
-          }
-          for (int q = 1; q < nch; ++q) v -= __ldcg(pp + (int64_t)q * c * nrhs + idx);
-          zs[idx] = v;
-        }
-      }
-      __syncthreads();
-      diag_solve(D, rinv, zs, c, nrhs, false);
-      for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = zs[idx];
-      __threadfence();
-      __syncthreads();
-      if (tid == 0) atomicExch(xdone + s, 1);
-    }
+    const int t = task_id;
+    __syncthreads();
+    if (t >= ntotal) break;
+    const int2 mt = order[t];
+    if (!active[mt.x]) continue;
+    const SweepView V = views[mt.x];
+    fwd_task(V, mt.y, *V.Lbase, 1, err, D, rinv, ys);
+  }
+}
+
+__global__ void __launch_bounds__(kSolveThreads, 3) k_bwd_models(int ntotal, const int2* __restrict__ order,
+                                                               const SweepView* __restrict__ views,
+                                                               const int* __restrict__ active, int* counter,
+                                                               int* err) {
+  __shared__ double D[kSnCols][kSnCols + 1];
+  __shared__ double rinv[kSnCols];
+  __shared__ double seg[4][kSnCols];
+  __shared__ double zs[kSnCols + kChunkRows];
+  __shared__ int task_id;
+  for (;;) {
+    if (threadIdx.x == 0) task_id = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = task_id;
+    __syncthreads();
+    if (t >= ntotal) break;
+    const int2 mt = order[t];
+    if (!active[mt.x]) continue;
+    const SweepView V = views[mt.x];
+    bwd_task(V, mt.y, *V.Lbase, 1, err, D, rinv, seg, zs);
   }
 }
 
@@ -1031,6 +1099,37 @@ void launch_two_error(temf_ctx& c, const double* a, const double* b, int nrhs, d
   k_err_partial<<<kErrBlocks, 256, 0, st>>>(c.pat.n, nrhs, a, b, partials);
   TEMF_CHECK_LAUNCH();
   k_err_final<<<ceil_div(nrhs, 64), 64, 0, st>>>(kErrBlocks, nrhs, partials, out);
+  TEMF_CHECK_LAUNCH();
+}
+
+// --- many models at once -----------------------------------------------------
+SweepView fwd_view(temf_ctx& c, double* const* Lbase, double* x, int* sync) {
+  FactorPlan& F = c.fplan;
+  SolvePlan& P = c.splan;
+  return SweepView{P.ftask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x, P.ftgt_ptr.p,
+                   P.ftgt.p, P.fexpect.p, nullptr, nullptr, nullptr, sync, P.nsn, P.n_ftask};
+}
+
+SweepView bwd_view(temf_ctx& c, double* const* Lbase, double* x, int* sync) {
+  FactorPlan& F = c.fplan;
+  SolvePlan& P = c.splan;
+  ensure_update_buffer(c, 1);
+  return SweepView{P.btask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x, P.btgt_ptr.p,
+                   P.btgt.p, nullptr, P.nchunk.p, P.part_off.p, c.d_part.p, sync, P.nsn, P.n_btask};
+}
+
+int models_grid(bool forward) {
+  return forward ? persistent_grid(k_fwd_models, 0) : persistent_grid(k_bwd_models, 0);
+}
+
+void launch_solve_models(int nf, const int2* order_f, const SweepView* vf, int nb, const int2* order_b,
+                         const SweepView* vb, const int* active, int* counters, int* err, int grid_f, int grid_b,
+                         cudaStream_t st) {
+  k_fwd_models<<<std::max(1, std::min(grid_f, nf)), kSolveThreads, 0, st>>>(nf, order_f, vf, active, counters,
+                                                                              err);
+  TEMF_CHECK_LAUNCH();
+  k_bwd_models<<<std::max(1, std::min(grid_b, nb)), kSolveThreads, 0, st>>>(nb, order_b, vb, active, counters + 1,
+                                                                              err);
   TEMF_CHECK_LAUNCH();
 }
 

@@ -2,6 +2,28 @@
 #include "ctx.h"
 
 namespace temf {
+// One model's view for the persistent sweeps: its schedule, factor and
+// right-hand side.  The single-model kernels build it from their arguments;
+// the multi-model kernels read one per task from a device array.
+struct SweepView {
+  const SolveTask* tasks;
+  const int* sn_first;
+  const int64_t* rows_ptr;
+  const int* sn_rows;
+  const int64_t* Lptr;
+  double* const* Lbase;
+  double* x;
+  const int* tgt_ptr;      // forward: supernodes each task's rows feed; backward: owners of its rows
+  const int* tgt;
+  const int* expect;       // forward: chunk tasks feeding each supernode
+  const int* nchunk;       // backward: row chunks per supernode
+  const int64_t* part_off; // backward: partial-sum offsets
+  double* part;
+  int* sync;               // ready | ydone | cdone | xdone (nsn each) | counters
+  int nsn;
+  int ntask;
+};
+
 void build_solve_plan(temf_ctx& c);
 void ensure_update_buffer(temf_ctx& c, int nrhs);
 
@@ -32,4 +54,17 @@ inline size_t two_error_len(int nrhs) { return (size_t)(1 + 296) * 2 * nrhs; }
 void launch_two_error(temf_ctx& c, const double* a, const double* b, int nrhs, double* out, cudaStream_t st);
 // plain y = M x (full symmetric)
 void launch_spmv(temf_ctx& c, const double* M, const double* x, double* y, int nrhs, cudaStream_t st);
+
+// Many models at once: views of one model's sweeps (the forward view carries
+// the forward schedule, the backward view the backward one; `sync` is that
+// model's 4*nsn+4 words, cleared by the caller before each solve), the
+// number of CTAs the merged kernels keep resident, and the launch of one
+// forward and one backward merged sweep over (model, task) lists.  counters:
+// two claim counters, cleared by the caller; err: timeout word.
+SweepView fwd_view(temf_ctx& c, double* const* Lbase, double* x, int* sync);
+SweepView bwd_view(temf_ctx& c, double* const* Lbase, double* x, int* sync);
+int models_grid(bool forward);
+void launch_solve_models(int nf, const int2* order_f, const SweepView* vf, int nb, const int2* order_b,
+                         const SweepView* vb, const int* active, int* counters, int* err, int grid_f, int grid_b,
+                         cudaStream_t st);
 }  // namespace temf

@@ -214,6 +214,10 @@ class FetdGPU:
         self._ck(self._L.temf_run(self._h, int(sp_division), int(sp_double), int(sp_dblesize), float(time_maximum),
                                   flags, iptr(f) if f is not None else None, len(f) if f is not None else 0,
                                   int(max_steps)), "temf_run")
+        return self.result()
+
+    def result(self) -> RunOutput:
+        """Output of the last run of this context (temf_run or a batch run)."""
         rows = C.c_int(0)
         self._ck(self._L.temf_result_rows(self._h, C.byref(rows)), "temf_result_rows")
         R = rows.value
@@ -290,6 +294,62 @@ class FetdGPU:
 
     def pardiso_dealloc(self) -> None:
         self._ck(self._L.temf_pardiso_dealloc(self._h), "temf_pardiso_dealloc")
+
+
+class FetdBatch:
+    """Several prepared models stepped together on one GPU (temf_batch_*):
+    one merged forward and one merged backward solve kernel per step."""
+
+    def __init__(self, models: Sequence[FetdGPU]):
+        self._L = lib()
+        self.models = list(models)
+        arr = (C.c_void_p * len(self.models))(*[m._h for m in self.models])
+        h = C.c_void_p()
+        rc = self._L.temf_batch_create(arr, len(self.models), C.byref(h))
+        self._h = h
+        if rc < 0:
+            msg = self._L.temf_batch_last_error(h).decode()
+            self.close()
+            raise TemfError(rc, "temf_batch_create: " + msg)
+
+    def _ck(self, rc: int, what: str) -> int:
+        if rc < 0:
+            raise TemfError(rc, "%s: %s" % (what, self._L.temf_batch_last_error(self._h).decode()))
+        return rc
+
+    def close(self) -> None:
+        if self._h:
+            self._L.temf_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def run(self, sp_division: int, sp_double: int, sp_dblesize: int, time_maximum: float,
+            legacy_linux: bool = False, graphs: bool = True, autotune: bool = False, max_steps: int = 0):
+        flags = (1 if legacy_linux else 0) | (0 if graphs else 2) | (4 if autotune else 0)
+        self._ck(self._L.temf_batch_run(self._h, int(sp_division), int(sp_double), int(sp_dblesize),
+                                        float(time_maximum), flags, int(max_steps)), "temf_batch_run")
+        return [m.result() for m in self.models]
+
+    def timing(self) -> Dict[str, float]:
+        ms = np.zeros(4)
+        cnt = (C.c_longlong * 3)()
+        self._ck(self._L.temf_batch_timing(self._h, dptr(ms), cnt), "temf_batch_timing")
+        return dict(ms_total=float(ms[0]), ms_factor=float(ms[1]), ms_steps=float(ms[2]), ms_tune=float(ms[3]),
+                    steps=int(cnt[0]), launches=int(cnt[1]), merged_solves=int(cnt[2]))
+
+    def tuning(self):
+        o, g = C.c_int(0), C.c_int(0)
+        cand = np.zeros(6)
+        tuned = self._ck(self._L.temf_batch_tuning(self._h, C.byref(o), C.byref(g), dptr(cand)), "temf_batch_tuning")
+        return dict(tuned=bool(tuned), order=o.value, grid_pct=g.value, candidate_ms=cand.tolist())
+
+    def set_tuning(self, order: int, grid_pct: int) -> None:
+        self._ck(self._L.temf_batch_set_tuning(self._h, int(order), int(grid_pct)), "temf_batch_set_tuning")
 
 
 def load_case(gpu: FetdGPU, mesh: meshio.Mesh, ctl: meshio.Control, rec_tet: Optional[np.ndarray] = None):
