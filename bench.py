@@ -202,6 +202,59 @@ def batched_measure(local: int, max_steps: int):
     return out
 
 
+def layered_models(n_models: int = 16, seed: int = 5):
+    """Independent 1-D layered models (3-6 layers, conductivities log-uniform
+    in [1e-4, 1e-1] S/m, thicknesses log-uniform in [10, 300] m) on graded
+    meshes of uneven size (mesh density drawn log-uniformly; about 0.1M to
+    0.7M edges)."""
+    from temf3dt_b200 import synth
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_models):
+        sc = float(np.exp(rng.uniform(np.log(0.3), np.log(0.9))))
+        kw = dict(COMMON)
+        out.append(synth.build_model("layered", seed=100 + i, scale=sc, ratio=2.0, **kw))
+    return out
+
+
+def models_measure(local: int, n_models: int = 16):
+    """The layered models one after another (plain runs) against all of them
+    in one lockstep batch with merged solve kernels (autotuned schedule).
+    Unit: model time steps per second of the whole job."""
+    from temf3dt_b200 import fetd
+    models = layered_models(n_models)
+    gs = []
+    try:
+        for m in models:
+            g = fetd.FetdGPU(local)
+            gs.append(g)
+            fetd.load_case(g, m.mesh, m.ctl)
+        c = models[0].ctl
+        args = (c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum)
+        seq_ms, seq_steps = 0.0, 0
+        for g in gs:
+            g.run(*args)
+            o = g.run(*args)
+            seq_ms += o.ms_total
+            seq_steps += len(o.steps) - 1
+        with fetd.FetdBatch(gs) as b:
+            b.run(*args, autotune=True)
+            outs = b.run(*args)
+            tm = b.timing()
+            tu = b.tuning()
+        bat_steps = sum(len(o.steps) - 1 for o in outs)
+        sizes = [int(g.stats()["n"]) for g in gs]
+    finally:
+        for g in gs:
+            g.close()
+    seq = seq_steps / (seq_ms / 1e3)
+    bat = bat_steps / (tm["ms_total"] / 1e3)
+    return {"value": bat, "unit": "model-steps/s", "sequential_value": seq, "batch_over_sequential": bat / seq,
+            "n_models": n_models, "edges_min": min(sizes), "edges_max": max(sizes), "edges_total": sum(sizes),
+            "ms_batch": tm["ms_total"], "ms_sequential": seq_ms, "batch_factor_ms": tm["ms_factor"],
+            "merged_solves": tm["merged_solves"], "tuning": tu}
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -317,6 +370,9 @@ def ours(args):
     adj = None
     if cfg != 2 and args.adjoint:
         adj = adjoint_measure(g, m, one_run, outs[-1].ms_total)
+    models = None
+    if cfg == 2 and args.models > 0 and world == 1:
+        models = models_measure(local, args.models)
     batched = None
     if cfg == 1 and args.batched_steps > 0 and world == 1:
         batched = batched_measure(local, args.batched_steps)
@@ -373,6 +429,7 @@ def ours(args):
         "batched_over_plain": (value / world / plain["value"]) if plain else None,
         "adjoint": adj,
         "batched": batched,
+        "models": models,
         "phases_ms_per_run": {"factor": o.ms_factor, "steps": o.ms_steps, "total": o.ms_total,
                               "factor_each": ms_fac, "solve_step_each": ms_step, "setup_s": t_setup},
     }
@@ -394,6 +451,8 @@ def main():
     ap.add_argument("--sample-steps", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--adjoint", type=int, default=1, help="1: also time one adjoint gradient (single-RHS configs)")
+    ap.add_argument("--models", type=int, default=16,
+                    help="config 2: also run this many layered models one by one and as one batch")
     ap.add_argument("--batched-steps", type=int, default=300,
                     help="config 1: also compare a 64-RHS block with one RHS on the config-2 mesh over these steps")
     args = ap.parse_args()

@@ -173,6 +173,28 @@ int temf_result_gates(temf_ctx* ctx, int n_gates, const double* gates, double* f
 int temf_result_timing(temf_ctx* ctx, double* ms_factor, double* ms_steps, double* ms_total, int* n_factor,
                        int* n_solve, long long* n_launch);
 
+/* ---- sweep schedule autotuner ------------------------------------------------
+ * No reference counterpart.  The persistent triangular-solve sweeps hand the
+ * supernodes below a split level (counted from the leaves) to CTAs through a
+ * ready queue, and claim the ones above it in schedule order with their panel
+ * copies issued before the dependency waits.  temf_tune_solve times one solve
+ * of nrhs columns (right-hand side all ones; nrhs > 1 tunes the 64-column
+ * block sweeps) with the factor in slot 1 or 2 for up to 8 candidate levels
+ * and keeps the fastest; temf_run tunes once on its first factorisation if
+ * nothing was tuned since temf_analyse.  cand_split/cand_ms (may be NULL)
+ * receive the candidates.  temf_solve_schedule reports the level in use. */
+int temf_tune_solve(temf_ctx* ctx, int slot, int nrhs, int* split, int* n_cand, int* cand_split, double* cand_ms);
+int temf_solve_schedule(temf_ctx* ctx, int nrhs, int* split, int* tuned);
+
+/* ---- profiling aid -------------------------------------------------------------
+ * No reference counterpart.  One single-column solve (right-hand side all
+ * ones) with the factor in slot 1 or 2, recording per task of the persistent
+ * sweeps: start, dependency satisfied, end (GPU global timer, ns), SM id,
+ * supernode, kind (0 diagonal, 1 row chunk), first row, supernode level --
+ * 8 words per task, the n_fwd forward tasks first, then the n_bwd backward
+ * ones.  With out = NULL only the counts are returned. */
+int temf_solve_timeline(temf_ctx* ctx, int slot, long long cap, unsigned long long* out, int* n_fwd, int* n_bwd);
+
 /* ---- adjoint gradient --------------------------------------------------------
  * No reference counterpart: the reference's inversion module (inv_modeling)
  * ships only as compiled objects.  These entries give the gradient of a
@@ -242,6 +264,12 @@ int temf_analysis_stats(temf_ctx* ctx, double* stats);
  * symbolic, structural nnz(L) (sum of column counts). */
 int temf_symbolic_host(int n, const long long* xadj, const int* adj, const double* xyz, int* perm_out,
                        double* stats);
+
+/* Host-only check of the triangular-solve schedules built from the same
+ * analysis (no GPU needed; no reference counterpart): replays both sweeps,
+ * claimed in order and through the ready queue, for both chunk heights.
+ * Returns 0, or 1 with the first violation in msg. */
+int temf_schedule_check(int n, const long long* xadj, const int* adj, const double* xyz, char* msg, int msg_len);
 
 /* ---- PARDISO-compatible shim ------------------------------------------------
  * Same argument meaning as the reference's module pardiso_multi_real_mpi

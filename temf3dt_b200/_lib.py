@@ -51,6 +51,10 @@ SIGNATURES = {
     "temf_analysis_stats": (_i, [_p, _dp]),
     "temf_symbolic_host": (_i, [_i, C.POINTER(C.c_longlong), _ip, _dp, _ip, _dp]),
     "temf_adjoint_record": (_i, [_p, _i]),
+    "temf_tune_solve": (_i, [_p, _i, _i, _ip, _ip, _ip, _dp]),
+    "temf_solve_schedule": (_i, [_p, _i, _ip, _ip]),
+    "temf_schedule_check": (_i, [_i, C.POINTER(C.c_longlong), _ip, _dp, C.c_char_p, _i]),
+    "temf_solve_timeline": (_i, [_p, _i, C.c_longlong, C.POINTER(C.c_ulonglong), _ip, _ip]),
     "temf_batch_create": (_i, [C.POINTER(C.c_void_p), _i, C.POINTER(C.c_void_p)]),
     "temf_batch_destroy": (_i, [_p]),
     "temf_batch_last_error": (C.c_char_p, [_p]),

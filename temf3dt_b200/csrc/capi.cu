@@ -907,6 +907,54 @@ int temf_batch_set_tuning(temf_batch* B, int order, int grid_pct) {
   });
 }
 
+int temf_tune_solve(temf_ctx* c, int slot, int nrhs, int* split, int* n_cand, int* cand_split, double* cand_ms) {
+  return guarded(c, [&] {
+    if (slot != 1 && slot != 2) throw ArgError("slot must be 1 or 2");
+    if (nrhs < 1) throw ArgError("nrhs must be >= 1");
+    need(c->slots[slot - 1].valid, "temf_tune_solve: the slot holds no valid factor");
+    clear_solve_error_flag(*c);
+    const int best = tune_solve(*c, slot - 1, nrhs);
+    if (const int fl = solve_error_flag(*c)) {
+      clear_solve_error_flag(*c);
+      throw StateError("a triangular-solve wait timed out while tuning (code " + std::to_string(fl) + ")");
+    }
+    const QueuePlan& Q = nrhs > 1 ? c->splan.qm : c->splan.q1;
+    if (split) *split = best;
+    if (n_cand) *n_cand = (int)Q.tune_ms.size();
+    for (size_t i = 0; i < Q.tune_ms.size(); ++i) {
+      if (cand_split) cand_split[i] = Q.tune_split[i];
+      if (cand_ms) cand_ms[i] = Q.tune_ms[i];
+    }
+    return TEMF_OK;
+  });
+}
+
+int temf_solve_schedule(temf_ctx* c, int nrhs, int* split, int* tuned) {
+  return guarded(c, [&] {
+    need(c->analysed, "temf_solve_schedule: call temf_analyse first");
+    const QueuePlan& Q = nrhs > 1 ? c->splan.qm : c->splan.q1;
+    if (split) *split = Q.split;
+    if (tuned) *tuned = Q.tuned ? 1 : 0;
+    return TEMF_OK;
+  });
+}
+
+int temf_solve_timeline(temf_ctx* c, int slot, long long cap, unsigned long long* out, int* n_fwd, int* n_bwd) {
+  return guarded(c, [&] {
+    if (slot != 1 && slot != 2) throw ArgError("slot must be 1 or 2");
+    need(c->slots[slot - 1].valid, "temf_solve_timeline: the slot holds no valid factor");
+    if (!n_fwd || !n_bwd) throw ArgError("NULL");
+    std::vector<double> ones(c->n_edges, 1.0);
+    clear_solve_error_flag(*c);
+    solve_timeline(*c, slot - 1, ones.data(), cap, out, n_fwd, n_bwd);
+    if (const int fl = solve_error_flag(*c)) {
+      clear_solve_error_flag(*c);
+      throw StateError("a triangular-solve wait timed out (code " + std::to_string(fl) + ")");
+    }
+    return TEMF_OK;
+  });
+}
+
 int temf_adjoint_record(temf_ctx* c, int checkpoint_every) {
   return guarded(c, [&] {
     if (checkpoint_every < 0) throw ArgError("checkpoint_every must be >= 0");
@@ -1007,6 +1055,25 @@ int temf_symbolic_host(int n, const long long* xadj, const int* adj, const doubl
       stats[8] = (double)S.nnzL_exact;
     }
     return TEMF_OK;
+  } catch (...) {
+    return TEMF_EINTERNAL;
+  }
+}
+
+int temf_schedule_check(int n, const long long* xadj, const int* adj, const double* xyz, char* msg, int msg_len) {
+  if (n <= 0 || !xadj || !adj || !xyz) return TEMF_EARG;
+  try {
+    std::vector<int64_t> xa(xadj, xadj + n + 1);
+    SymbolicOptions o;
+    o.max_sn_cols = kSnCols;
+    Symbolic S;
+    analyse(n, xa.data(), adj, xyz, o, S);
+    const std::string w = check_schedules(S);
+    if (msg && msg_len > 0) {
+      std::strncpy(msg, w.c_str(), msg_len - 1);
+      msg[msg_len - 1] = 0;
+    }
+    return w.empty() ? TEMF_OK : 1;
   } catch (...) {
     return TEMF_EINTERNAL;
   }

@@ -61,6 +61,24 @@ struct SolveTask {
   int r1;
 };
 
+// Ready-queue scheduling of a pair of sweep schedules: diagonal task per
+// supernode (forward, backward), backward dependants and completion counts,
+// initially ready tasks (stored as task + 1), and the per-solve queue words
+// [fq: n_ftask][bq: n_btask][bcnt: n_btask][fhead, bhead, ftail, btail].
+// The queue serves the supernodes below `split` (levels from the leaves); the
+// tasks above it are claimed in schedule order with their panels prefetched
+// before the dependency waits (forward tasks [0, f_hi), backward [b_lo, nb)
+// are queued).
+struct QueuePlan {
+  DBuf<int> fdiag, bdiag, bdep_ptr, bdep, bneed, finit, binit, qtails;
+  int n_finit = 0, n_binit = 0;
+  int split = 0, f_hi = 0, b_lo = 0;
+  bool tuned = false;
+  std::vector<double> tune_ms;  // per candidate split, when tuned
+  std::vector<int> tune_split;
+  DBuf<int> qbuf;
+};
+
 struct SolvePlan {
   int64_t u_len = 0;           // sum over supernodes of the rows below the diagonal block
   // persistent schedules (tasks in an order where every wait targets an earlier task)
@@ -72,12 +90,14 @@ struct SolvePlan {
   DBuf<int> nchunk;            // per supernode: row chunks of its panel
   DBuf<int64_t> part_off;      // per supernode: offset of its backward partial sums
   int64_t part_len = 0;
+  QueuePlan q1;                // ready-queue data of the schedules above
   // the same schedules with 64-row chunks for blocks of up to 64 right-hand sides
   DBuf<SolveTask> mftask, mbtask;
   int n_mftask = 0, n_mbtask = 0;
   DBuf<int> mftgt_ptr, mftgt, mfexpect, mbtgt_ptr, mbtgt, mnchunk;
   DBuf<int64_t> macc_off;      // per supernode with >= 2 chunks: row offset of its c x 64 accumulator
   int64_t macc_len = 0;
+  QueuePlan qm;
   DBuf<int> sync;              // ready | ydone | cdone | xdone (nsn each) | counters
   int nsn = 0;
 };

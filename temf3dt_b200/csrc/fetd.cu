@@ -338,6 +338,8 @@ struct Engine {
         cur = 0;
         factor(0, step_cur);
         set_current(0);
+        // first solve on this analysis: pick the sweep schedule (once)
+        if (!(nrhs > 1 ? c.splan.qm.tuned : c.splan.q1.tuned)) tune_solve(c, 0, nrhs);
         N = 0;
         e1 = E(1);
       }

@@ -31,6 +31,22 @@ constexpr int kChunkRowsMulti = 64;    // rows per task when solving blocks of r
 constexpr int kMultiCols = 64;         // right-hand sides per block
 constexpr int kSpinLimit = 1 << 22;    // bounded waits: ~seconds, then the error flag
 
+// Optional per-task timeline of the single-model sweeps (profiling aid; null
+// unless temf_solve_timeline is running): per task start, dependency
+// satisfied, end (global ns timer) and SM id.
+__device__ unsigned long long* g_timeline_f = nullptr;
+__device__ unsigned long long* g_timeline_b = nullptr;
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned smid() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+  return r;
+}
+
 // Bounded wait until *flag >= target (written by other CTAs of the same
 // kernel).  Polls tightly first, then with a short sleep.  On timeout the
 // error word is set and the wait gives up, so the kernel always terminates;
@@ -177,6 +193,67 @@ __device__ __forceinline__ void fin_bwd(const BwdRegs& R, const double* zs, int 
   }
 }
 
+// Ready queue: a task is appended once every task it depends on has finished
+// (the finishing task that completes its count appends it), and CTAs pop
+// tasks in the order they became ready, so no CTA holds a task that is still
+// waiting for its inputs.  Slots hold task + 1 (0 = not yet written).
+__device__ __forceinline__ bool in_queue(const SweepView& V, int task) {
+  return V.queue != nullptr && task >= V.q_lo && task < V.q_hi;
+}
+__device__ __forceinline__ void q_push(const SweepView& V, int task) {
+  if (!in_queue(V, task)) return;  // claimed in schedule order instead
+  const int pos = atomicAdd(V.qtail, 1);
+  atomicExch(V.queue + pos, task + 1);
+}
+// thread 0 only: next ready task, or -1 when all ntask tasks are handed out
+// (or a wait timed out: error word set)
+__device__ __forceinline__ int q_pop(const SweepView& V, int* err) {
+  const int idx = atomicAdd(V.qhead, 1);
+  if (idx >= V.q_hi - V.q_lo) return -1;
+  const volatile int* slot = V.queue + idx;
+  int it = 0, v;
+  while ((v = *slot) == 0) {
+    if (++it > kSpinLimit) {
+      atomicExch(err, 5);
+      return -1;
+    }
+    if (it > 256) __nanosleep(64);
+  }
+  __threadfence();
+  return v - 1;
+}
+
+// Next task of this CTA (every thread gets it; -1 when done).  Two phases:
+// the queue range through the ready queue, and the other tasks claimed in
+// schedule order from `counter` (with dependency waits).  Forward sweeps run
+// the queue phase first (their queue range is the bottom of the tree, at the
+// start of the schedule), backward sweeps last.  Without a queue every task
+// is claimed in order.
+__device__ __forceinline__ int next_task(const SweepView& V, int* counter, bool queue_first, int* err, int& phase,
+                                         int* sh) {
+  for (;;) {
+    const bool use_q = (phase == 0) == queue_first;
+    if (threadIdx.x == 0) {
+      int t = -1;
+      if (use_q) {
+        if (V.queue) t = q_pop(V, err);
+      } else {
+        const bool front = V.queue == nullptr || V.q_lo > 0;  // static tasks before the queue range
+        const int lo = front ? 0 : V.q_hi, hi = V.queue == nullptr ? V.ntask : (front ? V.q_lo : V.ntask);
+        const int i = atomicAdd(counter, 1);
+        t = lo + i < hi ? lo + i : -1;
+      }
+      *sh = t;
+    }
+    __syncthreads();
+    const int t = *sh;
+    __syncthreads();
+    if (t >= 0) return t;
+    if (phase == 1) return -1;
+    phase = 1;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // forward  L y = b : persistent, dependency driven
 //   diagonal task of s (with its first row chunk): wait until every chunk that
@@ -187,7 +264,8 @@ __device__ __forceinline__ void fin_bwd(const BwdRegs& R, const double* zs, int 
 //   chunk task (s, r0..r1), r0 >= 128: wait for y_s, push the same way.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double* Lb, int nrhs, int* err,
-                                         double (*D)[kSnCols + 1], double* rinv, double* ys) {
+                                         double (*D)[kSnCols + 1], double* rinv, double* ys,
+                                         unsigned long long* stamp = nullptr) {
   int* ready = V.sync;
   int* ydone = V.sync + V.nsn;
   double* x = V.x;
@@ -205,10 +283,12 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
   const bool row_on = i < T.r1;
   FwdRegs R;
   if (nrhs == 1) pre_fwd(R, Pc, c, ld, i, row_on);
+  const bool queued = in_queue(V, t);
   if (T.kind == 0) {
     load_diag(D, rinv, P, c, ld);
-    if (tid == 0) wait_geq(ready + s, V.expect[s], err, 1);
+    if (tid == 0 && !queued) wait_geq(ready + s, V.expect[s], err, 1);
     __syncthreads();
+    if (stamp && tid == 0) *stamp = gtime();
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) ys[idx] = __ldcg(x + (int64_t)f * nrhs + idx);
     __syncthreads();
     diag_solve(D, rinv, ys, c, nrhs, true);
@@ -216,9 +296,14 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
     __threadfence();
     __syncthreads();
     if (tid == 0) atomicExch(ydone + s, 1);
+    if (V.queue) {  // y_s is out: the other row chunks of s are ready (they follow this task)
+      const int nx = max(1, (int)((r + kChunkRows - 1) / kChunkRows)) - 1;
+      for (int k = tid; k < nx; k += blockDim.x) q_push(V, t + 1 + k);
+    }
   } else {
-    if (tid == 0) wait_geq(ydone + s, 1, err, 2);
+    if (tid == 0 && !queued) wait_geq(ydone + s, 1, err, 2);
     __syncthreads();
+    if (stamp && tid == 0) *stamp = gtime();
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) ys[idx] = __ldcg(x + (int64_t)f * nrhs + idx);
     __syncthreads();
   }
@@ -235,8 +320,14 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
     }
     __threadfence();
     __syncthreads();
-    if (tid == 0)
+    if (V.queue) {
+      for (int q = V.tgt_ptr[t] + tid; q < V.tgt_ptr[t + 1]; q += blockDim.x) {
+        const int o = V.tgt[q];
+        if (atomicAdd(ready + o, 1) == V.expect[o] - 1) q_push(V, V.diag_task[o]);
+      }
+    } else if (tid == 0) {
       for (int q = V.tgt_ptr[t]; q < V.tgt_ptr[t + 1]; ++q) atomicAdd(ready + V.tgt[q], 1);
+    }
   }
 }
 
@@ -259,7 +350,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_persistent(
     const int t = task_id;
     __syncthreads();
     if (t >= ntask) break;
-    fwd_task(V, t, Lb, nrhs, err, D, rinv, ys);
+    unsigned long long* rec = g_timeline_f ? g_timeline_f + 4 * (size_t)t : nullptr;
+    if (rec && threadIdx.x == 0) rec[0] = gtime();
+    fwd_task(V, t, Lb, nrhs, err, D, rinv, ys, rec ? rec + 1 : nullptr);
+    if (rec && threadIdx.x == 0) { rec[2] = gtime(); rec[3] = smid(); }
   }
 }
 
@@ -274,7 +368,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_persistent(
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double* Lb, int nrhs, int* err,
                                          double (*D)[kSnCols + 1], double* rinv, double (*seg)[kSnCols],
-                                         double* zs) {
+                                         double* zs, unsigned long long* stamp = nullptr) {
   int* cdone = V.sync + 2 * V.nsn;
   int* xdone = V.sync + 3 * V.nsn;
   double* x = V.x;
@@ -291,12 +385,14 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
   BwdRegs R;
   if (nrhs == 1 && nr > 0) pre_bwd(R, P, c, ld, T.r0, nr);
   if (T.kind == 0) load_diag(D, rinv, P, c, ld);
+  const bool queued = in_queue(V, t);
   // the chunk's rows need their owners' x; the diagonal task also its other chunks
-  if (tid == 0) {
+  if (tid == 0 && !queued) {
     for (int q = V.tgt_ptr[t]; q < V.tgt_ptr[t + 1]; ++q) wait_geq(xdone + V.tgt[q], 1, err, 3);
     if (T.kind == 0) wait_geq(cdone + s, V.nchunk[s] - (nr > 0 ? 1 : 0), err, 4);
   }
   __syncthreads();
+  if (stamp && tid == 0) *stamp = gtime();
   double* zx = zs + (T.kind == 0 ? kSnCols * nrhs : 0);  // chunk rows live after the diagonal block
   if (nr > 0) {
     for (int idx = tid; idx < nr * nrhs; idx += blockDim.x) {
@@ -328,7 +424,13 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
     }
     __threadfence();
     __syncthreads();
-    if (tid == 0) atomicAdd(cdone + s, 1);
+    if (tid == 0) {
+      atomicAdd(cdone + s, 1);
+      if (V.queue) {
+        const int d = V.diag_task[s];
+        if (atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
+      }
+    }
   } else {
     // z = y_s - (first chunk, computed here) - (other chunks, in order)
     const int nch = V.nchunk[s];
@@ -359,6 +461,11 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
     __threadfence();
     __syncthreads();
     if (tid == 0) atomicExch(xdone + s, 1);
+    if (V.queue)  // x_s is out: count it for every task whose rows s owns
+      for (int q = V.dep_ptr[s] + tid; q < V.dep_ptr[s + 1]; q += blockDim.x) {
+        const int d = V.dep[q];
+        if (atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
+      }
   }
 }
 
@@ -383,7 +490,46 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_persistent(
     const int t = task_id;
     __syncthreads();
     if (t >= ntask) break;
-    bwd_task(V, t, Lb, nrhs, err, D, rinv, seg, zs);
+    unsigned long long* rec = g_timeline_b ? g_timeline_b + 4 * (size_t)t : nullptr;
+    if (rec && threadIdx.x == 0) rec[0] = gtime();
+    bwd_task(V, t, Lb, nrhs, err, D, rinv, seg, zs, rec ? rec + 1 : nullptr);
+    if (rec && threadIdx.x == 0) { rec[2] = gtime(); rec[3] = smid(); }
+  }
+}
+
+// The same sweeps scheduled through the ready queue (single right-hand side).
+__global__ void __launch_bounds__(kSolveThreads) k_fwd_queued(const SweepView V, int* err) {
+  __shared__ double D[kSnCols][kSnCols + 1];
+  __shared__ double rinv[kSnCols];
+  __shared__ double ys[kSnCols];
+  __shared__ int task_id;
+  const double* Lb = *V.Lbase;
+  int phase = 0;
+  for (;;) {
+    const int t = next_task(V, V.sync + 4 * V.nsn, true, err, phase, &task_id);
+    if (t < 0) break;
+    unsigned long long* rec = g_timeline_f ? g_timeline_f + 4 * (size_t)t : nullptr;
+    if (rec && threadIdx.x == 0) rec[0] = gtime();
+    fwd_task(V, t, Lb, 1, err, D, rinv, ys, rec ? rec + 1 : nullptr);
+    if (rec && threadIdx.x == 0) { rec[2] = gtime(); rec[3] = smid(); }
+  }
+}
+
+__global__ void __launch_bounds__(kSolveThreads) k_bwd_queued(const SweepView V, int* err) {
+  __shared__ double D[kSnCols][kSnCols + 1];
+  __shared__ double rinv[kSnCols];
+  __shared__ double seg[4][kSnCols];
+  __shared__ double zs[kSnCols + kChunkRows];
+  __shared__ int task_id;
+  const double* Lb = *V.Lbase;
+  int phase = 0;
+  for (;;) {
+    const int t = next_task(V, V.sync + 4 * V.nsn + 1, false, err, phase, &task_id);
+    if (t < 0) break;
+    unsigned long long* rec = g_timeline_b ? g_timeline_b + 4 * (size_t)t : nullptr;
+    if (rec && threadIdx.x == 0) rec[0] = gtime();
+    bwd_task(V, t, Lb, 1, err, D, rinv, seg, zs, rec ? rec + 1 : nullptr);
+    if (rec && threadIdx.x == 0) { rec[2] = gtime(); rec[3] = smid(); }
   }
 }
 
@@ -582,39 +728,33 @@ __device__ __forceinline__ void diag_solve_block(MultiSmem& M, int c, bool forwa
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kSolveThreads) k_fwd_multi(
-    int ntask, const SolveTask* __restrict__ tasks, const int* __restrict__ sn_first,
-    const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows, const int64_t* __restrict__ Lptr,
-    double* const* Lbase, double* x, int ldx, int k, const int* __restrict__ tgt_ptr, const int* __restrict__ tgt,
-    const int* __restrict__ expect, int* sync, int nsn, int* err) {
+__global__ void __launch_bounds__(kSolveThreads) k_fwd_multi(const SweepView V, int ldx, int k, int* err) {
   extern __shared__ __align__(16) unsigned char smraw[];
   MultiSmem& M = *reinterpret_cast<MultiSmem*>(smraw);
   __shared__ int task_id;
-  int* ready = sync;
-  int* ydone = sync + nsn;
-  int* counter = sync + 4 * nsn;
+  int* ready = V.sync;
+  int* ydone = V.sync + V.nsn;
+  double* x = V.x;
   const int tid = threadIdx.x;
-  const double* Lb = *Lbase;
+  const double* Lb = *V.Lbase;
+  int phase = 0;
   for (;;) {
-    if (tid == 0) task_id = atomicAdd(counter, 1);
-    __syncthreads();
-    const int t = task_id;
-    __syncthreads();
-    if (t >= ntask) break;
-    const SolveTask T = tasks[t];
+    const int t = next_task(V, V.sync + 4 * V.nsn, true, err, phase, &task_id);
+    if (t < 0) break;
+    const SolveTask T = V.tasks[t];
     const int s = T.s;
-    const int f = sn_first[s];
-    const int c = sn_first[s + 1] - f;
-    const int64_t rp = rows_ptr[s];
-    const int64_t r = rows_ptr[s + 1] - rp;
+    const int f = V.sn_first[s];
+    const int c = V.sn_first[s + 1] - f;
+    const int64_t rp = V.rows_ptr[s];
+    const int64_t r = V.rows_ptr[s + 1] - rp;
     const int64_t ld = c + r;
-    const double* P = Lb + Lptr[s];
+    const double* P = Lb + V.Lptr[s];
     const int nr = T.r1 - T.r0;
-    // the factor does not depend on the sweep: start its copies before the waits
+    // the factor does not depend on the sweep: start its copies before any wait
     if (nr > 0) load_panel_block_async(M.A, P, c, ld, T.r0, nr);
     if (T.kind == 0) load_diag_async(M.D, P, c, ld);
-    if (tid == 0) {
-      if (T.kind == 0) wait_geq(ready + s, expect[s], err, 1);
+    if (tid == 0 && !in_queue(V, t)) {  // claimed in order: wait for the inputs
+      if (T.kind == 0) wait_geq(ready + s, V.expect[s], err, 1);
       else wait_geq(ydone + s, 1, err, 2);
     }
     __syncthreads();
@@ -632,6 +772,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_multi(
       __threadfence();
       __syncthreads();
       if (tid == 0) atomicExch(ydone + s, 1);
+      // y_s is out: the other row chunks of s (the tasks right after this one) are ready
+      const int nx = max(1, (int)((r + kChunkRowsMulti - 1) / kChunkRowsMulti)) - 1;
+      for (int q = tid; q < nx; q += blockDim.x) q_push(V, t + 1 + q);
     }
     if (nr > 0) {
       // U = L21[rows] Y_s (64 x 64 x c), then push -U into the rows' right-hand sides
@@ -643,55 +786,50 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_multi(
       __syncthreads();
       const int warp = tid >> 5, lane = tid & 31;
       for (int i = warp; i < nr; i += kSolveThreads / 32) {
-        double* dst = x + (int64_t)sn_rows[rp + T.r0 + i] * ldx;
+        double* dst = x + (int64_t)V.sn_rows[rp + T.r0 + i] * ldx;
         for (int col = lane; col < k; col += 32) atomicAdd(dst + col, -M.A[i * kLdm + col]);
       }
       __threadfence();
       __syncthreads();
-      if (tid == 0)
-        for (int q = tgt_ptr[t]; q < tgt_ptr[t + 1]; ++q) atomicAdd(ready + tgt[q], 1);
+      for (int q = V.tgt_ptr[t] + tid; q < V.tgt_ptr[t + 1]; q += blockDim.x) {
+        const int o = V.tgt[q];
+        if (atomicAdd(ready + o, 1) == V.expect[o] - 1) q_push(V, V.diag_task[o]);
+      }
     }
   }
 }
 
-__global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(
-    int ntask, const SolveTask* __restrict__ tasks, const int* __restrict__ sn_first,
-    const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows, const int64_t* __restrict__ Lptr,
-    double* const* Lbase, double* x, int ldx, int k, const int* __restrict__ own_ptr, const int* __restrict__ own,
-    const int* __restrict__ nchunk, const int64_t* __restrict__ acc_off, double* accum, int* sync, int nsn,
-    int* err) {
+__global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(const SweepView V, int ldx, int k, int* err) {
   extern __shared__ __align__(16) unsigned char smraw[];
   MultiSmem& M = *reinterpret_cast<MultiSmem*>(smraw);
   __shared__ int task_id;
-  int* cdone = sync + 2 * nsn;
-  int* xdone = sync + 3 * nsn;
-  int* counter = sync + 4 * nsn + 1;
+  int* cdone = V.sync + 2 * V.nsn;
+  int* xdone = V.sync + 3 * V.nsn;
+  double* x = V.x;
   const int tid = threadIdx.x;
-  const double* Lb = *Lbase;
+  const double* Lb = *V.Lbase;
+  int phase = 0;
   for (;;) {
-    if (tid == 0) task_id = atomicAdd(counter, 1);
-    __syncthreads();
-    const int t = task_id;
-    __syncthreads();
-    if (t >= ntask) break;
-    const SolveTask T = tasks[t];
+    const int t = next_task(V, V.sync + 4 * V.nsn + 1, false, err, phase, &task_id);
+    if (t < 0) break;
+    const SolveTask T = V.tasks[t];
     const int s = T.s;
-    const int f = sn_first[s];
-    const int c = sn_first[s + 1] - f;
-    const int64_t rp = rows_ptr[s];
-    const int64_t r = rows_ptr[s + 1] - rp;
+    const int f = V.sn_first[s];
+    const int c = V.sn_first[s + 1] - f;
+    const int64_t rp = V.rows_ptr[s];
+    const int64_t r = V.rows_ptr[s + 1] - rp;
     const int64_t ld = c + r;
-    const double* P = Lb + Lptr[s];
+    const double* P = Lb + V.Lptr[s];
     const int nr = T.r1 - T.r0;
     if (nr > 0) load_panel_block_async(M.A, P, c, ld, T.r0, nr);
     if (T.kind == 0) load_diag_async(M.D, P, c, ld);
-    if (tid == 0) {
-      for (int q = own_ptr[t]; q < own_ptr[t + 1]; ++q) wait_geq(xdone + own[q], 1, err, 3);
-      if (T.kind == 0) wait_geq(cdone + s, nchunk[s] - (nr > 0 ? 1 : 0), err, 4);
+    if (tid == 0 && !in_queue(V, t)) {  // claimed in order: wait for the inputs
+      for (int q = V.tgt_ptr[t]; q < V.tgt_ptr[t + 1]; ++q) wait_geq(xdone + V.tgt[q], 1, err, 3);
+      if (T.kind == 0) wait_geq(cdone + s, max(V.nchunk[s], 1) - 1, err, 4);
     }
     __syncthreads();
     // Xr = x[rows] (64 x k); C = L21[rows]^T Xr (c x k)
-    if (nr > 0) load_rows<false>(M.Y, x, ldx, k, nr, 0, sn_rows + rp + T.r0);
+    if (nr > 0) load_rows<false>(M.Y, x, ldx, k, nr, 0, V.sn_rows + rp + T.r0);
     cp_async_wait_all();
     __syncthreads();
     double acc[4][4][2];
@@ -700,7 +838,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(
       mma_tile64(acc, M.A, kLdm, 1, M.Y, 64);
       __syncthreads();
     }
-    double* as = accum + acc_off[s] * kMultiCols;  // this supernode's c x 64 accumulator
+    double* as = V.part + V.part_off[s] * kMultiCols;  // this supernode's c x 64 accumulator
     if (T.kind == 1) {
       store_tile64(acc, M.Y);
       __syncthreads();
@@ -709,13 +847,17 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(
         for (int col = lane; col < k; col += 32) atomicAdd(as + j * kMultiCols + col, M.Y[j * kLdm + col]);
       __threadfence();
       __syncthreads();
-      if (tid == 0) atomicAdd(cdone + s, 1);
+      if (tid == 0) {
+        atomicAdd(cdone + s, 1);
+        const int d = V.diag_task[s];
+        if (atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
+      }
     } else {
       // Z = Y_s - (first chunk, here) - (other chunks, accumulated); back-substitute
       finish_diag(M, c);
       store_tile64(acc, M.A);  // first-chunk products as [j][col]
       __syncthreads();
-      const bool more = nchunk[s] > 1;
+      const bool more = V.nchunk[s] > 1;
       for (int idx = tid; idx < kSnCols * kSnCols; idx += blockDim.x) {
         const int j = idx / kSnCols, col = idx % kSnCols;
         double v = 0.0;
@@ -735,6 +877,11 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(
       __threadfence();
       __syncthreads();
       if (tid == 0) atomicExch(xdone + s, 1);
+      // x_s is out: count it for every task whose rows s owns
+      for (int q = V.dep_ptr[s] + tid; q < V.dep_ptr[s + 1]; q += blockDim.x) {
+        const int d = V.dep[q];
+        if (atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
+      }
     }
   }
 }
@@ -916,6 +1063,178 @@ void build_sched(const Symbolic& S, int CH, Sched& o) {
       o.btp.push_back((int)o.btg.size());
     }
 }
+// Ready-queue data of a schedule: diagonal task per supernode (forward,
+// backward), backward completion counts and dependants, initially ready
+// tasks of both sweeps.
+struct QueueData {
+  std::vector<int> fdiag, bdiag, bneed, dptr, dep, finit, binit;
+};
+
+void build_queue_data(const Sched& a, int nsn, QueueData& q, int f_hi, int b_lo) {
+  q.fdiag.assign(nsn, -1);
+  q.bdiag.assign(nsn, -1);
+  q.bneed.assign(a.bt.size(), 0);
+  for (size_t i = 0; i < a.ft.size(); ++i)
+    if (a.ft[i].kind == 0) q.fdiag[a.ft[i].s] = (int)i;
+  for (size_t i = 0; i < a.bt.size(); ++i)
+    if (a.bt[i].kind == 0) q.bdiag[a.bt[i].s] = (int)i;
+  q.dptr.assign(nsn + 1, 0);
+  for (size_t i = 0; i < a.bt.size(); ++i) {
+    const SolveTask& T = a.bt[i];
+    // owners of its rows, and for a diagonal task its other row chunks
+    q.bneed[i] = (a.btp[i + 1] - a.btp[i]) + (T.kind == 0 ? std::max(a.nch[T.s], 1) - 1 : 0);
+    for (int k = a.btp[i]; k < a.btp[i + 1]; ++k) q.dptr[a.btg[k] + 1]++;
+  }
+  for (int k = 0; k < nsn; ++k) q.dptr[k + 1] += q.dptr[k];
+  q.dep.resize(q.dptr[nsn]);
+  std::vector<int> fill(q.dptr.begin(), q.dptr.end() - 1);
+  for (size_t i = 0; i < a.bt.size(); ++i)
+    for (int k = a.btp[i]; k < a.btp[i + 1]; ++k) q.dep[fill[a.btg[k]]++] = (int)i;
+  q.finit.clear();
+  q.binit.clear();
+  for (int i = 0; i < f_hi; ++i)
+    if (a.ft[i].kind == 0 && a.expect[a.ft[i].s] == 0) q.finit.push_back(i);
+  for (int i = b_lo; i < (int)a.bt.size(); ++i)
+    if (q.bneed[i] == 0) q.binit.push_back(i);
+}
+
+// queue ranges of a split level: forward tasks below it (a prefix of the
+// bottom-up schedule), backward tasks below it (a suffix of the top-down one)
+void split_ranges(const Sched& a, const Symbolic& S, int split, int& f_hi, int& b_lo) {
+  f_hi = 0;
+  while (f_hi < (int)a.ft.size() && S.sn_level[a.ft[f_hi].s] < split) ++f_hi;
+  b_lo = (int)a.bt.size();
+  while (b_lo > 0 && S.sn_level[a.bt[b_lo - 1].s] < split) --b_lo;
+}
+
+// first level (from the leaves) holding fewer than `width` supernodes
+int level_below_width(const Symbolic& S, int width) {
+  for (int l = 0; l < S.nlevels; ++l)
+    if (S.level_ptr[l + 1] - S.level_ptr[l] < width) return l;
+  return S.nlevels;
+}
+int default_split(const Symbolic& S) { return level_below_width(S, 512); }
+
+void upload_queue_plan(const Sched& a, const Symbolic& S, int split, QueuePlan& Q, cudaStream_t st) {
+  const int nsn = S.nsn;
+  int f_hi = 0, b_lo = 0;
+  split_ranges(a, S, split, f_hi, b_lo);
+  QueueData qd;
+  build_queue_data(a, nsn, qd, f_hi, b_lo);
+  Q.split = split;
+  Q.f_hi = f_hi;
+  Q.b_lo = b_lo;
+  auto up = [&](DBuf<int>& d, const std::vector<int>& v) {
+    if (v.empty()) d.alloc(1);
+    else d.upload(v.data(), v.size(), st);
+  };
+  up(Q.fdiag, qd.fdiag);
+  up(Q.bdiag, qd.bdiag);
+  up(Q.bneed, qd.bneed);
+  up(Q.bdep_ptr, qd.dptr);
+  up(Q.bdep, qd.dep);
+  // queue slots hold task + 1 (0 marks a slot not yet written)
+  std::vector<int> fi(qd.finit), bi(qd.binit);
+  for (int& v : fi) ++v;
+  for (int& v : bi) ++v;
+  up(Q.finit, fi);
+  up(Q.binit, bi);
+  Q.n_finit = (int)qd.finit.size();
+  Q.n_binit = (int)qd.binit.size();
+  const int tails[2] = {Q.n_finit, Q.n_binit};
+  Q.qtails.upload(tails, 2, st);
+  Q.qbuf.alloc(a.ft.size() + 2 * a.bt.size() + 4);
+  TEMF_CUDA(cudaStreamSynchronize(st));
+}
+
+// Host replay of both sweeps' protocols for chunk height CH and queue split
+// level `split`: tasks below the split go through the ready queue (handed
+// out once, only after their inputs), the others are claimed in schedule
+// order and must find their inputs complete when every earlier task is.
+// Forward: queue phase, then the ordered phase; backward: the other way
+// round, the ordered tasks' completions feeding the queue.  Returns an empty
+// string or the first violation.
+std::string check_schedule(const Symbolic& S, int CH, int split) {
+  Sched a;
+  build_sched(S, CH, a);
+  int f_hi = 0, b_lo = 0;
+  split_ranges(a, S, split, f_hi, b_lo);
+  QueueData q;
+  build_queue_data(a, S.nsn, q, f_hi, b_lo);
+  const int nsn = S.nsn, nf = (int)a.ft.size(), nb = (int)a.bt.size();
+  {
+    std::vector<int> ready(nsn, 0), ydone(nsn, 0), seen(nf, 0);
+    std::vector<int> queue(q.finit);
+    auto run = [&](int t, bool queued) -> std::string {
+      if (seen[t]++) return "forward: task handed out twice";
+      const SolveTask& T = a.ft[t];
+      if (T.kind == 0) {
+        if (ready[T.s] != a.expect[T.s]) return queued ? "forward queue: diagonal task before its inputs"
+                                                       : "forward: diagonal task claimed before its inputs";
+        ydone[T.s] = 1;
+        const int r = (int)(S.sn_rows_ptr[T.s + 1] - S.sn_rows_ptr[T.s]);
+        const int nx = std::max(1, (r + CH - 1) / CH) - 1;
+        for (int k = 0; k < nx; ++k)
+          if (t + 1 + k < f_hi) queue.push_back(t + 1 + k);
+      } else if (!ydone[T.s]) {
+        return "forward: chunk before its diagonal task";
+      }
+      for (int k = a.ftp[t]; k < a.ftp[t + 1]; ++k) {
+        const int o = a.ftg[k];
+        if (++ready[o] == a.expect[o] && q.fdiag[o] < f_hi) queue.push_back(q.fdiag[o]);
+      }
+      return std::string();
+    };
+    for (size_t h = 0; h < queue.size(); ++h) {
+      if (queue[h] >= f_hi) return "forward queue: task outside the queue range";
+      const std::string w = run(queue[h], true);
+      if (!w.empty()) return w;
+    }
+    if ((int)queue.size() != f_hi) return "forward queue: not every queued task handed out";
+    for (int t = f_hi; t < nf; ++t) {
+      const std::string w = run(t, false);
+      if (!w.empty()) return w;
+    }
+  }
+  {
+    std::vector<int> xdone(nsn, 0), cdone(nsn, 0), cnt(nb, 0), seen(nb, 0);
+    std::vector<int> queue(q.binit);
+    auto run = [&](int t, bool queued) -> std::string {
+      if (seen[t]++) return "backward: task handed out twice";
+      const SolveTask& T = a.bt[t];
+      if (queued) {
+        if (cnt[t] != q.bneed[t]) return "backward queue: task before its inputs";
+      } else {
+        for (int k = a.btp[t]; k < a.btp[t + 1]; ++k)
+          if (!xdone[a.btg[k]]) return "backward: task claimed before an owner of its rows";
+        if (T.kind == 0 && cdone[T.s] != std::max(a.nch[T.s], 1) - 1) return "backward: diagonal task before its chunks";
+      }
+      if (T.kind == 1) {
+        cdone[T.s]++;
+        const int d = q.bdiag[T.s];
+        if (++cnt[d] == q.bneed[d] && d >= b_lo) queue.push_back(d);
+      } else {
+        xdone[T.s] = 1;
+        for (int k = q.dptr[T.s]; k < q.dptr[T.s + 1]; ++k) {
+          const int d = q.dep[k];
+          if (++cnt[d] == q.bneed[d] && d >= b_lo) queue.push_back(d);
+        }
+      }
+      return std::string();
+    };
+    for (int t = 0; t < b_lo; ++t) {
+      const std::string w = run(t, false);
+      if (!w.empty()) return w;
+    }
+    for (size_t h = 0; h < queue.size(); ++h) {
+      if (queue[h] < b_lo) return "backward queue: task outside the queue range";
+      const std::string w = run(queue[h], true);
+      if (!w.empty()) return w;
+    }
+    if ((int)queue.size() != nb - b_lo) return "backward queue: not every queued task handed out";
+  }
+  return std::string();
+}
 }  // namespace
 
 void build_solve_plan(temf_ctx& c) {
@@ -939,6 +1258,7 @@ void build_solve_plan(temf_ctx& c) {
   P.nchunk.upload(a.nch.data(), a.nch.size(), st);
   P.part_len = a.poff[nsn];
   P.part_off.upload(a.poff.data(), a.poff.size(), st);
+  upload_queue_plan(a, S, default_split(S), P.q1, st);
   TEMF_CUDA(cudaStreamSynchronize(st));  // the host vectors of `a` go out of scope
   Sched b;
   build_sched(S, kChunkRowsMulti, b);
@@ -956,6 +1276,7 @@ void build_solve_plan(temf_ctx& c) {
   for (int s = 0; s < nsn; ++s) aoff[s + 1] = aoff[s] + (b.nch[s] > 1 ? S.sn_first[s + 1] - S.sn_first[s] : 0);
   P.macc_len = aoff[nsn];
   P.macc_off.upload(aoff.data(), aoff.size(), st);
+  upload_queue_plan(b, S, default_split(S), P.qm, st);
   P.sync.alloc(4 * (size_t)nsn + 4);
   TEMF_CUDA(cudaStreamSynchronize(st));
 }
@@ -977,8 +1298,10 @@ static int persistent_grid(K kernel, size_t smem) {
   return std::max(1, sms) * std::max(1, per);
 }
 
+static void queued_views(temf_ctx& c, bool block, double* const* Lbase, double* x, SweepView& vf, SweepView& vb);
+static void reset_queues(temf_ctx& c, bool block, cudaStream_t st);
+
 static void launch_solve_multi(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st) {
-  FactorPlan& F = c.fplan;
   SolvePlan& P = c.splan;
   const size_t smem = sizeof(MultiSmem);
   TEMF_CUDA(cudaFuncSetAttribute(k_fwd_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -987,46 +1310,71 @@ static void launch_solve_multi(temf_ctx& c, double* const* Lbase, double* x, int
   const int gridb = std::min(persistent_grid(k_bwd_multi, smem), std::max(P.n_mbtask, 1));
   for (int c0 = 0; c0 < nrhs; c0 += kMultiCols) {
     const int k = std::min(kMultiCols, nrhs - c0);
-    TEMF_CUDA(cudaMemsetAsync(P.sync.p, 0, P.sync.bytes(), st));
-    k_fwd_multi<<<gridf, kSolveThreads, smem, st>>>(P.n_mftask, P.mftask.p, F.sn_first.p, F.sn_rows_ptr.p,
-                                                   F.sn_rows.p, F.sn_Lptr.p, Lbase, x + c0, nrhs, k, P.mftgt_ptr.p,
-                                                   P.mftgt.p, P.mfexpect.p, P.sync.p, P.nsn, c.d_status.p + 1);
+    SweepView vf, vb;
+    queued_views(c, true, Lbase, x + c0, vf, vb);
+    reset_queues(c, true, st);
+    k_fwd_multi<<<gridf, kSolveThreads, smem, st>>>(vf, nrhs, k, c.d_status.p + 1);
     TEMF_CHECK_LAUNCH();
     TEMF_CUDA(cudaMemsetAsync(c.d_part.p, 0, (size_t)std::max<int64_t>(P.macc_len, 1) * kMultiCols * sizeof(double), st));
-    k_bwd_multi<<<gridb, kSolveThreads, smem, st>>>(P.n_mbtask, P.mbtask.p, F.sn_first.p, F.sn_rows_ptr.p,
-                                                   F.sn_rows.p, F.sn_Lptr.p, Lbase, x + c0, nrhs, k, P.mbtgt_ptr.p,
-                                                   P.mbtgt.p, P.mnchunk.p, P.macc_off.p, c.d_part.p, P.sync.p,
-                                                   P.nsn, c.d_status.p + 1);
+    k_bwd_multi<<<gridb, kSolveThreads, smem, st>>>(vb, nrhs, k, c.d_status.p + 1);
     TEMF_CHECK_LAUNCH();
   }
 }
 
 int solve_launch_count(int nrhs) { return nrhs == 1 ? 2 : 2 * ceil_div(nrhs, kMultiCols); }
 
-void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st) {
+// Views of the sweeps through the ready queue: the single-column schedules
+// (q1) or the 64-row ones of the block sweeps (qm, backward accumulators in
+// place of the partial sums)
+static void queued_views(temf_ctx& c, bool block, double* const* Lbase, double* x, SweepView& vf, SweepView& vb) {
   FactorPlan& F = c.fplan;
+  SolvePlan& P = c.splan;
+  QueuePlan& Q = block ? P.qm : P.q1;
+  const int nf = block ? P.n_mftask : P.n_ftask, nb = block ? P.n_mbtask : P.n_btask;
+  int* q = Q.qbuf.p;
+  int* words = q + (size_t)nf + 2 * (size_t)nb;  // fhead, bhead, ftail, btail
+  vf = SweepView{block ? P.mftask.p : P.ftask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x,
+                 block ? P.mftgt_ptr.p : P.ftgt_ptr.p, block ? P.mftgt.p : P.ftgt.p,
+                 block ? P.mfexpect.p : P.fexpect.p, nullptr, nullptr, nullptr, P.sync.p, P.nsn, nf,
+                 q, words + 0, words + 2, Q.fdiag.p, nullptr, nullptr, nullptr, nullptr, 0, Q.f_hi};
+  vb = SweepView{block ? P.mbtask.p : P.btask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x,
+                 block ? P.mbtgt_ptr.p : P.btgt_ptr.p, block ? P.mbtgt.p : P.btgt.p, nullptr,
+                 block ? P.mnchunk.p : P.nchunk.p, block ? P.macc_off.p : P.part_off.p, c.d_part.p, P.sync.p, P.nsn,
+                 nb, q + nf, words + 1, words + 3, Q.bdiag.p, Q.bdep_ptr.p, Q.bdep.p, Q.bneed.p, q + nf + nb,
+                 Q.b_lo, nb};
+}
+
+// clear the sweep words and seed both queues with their initially ready tasks
+static void reset_queues(temf_ctx& c, bool block, cudaStream_t st) {
+  SolvePlan& P = c.splan;
+  QueuePlan& Q = block ? P.qm : P.q1;
+  const int nf = block ? P.n_mftask : P.n_ftask, nb = block ? P.n_mbtask : P.n_btask;
+  int* q = Q.qbuf.p;
+  int* words = q + (size_t)nf + 2 * (size_t)nb;
+  TEMF_CUDA(cudaMemsetAsync(P.sync.p, 0, P.sync.bytes(), st));
+  TEMF_CUDA(cudaMemsetAsync(q, 0, Q.qbuf.bytes(), st));
+  if (Q.n_finit)
+    TEMF_CUDA(cudaMemcpyAsync(q, Q.finit.p, Q.n_finit * sizeof(int), cudaMemcpyDeviceToDevice, st));
+  if (Q.n_binit)
+    TEMF_CUDA(cudaMemcpyAsync(q + nf, Q.binit.p, Q.n_binit * sizeof(int), cudaMemcpyDeviceToDevice, st));
+  TEMF_CUDA(cudaMemcpyAsync(words + 2, Q.qtails.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st));
+}
+
+void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st) {
   SolvePlan& P = c.splan;
   ensure_update_buffer(c, nrhs);
   if (nrhs > 1) {
     launch_solve_multi(c, Lbase, x, nrhs, st);
     return;
   }
-  const size_t smem = (size_t)(kSnCols + kChunkRows) * nrhs * sizeof(double);
-  if (smem > 12 * 1024) {
-    TEMF_CUDA(cudaFuncSetAttribute(k_fwd_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TEMF_CUDA(cudaFuncSetAttribute(k_bwd_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  }
-  TEMF_CUDA(cudaMemsetAsync(P.sync.p, 0, P.sync.bytes(), st));
-  const int grid = std::min(persistent_grid(k_fwd_persistent, smem), std::max(P.n_ftask, 1));
-  k_fwd_persistent<<<grid, kSolveThreads, smem, st>>>(P.n_ftask, P.ftask.p, F.sn_first.p, F.sn_rows_ptr.p,
-                                                      F.sn_rows.p, F.sn_Lptr.p, Lbase, x, nrhs, P.ftgt_ptr.p, P.ftgt.p,
-                                                      P.fexpect.p, P.sync.p, P.nsn, c.d_status.p + 1);
+  SweepView vf, vb;
+  queued_views(c, false, Lbase, x, vf, vb);
+  reset_queues(c, false, st);
+  const int grid = std::min(persistent_grid(k_fwd_queued, 0), std::max(P.n_ftask, 1));
+  k_fwd_queued<<<grid, kSolveThreads, 0, st>>>(vf, c.d_status.p + 1);
   TEMF_CHECK_LAUNCH();
-  const int gridb = std::min(persistent_grid(k_bwd_persistent, smem), std::max(P.n_btask, 1));
-  k_bwd_persistent<<<gridb, kSolveThreads, smem, st>>>(P.n_btask, P.btask.p, F.sn_first.p, F.sn_rows_ptr.p,
-                                                       F.sn_rows.p, F.sn_Lptr.p, Lbase, x, nrhs, P.btgt_ptr.p,
-                                                       P.btgt.p, P.nchunk.p, P.part_off.p, c.d_part.p, P.sync.p,
-                                                       P.nsn, c.d_status.p + 1);
+  const int gridb = std::min(persistent_grid(k_bwd_queued, 0), std::max(P.n_btask, 1));
+  k_bwd_queued<<<gridb, kSolveThreads, 0, st>>>(vb, c.d_status.p + 1);
   TEMF_CHECK_LAUNCH();
 }
 
@@ -1131,6 +1479,121 @@ void launch_solve_models(int nf, const int2* order_f, const SweepView* vf, int n
   k_bwd_models<<<std::max(1, std::min(grid_b, nb)), kSolveThreads, 0, st>>>(nb, order_b, vb, active, counters + 1,
                                                                               err);
   TEMF_CHECK_LAUNCH();
+}
+
+// One single-column solve of b with the per-task timeline recorded.
+// out: 8 words per task, forward tasks then backward tasks: start, dependency
+// satisfied, end (ns), SM, supernode, kind, first row, supernode level.
+void solve_timeline(temf_ctx& c, int slot, const double* b_perm, int64_t cap, unsigned long long* out,
+                    int* n_fwd, int* n_bwd) {
+  SolvePlan& P = c.splan;
+  const int64_t nt = (int64_t)P.n_ftask + P.n_btask;
+  *n_fwd = P.n_ftask;
+  *n_bwd = P.n_btask;
+  if (!out) return;
+  if (cap < 8 * nt) throw ArgError("timeline buffer too small: need 8 words per task");
+  cudaStream_t st = c.stream;
+  DBuf<unsigned long long> rec;
+  rec.alloc(4 * (size_t)nt);
+  TEMF_CUDA(cudaMemsetAsync(rec.p, 0, rec.bytes(), st));
+  DBuf<double> x;
+  x.upload(b_perm, c.n_edges, st);
+  DBuf<double*> lb;
+  lb.alloc(1);
+  double* Lp = c.slots[slot].L.p;
+  TEMF_CUDA(cudaMemcpyAsync(lb.p, &Lp, sizeof(double*), cudaMemcpyHostToDevice, st));
+  unsigned long long* pf = rec.p;
+  unsigned long long* pb = rec.p + 4 * (size_t)P.n_ftask;
+  unsigned long long* none = nullptr;
+  TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_f, &pf, sizeof(pf), 0, cudaMemcpyHostToDevice, st));
+  TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_b, &pb, sizeof(pb), 0, cudaMemcpyHostToDevice, st));
+  launch_solve(c, lb.p, x.p, 1, st);
+  TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_f, &none, sizeof(none), 0, cudaMemcpyHostToDevice, st));
+  TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_b, &none, sizeof(none), 0, cudaMemcpyHostToDevice, st));
+  std::vector<unsigned long long> h(4 * (size_t)nt);
+  std::vector<SolveTask> tf(P.n_ftask), tb(P.n_btask);
+  TEMF_CUDA(cudaMemcpyAsync(h.data(), rec.p, rec.bytes(), cudaMemcpyDeviceToHost, st));
+  TEMF_CUDA(cudaMemcpyAsync(tf.data(), P.ftask.p, tf.size() * sizeof(SolveTask), cudaMemcpyDeviceToHost, st));
+  TEMF_CUDA(cudaMemcpyAsync(tb.data(), P.btask.p, tb.size() * sizeof(SolveTask), cudaMemcpyDeviceToHost, st));
+  TEMF_CUDA(cudaStreamSynchronize(st));
+  for (int64_t i = 0; i < nt; ++i) {
+    const SolveTask& T = i < P.n_ftask ? tf[i] : tb[i - P.n_ftask];
+    unsigned long long* o = out + 8 * i;
+    for (int q = 0; q < 4; ++q) o[q] = h[4 * i + q];
+    o[4] = (unsigned long long)T.s;
+    o[5] = (unsigned long long)T.kind;
+    o[6] = (unsigned long long)T.r0;
+    o[7] = (unsigned long long)c.sym.sn_level[T.s];
+  }
+}
+
+std::string check_schedules(const Symbolic& S) {
+  const int splits[5] = {0, level_below_width(S, 2048), default_split(S), level_below_width(S, 64), S.nlevels};
+  for (int sp : splits) {
+    std::string w = check_schedule(S, kChunkRows, sp);
+    if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ": " + w;
+    w = check_schedule(S, kChunkRowsMulti, sp);
+    if (!w.empty()) return "64-row chunks, split " + std::to_string(sp) + ": " + w;
+  }
+  return std::string();
+}
+
+// Autotuner of the queue split: times one solve (right-hand side all ones,
+// nrhs columns) for each candidate split level and keeps the fastest.
+int tune_solve(temf_ctx& c, int slot, int nrhs) {
+  const Symbolic& S = c.sym;
+  SolvePlan& P = c.splan;
+  const bool block = nrhs > 1;
+  QueuePlan& Q = block ? P.qm : P.q1;
+  cudaStream_t st = c.stream;
+  Sched a;
+  build_sched(S, block ? kChunkRowsMulti : kChunkRows, a);
+  std::vector<int> cand = {0, level_below_width(S, 4096), level_below_width(S, 1024), level_below_width(S, 512),
+                           level_below_width(S, 148), level_below_width(S, 32), S.nlevels};
+  std::sort(cand.begin(), cand.end());
+  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+  const size_t vec = (size_t)c.n_edges * nrhs;
+  DBuf<double> ones, x;
+  std::vector<double> h(vec, 1.0);
+  ones.upload(h.data(), vec, st);
+  x.alloc(vec);
+  DBuf<double*> lb;
+  lb.alloc(1);
+  double* Lp = c.slots[slot].L.p;
+  TEMF_CUDA(cudaMemcpyAsync(lb.p, &Lp, sizeof(double*), cudaMemcpyHostToDevice, st));
+  cudaEvent_t e0, e1;
+  TEMF_CUDA(cudaEventCreate(&e0));
+  TEMF_CUDA(cudaEventCreate(&e1));
+  Q.tune_ms.clear();
+  Q.tune_split.clear();
+  int best = Q.split;
+  double best_ms = 1e30;
+  for (int sp : cand) {
+    upload_queue_plan(a, S, sp, Q, st);
+    double tot = 0.0;
+    for (int rep = 0; rep < 4; ++rep) {
+      TEMF_CUDA(cudaMemcpyAsync(x.p, ones.p, vec * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      TEMF_CUDA(cudaEventRecord(e0, st));
+      launch_solve(c, lb.p, x.p, nrhs, st);
+      TEMF_CUDA(cudaEventRecord(e1, st));
+      TEMF_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      TEMF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (rep > 0) tot += ms;  // the first solve warms up
+    }
+    tot /= 3.0;
+    Q.tune_ms.push_back(tot);
+    Q.tune_split.push_back(sp);
+    if (tot < best_ms) {
+      best_ms = tot;
+      best = sp;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  upload_queue_plan(a, S, best, Q, st);
+  Q.tuned = true;
+  return best;
 }
 
 }  // namespace temf

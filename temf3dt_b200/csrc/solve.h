@@ -1,4 +1,6 @@
 #pragma once
+#include <string>
+
 #include "ctx.h"
 
 namespace temf {
@@ -22,9 +24,22 @@ struct SweepView {
   int* sync;               // ready | ydone | cdone | xdone (nsn each) | counters
   int nsn;
   int ntask;
+  // ready-queue scheduling (null queue: tasks are claimed in schedule order)
+  int* queue;              // ntask slots: task + 1 once ready, 0 before
+  int* qhead;              // pop counter
+  int* qtail;              // push counter
+  const int* diag_task;    // per supernode: index of its diagonal task in this sweep
+  const int* dep_ptr;      // backward: per supernode, the tasks waiting for its x
+  const int* dep;
+  const int* need;         // backward: per task, completions it waits for
+  int* cnt;                // backward: per task, completions so far
+  int q_lo, q_hi;          // tasks [q_lo, q_hi) go through the queue, the rest are claimed in order
 };
 
 void build_solve_plan(temf_ctx& c);
+// Host replay of the sweep schedules of a symbolic analysis (both chunk
+// heights; claim order and ready queue).  Empty string, or the violation.
+std::string check_schedules(const Symbolic& S);
 void ensure_update_buffer(temf_ctx& c, int nrhs);
 
 // x (device, permuted order, row-major n x nrhs) is overwritten: b -> A^{-1} b.
@@ -64,6 +79,15 @@ void launch_spmv(temf_ctx& c, const double* M, const double* x, double* y, int n
 SweepView fwd_view(temf_ctx& c, double* const* Lbase, double* x, int* sync);
 SweepView bwd_view(temf_ctx& c, double* const* Lbase, double* x, int* sync);
 int models_grid(bool forward);
+// Autotuner of the sweeps' ready-queue split level (the supernodes below it
+// are scheduled through the queue, the ones above are claimed in order with
+// their panels prefetched): times one solve of nrhs columns with the factor
+// in `slot` per candidate and keeps the fastest.  Returns the chosen level.
+int tune_solve(temf_ctx& c, int slot, int nrhs);
+// Profiling aid: one single-column solve of b (permuted order) in `slot` with
+// a per-task timeline (8 words per task; see solve.cu).
+void solve_timeline(temf_ctx& c, int slot, const double* b_perm, int64_t cap, unsigned long long* out,
+                    int* n_fwd, int* n_bwd);
 void launch_solve_models(int nf, const int2* order_f, const SweepView* vf, int nb, const int2* order_b,
                          const SweepView* vb, const int* active, int* counters, int* err, int grid_f, int grid_b,
                          cudaStream_t st);

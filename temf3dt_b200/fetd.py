@@ -247,6 +247,34 @@ class FetdGPU:
         self._ck(self._L.temf_result_gates(self._h, len(g), dptr(g), dptr(out), iptr(done)), "temf_result_gates")
         return out.reshape(len(g), max(self.nrec, 1), 9), done.astype(bool)
 
+    def tune_solve(self, slot: int, nrhs: int = 1):
+        """Autotune the sweeps' queue split level on the factor in `slot`;
+        returns (chosen level, {level: ms per solve})."""
+        sp, n = C.c_int(0), C.c_int(0)
+        cs = np.zeros(8, dtype=np.int32)
+        cm = np.zeros(8)
+        self._ck(self._L.temf_tune_solve(self._h, slot, nrhs, C.byref(sp), C.byref(n), iptr(cs), dptr(cm)),
+                 "temf_tune_solve")
+        return sp.value, {int(cs[i]): float(cm[i]) for i in range(n.value)}
+
+    def solve_schedule(self, nrhs: int = 1):
+        """(split level in use, tuned?) of the single-column or block sweeps."""
+        sp, tu = C.c_int(0), C.c_int(0)
+        self._ck(self._L.temf_solve_schedule(self._h, nrhs, C.byref(sp), C.byref(tu)), "temf_solve_schedule")
+        return sp.value, bool(tu.value)
+
+    def solve_timeline(self, slot: int):
+        """Per-task timeline of one single-column solve (profiling aid):
+        (forward, backward) arrays of rows (start_ns, ready_ns, end_ns, sm,
+        supernode, kind, r0, level)."""
+        nf, nb = C.c_int(0), C.c_int(0)
+        self._ck(self._L.temf_solve_timeline(self._h, slot, 0, None, C.byref(nf), C.byref(nb)), "temf_solve_timeline")
+        out = np.zeros(8 * (nf.value + nb.value), dtype=np.uint64)
+        self._ck(self._L.temf_solve_timeline(self._h, slot, out.size, out.ctypes.data_as(C.POINTER(C.c_ulonglong)),
+                                             C.byref(nf), C.byref(nb)), "temf_solve_timeline")
+        out = out.reshape(-1, 8).astype(np.int64)
+        return out[:nf.value], out[nf.value:]
+
     # -- adjoint gradient ---------------------------------------------------------------
     def adjoint_record(self, checkpoint_every: int = 50) -> None:
         """Record the next runs' solve graph for :meth:`adjoint` (0 = off)."""

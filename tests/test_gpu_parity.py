@@ -77,6 +77,25 @@ def test_factor_solve_backward_error(small, dt):
     assert np.linalg.norm(A @ x - B[:, 0]) <= 1e-12 * np.linalg.norm(B[:, 0])
 
 
+@pytest.mark.parametrize("nrhs", [1, 64])
+def test_tuned_sweep_schedules_solve_to_backward_error(small, nrhs):
+    """The autotuner times each candidate queue split and keeps one; solves
+    with the chosen schedule keep backward error 1e-12 (1 and 64 columns)."""
+    m, om, g, info = small
+    dt = 1e-6
+    A = 3 * O.full_from_upper(om.B) + 2 * dt * O.full_from_upper(om.C)
+    assert g.factor(1, dt) == 0
+    split, cand = g.tune_solve(1, nrhs)
+    assert split in cand and len(cand) >= 2
+    assert g.solve_schedule(nrhs) == (split, True)
+    rng = np.random.default_rng(5)
+    X0 = rng.standard_normal((om.n, nrhs))
+    B = A @ X0
+    X = g.solve(1, B if nrhs > 1 else B[:, 0]).reshape(om.n, nrhs)
+    rel = np.linalg.norm(A @ X - B, axis=0) / np.linalg.norm(B, axis=0)
+    assert rel.max() <= 1e-12, rel.max()
+
+
 def test_block_solve_of_many_columns(small):
     """70 right-hand sides: one full 64-column block through the tensor-core
     block sweeps plus a 6-column remainder; every column to backward error

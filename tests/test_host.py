@@ -178,3 +178,34 @@ def test_synth_models(kind):
             if (lam > 1e-9).all():
                 inside += 1
         assert inside == 1
+
+
+def _edge_pattern(model):
+    """Edge-adjacency pattern (no diagonal) and edge midpoints of a synthetic mesh."""
+    import scipy.sparse as sp
+    from temf3dt_b200 import fetd
+    ev, te, _ = fetd.mesh_topology(model.mesh.tet_vex)
+    n, T = ev.shape[0], te.shape[0]
+    I = sp.csr_matrix((np.ones(6 * T), (np.repeat(np.arange(T), 6), (te - 1).reshape(-1))), shape=(T, n))
+    A = (I.T @ I).tocsr()
+    A.setdiag(0)
+    A.eliminate_zeros()
+    A.sort_indices()
+    mid = 0.5 * (model.mesh.nod_cor[ev[:, 0] - 1] + model.mesh.nod_cor[ev[:, 1] - 1])
+    return n, A.indptr.astype(np.int64), A.indices.astype(np.int32), np.ascontiguousarray(mid)
+
+
+@pytest.mark.parametrize("kind", ["grid", "mesh"])
+def test_solve_schedules_replay(kind):
+    """The persistent sweeps' task schedules, replayed on the host for both
+    chunk heights: claimed in order every wait targets an earlier task, and
+    through the ready queue every task is handed out once, after its inputs."""
+    if kind == "grid":
+        n, xadj, adj, xyz = _grid_pattern(13, 11, 9)
+    else:
+        from tests.golden_cases import tiny_synth
+        n, xadj, adj, xyz = _edge_pattern(tiny_synth())
+    msg = C.create_string_buffer(256)
+    rc = _lib.lib().temf_schedule_check(n, xadj.ctypes.data_as(C.POINTER(C.c_longlong)), _lib.iptr(adj),
+                                        _lib.dptr(xyz), msg, 256)
+    assert rc == 0, msg.value.decode()
