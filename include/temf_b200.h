@@ -251,6 +251,12 @@ int temf_batch_timing(temf_batch* batch, double* ms, long long* counts);
 int temf_batch_tuning(temf_batch* batch, int* order, int* grid_pct, double* candidate_ms);
 int temf_batch_set_tuning(temf_batch* batch, int order, int grid_pct);
 
+/* Options of the next temf_analyse (no reference counterpart; MKL's ordering
+ * has its own knobs in iparm): nested-dissection leaf size (default 96) and
+ * supernode amalgamation (0 none, 1 default: merge while few explicit zeros
+ * are added, 2: merge small supernodes harder, for fewer and larger tasks). */
+int temf_set_analysis_options(temf_ctx* ctx, int leaf_size, int amalg_level);
+
 /* ---- statistics of the symbolic analysis ----------------------------------
  * stats[0..9] = n, nnz(A full), supernodes, levels, nnz(L), stored doubles,
  * factor flops, update tiles, seconds ordering, seconds symbolic. */

@@ -436,10 +436,29 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
     const int nch = V.nchunk[s];
     const double* pp = V.part + V.part_off[s] * nrhs;
     if (nrhs == 1) {
+      // the other chunks' partials: thread (j, h) sums chunks q = 1 + h, 3 + h, ...
+      // with eight loads in flight; fixed order, so still deterministic
+      double* psum = zx;  // the chunk rows are consumed: reuse as [2][64]
+      if (nch > 1) {
+        const int j = tid & (kSnCols - 1), h = tid / kSnCols;
+        double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (j < c && h < 2) {
+          int q = 1 + h;
+          for (; q + 14 < nch; q += 16) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) a[u] += __ldcg(pp + (int64_t)(q + 2 * u) * c + j);
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (q + 2 * u < nch) a[u] += __ldcg(pp + (int64_t)(q + 2 * u) * c + j);
+        }
+        if (h < 2) psum[h * kSnCols + j] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+        __syncthreads();
+      }
       for (int j = tid; j < c; j += blockDim.x) {
         double v = __ldcg(x + f + j);
         if (nr > 0) v -= (seg[0][j] + seg[1][j]) + (seg[2][j] + seg[3][j]);
-        for (int q = 1; q < nch; ++q) v -= __ldcg(pp + (int64_t)q * c + j);
+        if (nch > 1) v -= psum[j] + psum[kSnCols + j];
         zs[j] = v;
       }
     } else {

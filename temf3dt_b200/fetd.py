@@ -125,6 +125,12 @@ class FetdGPU:
         s, m = as_f64(sig), as_f64(mu)
         self._ck(self._L.temf_set_media(self._h, dptr(s), dptr(m)), "temf_set_media")
 
+    def set_analysis_options(self, leaf_size: int = 96, amalg_level: int = 1) -> None:
+        """Options of the next analyse(): nested-dissection leaf size and
+        supernode amalgamation (0 none, 1 default, 2 harder)."""
+        self._ck(self._L.temf_set_analysis_options(self._h, int(leaf_size), int(amalg_level)),
+                 "temf_set_analysis_options")
+
     def analyse(self) -> None:
         self._ck(self._L.temf_analyse(self._h), "temf_analyse")
 
