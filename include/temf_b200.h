@@ -253,8 +253,9 @@ int temf_batch_set_tuning(temf_batch* batch, int order, int grid_pct);
 
 /* Options of the next temf_analyse (no reference counterpart; MKL's ordering
  * has its own knobs in iparm): nested-dissection leaf size (default 96) and
- * supernode amalgamation (0 none, 1 default: merge while few explicit zeros
- * are added, 2: merge small supernodes harder, for fewer and larger tasks). */
+ * supernode amalgamation (0 none, 1: merge while few explicit zeros are
+ * added, 2 (default): also merge small supernodes harder, for fewer and
+ * larger solve tasks). */
 int temf_set_analysis_options(temf_ctx* ctx, int leaf_size, int amalg_level);
 
 /* ---- statistics of the symbolic analysis ----------------------------------

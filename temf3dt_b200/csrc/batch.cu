@@ -70,7 +70,18 @@ struct BatchEngine {
   DBuf<int> active;         // [site][model]
   int* act_h = nullptr;     // pinned copy of the table
   DBuf<int> errw;
-  DBuf<int2> ordf, ordb;
+  DBuf<int2> ordf, ordb;   // merged in-order (above-split) tasks
+  // shared ready queues: [forward slots][backward slots][per-model backward
+  // counts][fhead, bhead, ftail, btail]
+  DBuf<int> gq;
+  size_t gq_f = 0, gq_b = 0, gq_cnt = 0, gq_words = 0;
+  std::vector<int> f_hi, b_lo, cnt_off;
+  std::vector<std::vector<int>> finit_h, binit_h;
+  struct InitSet {
+    DBuf<int> f, b, tails;
+    int nf = 0, nb = 0, qlim_f = 0, qlim_b = 0;
+  };
+  std::map<std::vector<int>, std::unique_ptr<InitSet>> init_sets;  // key: active flags
   int nf = 0, nb = 0, gridf = 0, gridb = 0;
   std::vector<std::vector<SolveTask>> ftask_h, btask_h;
   std::map<std::vector<int>, cudaGraphExec_t> graphs;  // key: N, then the participating models
@@ -90,6 +101,22 @@ struct BatchEngine {
     dsz = opt.step_dblesize;
     nsite = dbl + dsz + 1;
     B.results.assign(nm, RunResult());
+    f_hi.assign(nm, 0);
+    b_lo.assign(nm, 0);
+    cnt_off.assign(nm, 0);
+    finit_h.resize(nm);
+    binit_h.resize(nm);
+    for (int m = 0; m < nm; ++m) {
+      const temf_ctx& c = *B.models[m];
+      queue_ranges(c, f_hi[m], b_lo[m]);
+      queue_init_lists(c, finit_h[m], binit_h[m]);
+      cnt_off[m] = (int)(gq_cnt);
+      gq_f += f_hi[m];
+      gq_b += c.splan.n_btask - b_lo[m];
+      gq_cnt += c.splan.n_btask;
+    }
+    gq.alloc(gq_f + gq_b + gq_cnt + 4);
+    gq_words = gq_f + gq_b + gq_cnt;
     std::vector<size_t> soff(nm);
     size_t words = 2;
     for (int m = 0; m < nm; ++m) {
@@ -135,8 +162,29 @@ struct BatchEngine {
                     : site < dbl - 1 + dsz ? R->T(site - (dbl - 1))
                                            : R->vco.p;
         double* const* Lb = R->lptr.p + (site == site_coarse() ? 3 : 2);
-        hf[(size_t)site * nm + m] = fwd_view(c, Lb, x, sy);
-        hb[(size_t)site * nm + m] = bwd_view(c, Lb, x, sy);
+        SweepView a = fwd_view(c, Lb, x, sy), b = bwd_view(c, Lb, x, sy);
+        const QueuePlan& Q = c.splan.q1;
+        int* w = gq.p + gq_words;
+        a.queue = gq.p;
+        a.qhead = w + 0;
+        a.qtail = w + 2;
+        a.diag_task = Q.fdiag.p;
+        a.q_lo = 0;
+        a.q_hi = f_hi[m];
+        a.tag = m << 24;
+        b.queue = gq.p + gq_f;
+        b.qhead = w + 1;
+        b.qtail = w + 3;
+        b.diag_task = Q.bdiag.p;
+        b.dep_ptr = Q.bdep_ptr.p;
+        b.dep = Q.bdep.p;
+        b.need = Q.bneed.p;
+        b.cnt = gq.p + gq_f + gq_b + cnt_off[m];
+        b.q_lo = b_lo[m];
+        b.q_hi = c.splan.n_btask;
+        b.tag = m << 24;
+        hf[(size_t)site * nm + m] = a;
+        hb[(size_t)site * nm + m] = b;
       }
       // host copies of the task lists (for the merge orders)
       ftask_h.emplace_back(c.splan.n_ftask);
@@ -204,8 +252,15 @@ struct BatchEngine {
   }
 
   void set_tuning(const BatchTuning& t) {
-    auto of = merge(ftask_h, t.order, true);
-    auto ob = merge(btask_h, t.order, false);
+    // only the in-order tasks are merged; the queued ones go through the shared queue
+    std::vector<std::vector<SolveTask>> fs(nm), bs(nm);
+    for (int m = 0; m < nm; ++m) {
+      fs[m].assign(ftask_h[m].begin() + f_hi[m], ftask_h[m].end());
+      bs[m].assign(btask_h[m].begin(), btask_h[m].begin() + b_lo[m]);
+    }
+    auto of = merge(fs, t.order, true);
+    auto ob = merge(bs, t.order, false);
+    for (auto& v : of) v.y += f_hi[v.x];  // back to schedule indices
     nf = (int)of.size();
     nb = (int)ob.size();
     ordf.upload(of.data(), of.size(), st);
@@ -216,10 +271,39 @@ struct BatchEngine {
   }
 
   // one merged solve of site `site` for the models flagged in its active row
+  // initially ready queued tasks of an active set (cached: the set changes rarely)
+  InitSet& init_set(const std::vector<int>& act) {
+    auto it = init_sets.find(act);
+    if (it != init_sets.end()) return *it->second;
+    auto I = std::make_unique<InitSet>();
+    std::vector<int> f, b;
+    for (int m = 0; m < nm; ++m) {
+      if (!act[m]) continue;
+      for (int t : finit_h[m]) f.push_back((m << 24 | t) + 1);
+      for (int t : binit_h[m]) b.push_back((m << 24 | t) + 1);
+      I->qlim_f += f_hi[m];
+      I->qlim_b += B.models[m]->splan.n_btask - b_lo[m];
+    }
+    I->nf = (int)f.size();
+    I->nb = (int)b.size();
+    if (f.empty()) I->f.alloc(1); else I->f.upload(f.data(), f.size(), st);
+    if (b.empty()) I->b.alloc(1); else I->b.upload(b.data(), b.size(), st);
+    const int tails[2] = {I->nf, I->nb};
+    I->tails.upload(tails, 2, st);
+    TEMF_CUDA(cudaStreamSynchronize(st));
+    return *init_sets.emplace(act, std::move(I)).first->second;
+  }
+
   void solve_site(int site) {
+    std::vector<int> act(act_h + (size_t)site * nm, act_h + (size_t)(site + 1) * nm);
+    InitSet& I = init_set(act);
     TEMF_CUDA(cudaMemsetAsync(syncw.p, 0, syncw.bytes(), st));
+    TEMF_CUDA(cudaMemsetAsync(gq.p, 0, gq.bytes(), st));
+    if (I.nf) TEMF_CUDA(cudaMemcpyAsync(gq.p, I.f.p, I.nf * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    if (I.nb) TEMF_CUDA(cudaMemcpyAsync(gq.p + gq_f, I.b.p, I.nb * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    TEMF_CUDA(cudaMemcpyAsync(gq.p + gq_words + 2, I.tails.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st));
     launch_solve_models(nf, ordf.p, vf.p + (size_t)site * nm, nb, ordb.p, vb.p + (size_t)site * nm,
-                        active.p + (size_t)site * nm, syncw.p, errw.p, gridf, gridb, st);
+                        active.p + (size_t)site * nm, syncw.p, errw.p, gridf, gridb, I.qlim_f, I.qlim_b, st);
     S.launches += 2;
     S.solves += 1;
   }
@@ -595,7 +679,13 @@ void run_batch(Batch& B, const RunOptions& opt, bool autotune) {
     if (std::max(1, c->src.nrhs) != 1) throw ArgError("batched models take one right-hand side each");
     if (c->src.pulse_type == 3) throw ArgError("batched models run from rest (pulse types 1 and 2)");
   }
+  if (B.models.size() > 127) throw ArgError("a batch holds at most 127 models");
+  for (temf_ctx* c : B.models)
+    if (c->splan.n_ftask >= (1 << 24) || c->splan.n_btask >= (1 << 24))
+      throw ArgError("a batched model has too many solve tasks (2^24)");
+  const std::vector<double> tuned_ms = B.stats.tune_ms;  // keep the last tuning's candidate times
   B.stats = BatchStats();
+  B.stats.tune_ms = tuned_ms;
   BatchEngine eng(B, opt);
   eng.run(autotune);
   for (temf_ctx* c : B.models) c->slots[0].valid = c->slots[1].valid = false;

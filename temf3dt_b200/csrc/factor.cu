@@ -143,6 +143,13 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 
 constexpr int kLdsU = kUpdTile + 8;  // 72 doubles: two 128-byte wavefronts per fragment load
 
+// 8-byte asynchronous global -> shared copy (L1-allocating; only for panels
+// no CTA of the running kernel writes)
+__device__ __forceinline__ void cp_async8_f(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
 __global__ void __launch_bounds__(128) k_update(
     const UpdTile* __restrict__ tiles, const int* __restrict__ sn_first,
     const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows,
@@ -163,12 +170,17 @@ __global__ void __launch_bounds__(128) k_update(
   const double* P = L + Lptr[s] + c;  // row 0 of L21
   const int kpad = (c + 3) & ~3;
   const int tid = threadIdx.x;
+  // the panel of s is final at this level (its targets are ancestors): copy
+  // both 64-row blocks asynchronously, every copy of a thread in flight at once
   for (int idx = tid; idx < kpad * kUpdTile; idx += blockDim.x) {
     const int k = idx / kUpdTile, ii = idx % kUpdTile;
     const int gi = tile.i0 + ii, gj = tile.j0 + ii;
-    As[k * kLdsU + ii] = (k < c && gi < r) ? P[(int64_t)k * ld + gi] : 0.0;
-    Bs[k * kLdsU + ii] = (k < c && gj < r) ? P[(int64_t)k * ld + gj] : 0.0;
+    if (k < c && gi < r) cp_async8_f(As + k * kLdsU + ii, P + (int64_t)k * ld + gi);
+    else As[k * kLdsU + ii] = 0.0;
+    if (k < c && gj < r) cp_async8_f(Bs + k * kLdsU + ii, P + (int64_t)k * ld + gj);
+    else Bs[k * kLdsU + ii] = 0.0;
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;

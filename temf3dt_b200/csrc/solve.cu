@@ -203,14 +203,14 @@ __device__ __forceinline__ bool in_queue(const SweepView& V, int task) {
 __device__ __forceinline__ void q_push(const SweepView& V, int task) {
   if (!in_queue(V, task)) return;  // claimed in schedule order instead
   const int pos = atomicAdd(V.qtail, 1);
-  atomicExch(V.queue + pos, task + 1);
+  atomicExch(V.queue + pos, (V.tag | task) + 1);
 }
 // thread 0 only: next ready task, or -1 when all ntask tasks are handed out
 // (or a wait timed out: error word set)
-__device__ __forceinline__ int q_pop(const SweepView& V, int* err) {
-  const int idx = atomicAdd(V.qhead, 1);
-  if (idx >= V.q_hi - V.q_lo) return -1;
-  const volatile int* slot = V.queue + idx;
+__device__ __forceinline__ int q_pop(int* qhead, const int* queue, int limit, int* err) {
+  const int idx = atomicAdd(qhead, 1);
+  if (idx >= limit) return -1;
+  const volatile int* slot = queue + idx;
   int it = 0, v;
   while ((v = *slot) == 0) {
     if (++it > kSpinLimit) {
@@ -236,7 +236,7 @@ __device__ __forceinline__ int next_task(const SweepView& V, int* counter, bool 
     if (threadIdx.x == 0) {
       int t = -1;
       if (use_q) {
-        if (V.queue) t = q_pop(V, err);
+        if (V.queue) t = q_pop(V.qhead, V.queue, V.q_hi - V.q_lo, err);
       } else {
         const bool front = V.queue == nullptr || V.q_lo > 0;  // static tasks before the queue range
         const int lo = front ? 0 : V.q_hi, hi = V.queue == nullptr ? V.ntask : (front ? V.q_lo : V.ntask);
@@ -323,7 +323,9 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
     if (V.queue) {
       for (int q = V.tgt_ptr[t] + tid; q < V.tgt_ptr[t + 1]; q += blockDim.x) {
         const int o = V.tgt[q];
-        if (atomicAdd(ready + o, 1) == V.expect[o] - 1) q_push(V, V.diag_task[o]);
+        const int d = V.diag_task[o];
+        if (!in_queue(V, d)) atomicAdd(ready + o, 1);  // claimed in order: only its count matters
+        else if (atomicAdd(ready + o, 1) == V.expect[o] - 1) q_push(V, d);
       }
     } else if (tid == 0) {
       for (int q = V.tgt_ptr[t]; q < V.tgt_ptr[t + 1]; ++q) atomicAdd(ready + V.tgt[q], 1);
@@ -428,7 +430,7 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
       atomicAdd(cdone + s, 1);
       if (V.queue) {
         const int d = V.diag_task[s];
-        if (atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
+        if (in_queue(V, d) && atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
       }
     }
   } else {
@@ -480,10 +482,10 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
     __threadfence();
     __syncthreads();
     if (tid == 0) atomicExch(xdone + s, 1);
-    if (V.queue)  // x_s is out: count it for every task whose rows s owns
+    if (V.queue)  // x_s is out: count it for every queued task whose rows s owns
       for (int q = V.dep_ptr[s] + tid; q < V.dep_ptr[s + 1]; q += blockDim.x) {
         const int d = V.dep[q];
-        if (atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
+        if (in_queue(V, d) && atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
       }
   }
 }
@@ -560,44 +562,77 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_queued(const SweepView V,
 // skipped.  The dependency chains of the models overlap, which fills the GPU
 // where one small model alone leaves most SMs waiting.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kSolveThreads, 3) k_fwd_models(int ntotal, const int2* __restrict__ order,
-                                                               const SweepView* __restrict__ views,
-                                                               const int* __restrict__ active, int* counter,
-                                                               int* err) {
+// Next (model, task) of a merged sweep for this CTA; (-1, -1) when done.
+// Phase order as next_task: forward queue first, backward queue last.
+__device__ __forceinline__ int2 next_model_task(int nstatic, const int2* __restrict__ order,
+                                                const int* __restrict__ active, int* counter, int* qhead,
+                                                const int* queue, int qlim, bool queue_first, int* err, int& phase,
+                                                int2* sh) {
+  for (;;) {
+    const bool use_q = (phase == 0) == queue_first;
+    if (threadIdx.x == 0) {
+      int2 r = make_int2(-1, -1);
+      if (use_q) {
+        if (queue) {
+          const int v = q_pop(qhead, queue, qlim, err);
+          if (v >= 0) r = make_int2(v >> 24, v & 0xFFFFFF);
+        }
+      } else {
+        for (;;) {  // skip the tasks of models that are not stepping
+          const int i = atomicAdd(counter, 1);
+          if (i >= nstatic) break;
+          const int2 mt = order[i];
+          if (active[mt.x]) {
+            r = mt;
+            break;
+          }
+        }
+      }
+      *sh = r;
+    }
+    __syncthreads();
+    const int2 r = *sh;
+    __syncthreads();
+    if (r.x >= 0) return r;
+    if (phase == 1) return r;
+    phase = 1;
+  }
+}
+
+__global__ void __launch_bounds__(kSolveThreads, 3) k_fwd_models(int nstatic, const int2* __restrict__ order,
+                                                                  const SweepView* __restrict__ views,
+                                                                  const int* __restrict__ active, int* counter,
+                                                                  int* err, int qlim) {
   __shared__ double D[kSnCols][kSnCols + 1];
   __shared__ double rinv[kSnCols];
   __shared__ double ys[kSnCols];
-  __shared__ int task_id;
+  __shared__ int2 mt_sh;
+  const SweepView& V0 = views[0];  // the shared queue lives in every view
+  int phase = 0;
   for (;;) {
-    if (threadIdx.x == 0) task_id = atomicAdd(counter, 1);
-    __syncthreads();
-    const int t = task_id;
-    __syncthreads();
-    if (t >= ntotal) break;
-    const int2 mt = order[t];
-    if (!active[mt.x]) continue;
+    const int2 mt = next_model_task(nstatic, order, active, counter, V0.qhead, V0.queue, qlim, true, err, phase,
+                                    &mt_sh);
+    if (mt.x < 0) break;
     const SweepView V = views[mt.x];
     fwd_task(V, mt.y, *V.Lbase, 1, err, D, rinv, ys);
   }
 }
 
-__global__ void __launch_bounds__(kSolveThreads, 3) k_bwd_models(int ntotal, const int2* __restrict__ order,
-                                                               const SweepView* __restrict__ views,
-                                                               const int* __restrict__ active, int* counter,
-                                                               int* err) {
+__global__ void __launch_bounds__(kSolveThreads, 3) k_bwd_models(int nstatic, const int2* __restrict__ order,
+                                                                  const SweepView* __restrict__ views,
+                                                                  const int* __restrict__ active, int* counter,
+                                                                  int* err, int qlim) {
   __shared__ double D[kSnCols][kSnCols + 1];
   __shared__ double rinv[kSnCols];
   __shared__ double seg[4][kSnCols];
   __shared__ double zs[kSnCols + kChunkRows];
-  __shared__ int task_id;
+  __shared__ int2 mt_sh;
+  const SweepView& V0 = views[0];
+  int phase = 0;
   for (;;) {
-    if (threadIdx.x == 0) task_id = atomicAdd(counter, 1);
-    __syncthreads();
-    const int t = task_id;
-    __syncthreads();
-    if (t >= ntotal) break;
-    const int2 mt = order[t];
-    if (!active[mt.x]) continue;
+    const int2 mt = next_model_task(nstatic, order, active, counter, V0.qhead, V0.queue, qlim, false, err, phase,
+                                    &mt_sh);
+    if (mt.x < 0) break;
     const SweepView V = views[mt.x];
     bwd_task(V, mt.y, *V.Lbase, 1, err, D, rinv, seg, zs);
   }
@@ -812,7 +847,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_multi(const SweepView V, 
       __syncthreads();
       for (int q = V.tgt_ptr[t] + tid; q < V.tgt_ptr[t + 1]; q += blockDim.x) {
         const int o = V.tgt[q];
-        if (atomicAdd(ready + o, 1) == V.expect[o] - 1) q_push(V, V.diag_task[o]);
+        const int d = V.diag_task[o];
+        if (!in_queue(V, d)) atomicAdd(ready + o, 1);
+        else if (atomicAdd(ready + o, 1) == V.expect[o] - 1) q_push(V, d);
       }
     }
   }
@@ -869,7 +906,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(const SweepView V, 
       if (tid == 0) {
         atomicAdd(cdone + s, 1);
         const int d = V.diag_task[s];
-        if (atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
+        if (in_queue(V, d) && atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
       }
     } else {
       // Z = Y_s - (first chunk, here) - (other chunks, accumulated); back-substitute
@@ -896,10 +933,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(const SweepView V, 
       __threadfence();
       __syncthreads();
       if (tid == 0) atomicExch(xdone + s, 1);
-      // x_s is out: count it for every task whose rows s owns
+      // x_s is out: count it for every queued task whose rows s owns
       for (int q = V.dep_ptr[s] + tid; q < V.dep_ptr[s + 1]; q += blockDim.x) {
         const int d = V.dep[q];
-        if (atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
+        if (in_queue(V, d) && atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
       }
     }
   }
@@ -1491,13 +1528,29 @@ int models_grid(bool forward) {
 
 void launch_solve_models(int nf, const int2* order_f, const SweepView* vf, int nb, const int2* order_b,
                          const SweepView* vb, const int* active, int* counters, int* err, int grid_f, int grid_b,
-                         cudaStream_t st) {
-  k_fwd_models<<<std::max(1, std::min(grid_f, nf)), kSolveThreads, 0, st>>>(nf, order_f, vf, active, counters,
-                                                                              err);
+                         int qlim_f, int qlim_b, cudaStream_t st) {
+  k_fwd_models<<<std::max(1, std::min(grid_f, nf + qlim_f)), kSolveThreads, 0, st>>>(nf, order_f, vf, active,
+                                                                                      counters, err, qlim_f);
   TEMF_CHECK_LAUNCH();
-  k_bwd_models<<<std::max(1, std::min(grid_b, nb)), kSolveThreads, 0, st>>>(nb, order_b, vb, active, counters + 1,
-                                                                              err);
+  k_bwd_models<<<std::max(1, std::min(grid_b, nb + qlim_b)), kSolveThreads, 0, st>>>(nb, order_b, vb, active,
+                                                                                      counters + 1, err, qlim_b);
   TEMF_CHECK_LAUNCH();
+}
+
+void queue_ranges(const temf_ctx& c, int& f_hi, int& b_lo) {
+  f_hi = c.splan.q1.f_hi;
+  b_lo = c.splan.q1.b_lo;
+}
+
+void queue_init_lists(const temf_ctx& c, std::vector<int>& finit, std::vector<int>& binit) {
+  const QueuePlan& Q = c.splan.q1;
+  finit.resize(Q.n_finit);
+  binit.resize(Q.n_binit);
+  // stored as task + 1
+  if (Q.n_finit) TEMF_CUDA(cudaMemcpy(finit.data(), Q.finit.p, Q.n_finit * sizeof(int), cudaMemcpyDeviceToHost));
+  if (Q.n_binit) TEMF_CUDA(cudaMemcpy(binit.data(), Q.binit.p, Q.n_binit * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int& v : finit) --v;
+  for (int& v : binit) --v;
 }
 
 // One single-column solve of b with the per-task timeline recorded.

@@ -1,5 +1,6 @@
 #pragma once
 #include <string>
+#include <vector>
 
 #include "ctx.h"
 
@@ -34,6 +35,7 @@ struct SweepView {
   const int* need;         // backward: per task, completions it waits for
   int* cnt;                // backward: per task, completions so far
   int q_lo, q_hi;          // tasks [q_lo, q_hi) go through the queue, the rest are claimed in order
+  int tag;                 // model id << 24 when several models share one queue (0 otherwise)
 };
 
 void build_solve_plan(temf_ctx& c);
@@ -88,7 +90,15 @@ int tune_solve(temf_ctx& c, int slot, int nrhs);
 // a per-task timeline (8 words per task; see solve.cu).
 void solve_timeline(temf_ctx& c, int slot, const double* b_perm, int64_t cap, unsigned long long* out,
                     int* n_fwd, int* n_bwd);
+// Merged sweeps with a shared ready queue: order_f/order_b list the models'
+// in-order (above-split) tasks; the views carry the shared queues (forward
+// and backward), each model's own queue range and completion counts; qlim_f,
+// qlim_b = queued tasks of the active models.  counters: 2 claim counters.
 void launch_solve_models(int nf, const int2* order_f, const SweepView* vf, int nb, const int2* order_b,
                          const SweepView* vb, const int* active, int* counters, int* err, int grid_f, int grid_b,
-                         cudaStream_t st);
+                         int qlim_f, int qlim_b, cudaStream_t st);
+// queue ranges [0, f_hi) (forward) and [b_lo, nb) (backward) of a context's
+// single-column schedule, and its initially ready queued tasks
+void queue_ranges(const temf_ctx& c, int& f_hi, int& b_lo);
+void queue_init_lists(const temf_ctx& c, std::vector<int>& finit, std::vector<int>& binit);
 }  // namespace temf

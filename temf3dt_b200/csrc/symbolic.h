@@ -18,7 +18,7 @@ struct SymbolicOptions {
   int leaf_size = 96;          // nested-dissection leaf size
   int max_sn_cols = 64;        // supernodes are split into column blocks of at most this width
   bool amalgamate = true;      // relaxed supernode amalgamation
-  int amalg_level = 1;         // 1: merge while the zero fraction stays small; 2: merge small supernodes harder
+  int amalg_level = 2;         // 1: merge while the zero fraction stays small; 2: merge small supernodes harder
 };
 
 struct Symbolic {

@@ -125,9 +125,9 @@ class FetdGPU:
         s, m = as_f64(sig), as_f64(mu)
         self._ck(self._L.temf_set_media(self._h, dptr(s), dptr(m)), "temf_set_media")
 
-    def set_analysis_options(self, leaf_size: int = 96, amalg_level: int = 1) -> None:
+    def set_analysis_options(self, leaf_size: int = 96, amalg_level: int = 2) -> None:
         """Options of the next analyse(): nested-dissection leaf size and
-        supernode amalgamation (0 none, 1 default, 2 harder)."""
+        supernode amalgamation (0 none, 1 light, 2 harder: the default)."""
         self._ck(self._L.temf_set_analysis_options(self._h, int(leaf_size), int(amalg_level)),
                  "temf_set_analysis_options")
 
