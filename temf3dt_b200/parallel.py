@@ -35,3 +35,18 @@ def gather_traces(local: np.ndarray, world: int, group=None) -> List[np.ndarray]
 def assemble_traces(parts: List[np.ndarray]) -> np.ndarray:
     """Concatenate rank-ordered traces along the receiver axis."""
     return np.concatenate(parts, axis=1)
+
+
+def reduce_gradients(local: np.ndarray, world: int, group=None) -> np.ndarray:
+    """Sum per-rank adjoint gradients (each rank's sources) over all ranks:
+    one all-reduce of the inversion-grid vector.  Works on the process
+    group's backend (gloo on CPU tensors, NCCL on the rank's GPU)."""
+    if world == 1:
+        return np.asarray(local, dtype=np.float64)
+    import torch
+    import torch.distributed as dist
+    backend = dist.get_backend(group)
+    dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    t = torch.as_tensor(np.asarray(local, dtype=np.float64), device=dev).clone()
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.cpu().numpy()
