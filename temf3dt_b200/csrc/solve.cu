@@ -293,13 +293,7 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
     __syncthreads();
     diag_solve(D, rinv, ys, c, nrhs, true);
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = ys[idx];
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) atomicExch(ydone + s, 1);
-    if (V.queue) {  // y_s is out: the other row chunks of s are ready (they follow this task)
-      const int nx = max(1, (int)((r + kChunkRows - 1) / kChunkRows)) - 1;
-      for (int k = tid; k < nx; k += blockDim.x) q_push(V, t + 1 + k);
-    }
+    // y_s is published together with the first chunk's pushes below: one fence for both
   } else {
     if (tid == 0 && !queued) wait_geq(ydone + s, 1, err, 2);
     __syncthreads();
@@ -318,8 +312,17 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
         atomicAdd(dst + col, -a);
       }
     }
-    __threadfence();
-    __syncthreads();
+  }
+  __threadfence();
+  __syncthreads();
+  if (T.kind == 0) {
+    if (tid == 0) atomicExch(ydone + s, 1);
+    if (V.queue) {  // y_s is out: the other row chunks of s are ready (they follow this task)
+      const int nx = max(1, (int)((r + kChunkRows - 1) / kChunkRows)) - 1;
+      for (int k = tid; k < nx; k += blockDim.x) q_push(V, t + 1 + k);
+    }
+  }
+  if (T.r1 > T.r0) {
     if (V.queue) {
       for (int q = V.tgt_ptr[t] + tid; q < V.tgt_ptr[t + 1]; q += blockDim.x) {
         const int o = V.tgt[q];
@@ -389,9 +392,10 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
   if (T.kind == 0) load_diag(D, rinv, P, c, ld);
   const bool queued = in_queue(V, t);
   // the chunk's rows need their owners' x; the diagonal task also its other chunks
-  if (tid == 0 && !queued) {
-    for (int q = V.tgt_ptr[t]; q < V.tgt_ptr[t + 1]; ++q) wait_geq(xdone + V.tgt[q], 1, err, 3);
-    if (T.kind == 0) wait_geq(cdone + s, V.nchunk[s] - (nr > 0 ? 1 : 0), err, 4);
+  if (!queued) {  // one polling thread per owner (and one for the chunk count)
+    const int q0 = V.tgt_ptr[t], nq = V.tgt_ptr[t + 1] - q0;
+    for (int q = tid; q < nq; q += blockDim.x) wait_geq(xdone + V.tgt[q0 + q], 1, err, 3);
+    if (T.kind == 0 && tid == blockDim.x - 1) wait_geq(cdone + s, V.nchunk[s] - (nr > 0 ? 1 : 0), err, 4);
   }
   __syncthreads();
   if (stamp && tid == 0) *stamp = gtime();
@@ -879,9 +883,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(const SweepView V, 
     const int nr = T.r1 - T.r0;
     if (nr > 0) load_panel_block_async(M.A, P, c, ld, T.r0, nr);
     if (T.kind == 0) load_diag_async(M.D, P, c, ld);
-    if (tid == 0 && !in_queue(V, t)) {  // claimed in order: wait for the inputs
-      for (int q = V.tgt_ptr[t]; q < V.tgt_ptr[t + 1]; ++q) wait_geq(xdone + V.tgt[q], 1, err, 3);
-      if (T.kind == 0) wait_geq(cdone + s, max(V.nchunk[s], 1) - 1, err, 4);
+    if (!in_queue(V, t)) {  // claimed in order: wait for the inputs, one polling thread each
+      const int q0 = V.tgt_ptr[t], nq = V.tgt_ptr[t + 1] - q0;
+      for (int q = tid; q < nq; q += blockDim.x) wait_geq(xdone + V.tgt[q0 + q], 1, err, 3);
+      if (T.kind == 0 && tid == blockDim.x - 1) wait_geq(cdone + s, max(V.nchunk[s], 1) - 1, err, 4);
     }
     __syncthreads();
     // Xr = x[rows] (64 x k); C = L21[rows]^T Xr (c x k)
