@@ -47,6 +47,14 @@ __device__ __forceinline__ unsigned smid() {
   return r;
 }
 
+// 8-byte asynchronous global -> shared copy (L1-allocating: only for data
+// no CTA writes during the sweep, i.e. the factor panels)
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Bounded wait until *flag >= target (written by other CTAs of the same
 // kernel).  Polls tightly first, then with a short sleep.  On timeout the
 // error word is set and the wait gives up, so the kernel always terminates;
@@ -121,19 +129,20 @@ __device__ void diag_solve(const double (*D)[kSnCols + 1], const double* rinv, d
   }
 }
 
-// Lower triangle of the diagonal block (one warp per column, coalesced) and
-// the reciprocals of its diagonal.
-__device__ __forceinline__ void load_diag(double (*D)[kSnCols + 1], double* rinv, const double* P, int c,
-                                          int64_t ld) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int j = warp; j < c; j += nw) {
-    const double* col = P + (int64_t)j * ld;
-    for (int i = j + lane; i < c; i += 32) {
-      const double v = __ldg(col + i);
-      D[i][j] = v;
-      if (i == j) rinv[j] = 1.0 / v;
-    }
+// Lower triangle of the diagonal block into D with asynchronous copies
+// (issued before a dependency wait; coalesced per column), and the
+// reciprocals of its diagonal once the copies have landed.
+__device__ __forceinline__ void load_diag_start(double (*D)[kSnCols + 1], const double* P, int c, int64_t ld) {
+  for (int idx = threadIdx.x; idx < c * c; idx += blockDim.x) {
+    const int j = idx / c, i = idx - j * c;
+    if (i >= j) cp_async8(&D[i][j], P + (int64_t)j * ld + i);
   }
+}
+__device__ __forceinline__ void load_diag_finish(double (*D)[kSnCols + 1], double* rinv, int c) {
+  cp_async_wait_all();
+  __syncthreads();
+  if ((int)threadIdx.x < c) rinv[threadIdx.x] = 1.0 / D[threadIdx.x][threadIdx.x];
+  __syncthreads();
 }
 
 // Row-chunk products, single right-hand side.  The panel values are loaded
@@ -285,12 +294,12 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
   if (nrhs == 1) pre_fwd(R, Pc, c, ld, i, row_on);
   const bool queued = in_queue(V, t);
   if (T.kind == 0) {
-    load_diag(D, rinv, P, c, ld);
+    load_diag_start(D, P, c, ld);
     if (tid == 0 && !queued) wait_geq(ready + s, V.expect[s], err, 1);
     __syncthreads();
     if (stamp && tid == 0) *stamp = gtime();
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) ys[idx] = __ldcg(x + (int64_t)f * nrhs + idx);
-    __syncthreads();
+    load_diag_finish(D, rinv, c);
     diag_solve(D, rinv, ys, c, nrhs, true);
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = ys[idx];
     // y_s is published together with the first chunk's pushes below: one fence for both
@@ -389,7 +398,7 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
   const int nr = T.r1 - T.r0;
   BwdRegs R;
   if (nrhs == 1 && nr > 0) pre_bwd(R, P, c, ld, T.r0, nr);
-  if (T.kind == 0) load_diag(D, rinv, P, c, ld);
+  if (T.kind == 0) load_diag_start(D, P, c, ld);
   const bool queued = in_queue(V, t);
   // the chunk's rows need their owners' x; the diagonal task also its other chunks
   if (!queued) {  // one polling thread per owner (and one for the chunk count)
@@ -480,7 +489,7 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
         zs[idx] = v;
       }
     }
-    __syncthreads();
+    load_diag_finish(D, rinv, c);
     diag_solve(D, rinv, zs, c, nrhs, false);
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = zs[idx];
     __threadfence();
@@ -665,13 +674,6 @@ __device__ __forceinline__ void dmma8(double& d0, double& d1, double a, double b
                : "d"(a), "d"(b));
 }
 
-// 8-byte asynchronous global -> shared copy (L1-allocating: only for data
-// no CTA writes during the sweep, i.e. the factor panels)
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 struct MultiSmem {
   double D[kSnCols][kSnCols + 1];
