@@ -71,6 +71,23 @@ int temf_set_media(temf_ctx* ctx, const double* sig_tet, const double* mu_tet);
  * mesh; replaces the reorder/symbolic half of PARDISO phase 12,
  * src/FETD_UTILITY.f90:912-917).  Must follow temf_set_mesh. */
 int temf_analyse(temf_ctx* ctx);
+/* Anisotropic media ('anisotropic' section of model_ctl,
+ * src/FETD_FWD.f90:368-410): per tet the row-major 3 x 3 conductivity tensor
+ * sig9(9, n_tets) and permeability tensor mu9(9, n_tets) (absolute, H/m; the
+ * reference builds both as dm diag(values) dm^T).  Assembly then uses
+ * f_kind_ani / e_kind_ani (:853-912), the curl-curl term with the
+ * elementwise reciprocal of mu9 as mesh_process passes it (:624-633).
+ * Replaces temf_set_media; temf_set_media switches back to scalar media.
+ * The adjoint gradient covers scalar conductivities only. */
+int temf_set_media_tensor(temf_ctx* ctx, const double* sig9, const double* mu9);
+/* Boundary condition (model_ctl 'boundary condition', :411-412): 0 = PEC,
+ * 1 = first-order absorbing boundary, the face integrals of
+ * surface_integral (:914-1007) added to the sigma-mass of every tet with a
+ * boundary face (:635-640).  face_mask (n_tets bytes, bit f = local face f
+ * (vertices ind_tri(f+1,:)) on the boundary) may be NULL: the faces that
+ * belong to one tet are used, which is what the reference's plane test finds
+ * on a convex mesh.  Takes effect at the next temf_assemble. */
+int temf_set_boundary(temf_ctx* ctx, int bound_cond, const unsigned char* face_mask);
 
 /* K1: assemble M_sigma (b_mkl) and the curl-curl matrix K (c_mkl) on the GPU:
  * mesh_process, src/FETD_FWD.f90:588-711.  Needs temf_analyse and media. */

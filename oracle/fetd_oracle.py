@@ -139,6 +139,15 @@ class Control:
     o_f: np.ndarray = field(default_factory=lambda: np.zeros(9, dtype=bool))
     time_channels: Optional[np.ndarray] = None
     vtk_num: int = 0
+    # anisotropic media (src/FETD_FWD.f90:368-410): per domain three principal
+    # values and three rotation angles (radians) of sigma, eps_r and mu_r
+    aniso: bool = False
+    sig_ani: Optional[np.ndarray] = None
+    sig_ang: Optional[np.ndarray] = None
+    per_ani: Optional[np.ndarray] = None
+    per_ang: Optional[np.ndarray] = None
+    mag_ani: Optional[np.ndarray] = None
+    mag_ang: Optional[np.ndarray] = None
 
 
 def read_cntl(path: str) -> Control:
@@ -172,7 +181,16 @@ def read_cntl(path: str) -> Control:
             c.per_dom = np.array([_f(r[2]) for r in rows]) * EPS0
             c.mag_dom = np.array([_f(r[3]) for r in rows]) * MU0
         elif code == "anisotropic":
-            raise NotImplementedError("anisotropic media are outside the restated path")
+            # three lines per domain (sigma, eps_r, mu_r): index, 3 values, 3 angles in degrees
+            k = int(val.split()[0])
+            rows = [[_f(t) for t in lines[i + q].split()[:7]] for q in range(3 * k)]
+            i += 3 * k
+            c.aniso = True
+            c.dom_ind = np.array([int(rows[3 * q][0]) for q in range(k)])
+            d2r = math.pi / 180.0
+            for off, nv, na in ((0, "sig_ani", "sig_ang"), (1, "per_ani", "per_ang"), (2, "mag_ani", "mag_ang")):
+                setattr(c, nv, np.array([rows[3 * q + off][1:4] for q in range(k)]))
+                setattr(c, na, np.array([rows[3 * q + off][4:7] for q in range(k)]) * d2r)
         elif code == "boundary condition":
             c.bound_cond = int(val.split()[0])
         elif code == "source":
@@ -308,6 +326,124 @@ def e_kind_iso(b, c, d, vol, tet_len, scal):
     coef = 4.0 * vol / (6.0 * vol) ** 4
     E = tet_len[:, :, None] * tet_len[:, None, :] * coef[:, None, None] * dots
     return E * scal[:, None, None]
+
+
+def rotation(ang) -> np.ndarray:
+    """dm = dx dy dz of the anisotropic media (src/FETD_FWD.f90:387-390), angles
+    in radians.  The reference's z rotation puts cos of the second angle at
+    its (2,2) entry; this is kept, so the result matches the reference's
+    tensors (a rotation only when that entry equals cos of the third angle)."""
+    a1, a2, a3 = ang
+    dx = np.array([[1.0, 0.0, 0.0], [0.0, math.cos(a1), -math.sin(a1)], [0.0, math.sin(a1), math.cos(a1)]])
+    dy = np.array([[math.cos(a2), 0.0, math.sin(a2)], [0.0, 1.0, 0.0], [-math.sin(a2), 0.0, math.cos(a2)]])
+    dz = np.array([[math.cos(a3), -math.sin(a3), 0.0], [math.sin(a3), math.cos(a2), 0.0], [0.0, 0.0, 1.0]])
+    return dx @ dy @ dz
+
+
+def media_tensor(values, ang) -> np.ndarray:
+    """dm diag(values) dm^T (src/FETD_FWD.f90:391-392)."""
+    dm = rotation(ang)
+    return dm @ np.diag(np.asarray(values, dtype=np.float64)) @ dm.T
+
+
+def f_kind_ani(b, c, d, vol, tet_len, S):
+    """Anisotropic mass integral  int N_i . S N_j dV, src/FETD_FWD.f90:884-912
+    (S: (T,3,3) per tet; the iso bracket with g_k . S g_l in place of g_k . g_l)."""
+    G = np.stack([b, c, d], axis=2)                         # (T,4,3)
+    H = np.einsum("tkx,txy,tly->tkl", G, S, G)              # (T,4,4)
+    F = np.empty((G.shape[0], 6, 6))
+    for i in range(6):
+        pi_, qi = IND_TET[i]
+        for j in range(6):
+            pj, qj = IND_TET[j]
+            v = (H[:, qi, qj] * (1 + (pi_ == pj))
+                 - H[:, pi_, qj] * (1 + (qi == pj))
+                 - H[:, qi, pj] * (1 + (pi_ == qj))
+                 + H[:, pi_, pj] * (1 + (qi == qj)))
+            F[:, i, j] = tet_len[:, i] * tet_len[:, j] / (vol * 720.0) * v
+    return F
+
+
+def e_kind_ani(b, c, d, vol, tet_len, Tm):
+    """Anisotropic curl-curl integral  V (curl N_i) . Tm (curl N_j),
+    src/FETD_FWD.f90:853-882, with Tm the elementwise reciprocal of the mu
+    tensor (0 where an entry is 0), as mesh_process passes it (:624-633)."""
+    G = np.stack([b, c, d], axis=2)
+    cr = np.cross(G[:, IND_TET[:, 0], :], G[:, IND_TET[:, 1], :])             # (T,6,3)
+    e = cr * (2.0 * tet_len / ((6.0 * vol) ** 2)[:, None])[:, :, None]
+    return vol[:, None, None] * np.einsum("tix,txy,tjy->tij", e, Tm, e)
+
+
+# local face i (vertices IND_TRI[i]) and its edges IND_EDG[i] with directions
+# IND_DIR[i], src/FETD_FWD.f90:24-26 (0-based)
+IND_TRI = np.array([[0, 2, 1], [3, 1, 2], [0, 3, 2], [0, 1, 3]])
+IND_EDG = np.array([[3, 0, 1], [3, 5, 4], [5, 1, 2], [4, 2, 0]])
+IND_DIR = np.array([[-1, -1, 1], [1, 1, 1], [-1, -1, 1], [-1, -1, 1]])
+
+
+def f_int_2d(x, y) -> np.ndarray:
+    """Triangle integral of the first-order ABC in local coordinates,
+    src/FETD_FWD.f90:990-1007 (restated as written)."""
+    length = np.array([math.hypot(x[0] - x[1], y[0] - y[1]), math.hypot(x[1] - x[2], y[1] - y[2]),
+                       math.hypot(x[2] - x[0], y[2] - y[0])])
+    area = 0.5 * (x[0] * (y[1] - y[2]) - y[0] * (x[1] - x[2]) + 1.0 * (x[1] * y[2] - x[2] * y[1]))
+    f = np.empty((3, 3))
+    for i in range(3):
+        for j in range(3):
+            v = (6.0 * (y[i] - y[2]) * (y[j] - y[2]) - 2.0 * (y[i] + y[j] - 2.0 * y[2]) * (y[0] + y[1] - 2.0 * y[2])
+                 + (y[0] - y[2]) ** 2 + (y[1] - y[2]) ** 2 + (y[0] - y[2]) * (y[1] - y[2])
+                 + 6.0 * (x[i] - x[2]) * (x[j] - x[2]) - 2.0 * (x[i] + x[j] - 2.0 * x[2]) * (x[0] + x[1] - 2.0 * x[2])
+                 + (x[0] - x[2]) ** 2 + (x[1] - x[2]) ** 2 + (x[0] - x[2]) * (x[1] - x[2]))
+            f[i, j] = v * length[i] * length[j] / 24.0 / area
+    return f
+
+
+def triangle_int(P: np.ndarray) -> np.ndarray:
+    """Local (u, v) coordinates of a 3-D triangle and its f_int_2d,
+    src/FETD_FWD.f90:976-989."""
+    u = np.zeros(3); v = np.zeros(3)
+    d21 = P[1] - P[0]; d31 = P[2] - P[0]
+    u[1] = math.sqrt(float(d21 @ d21))
+    u[2] = float(d31 @ d21) / u[1]
+    l31 = math.sqrt(float(d31 @ d31))
+    v[2] = math.sqrt(1.0 - (u[2] / l31) ** 2) * l31
+    return f_int_2d(u, v)
+
+
+def boundary_faces(nod_cor, tet_vex) -> np.ndarray:
+    """(T,4) bool: faces of the mesh boundary the way surface_integral finds
+    them (src/FETD_FWD.f90:928-950): no mesh node strictly on both sides of
+    the face's plane.  An interior face has the fourth vertices of its two
+    tets on opposite sides, so only faces that belong to one tet are tested."""
+    T = tet_vex.shape[0]
+    keys = np.sort(tet_vex[:, IND_TRI].reshape(T * 4, 3), axis=1)
+    _, inv, cnt = np.unique(keys, axis=0, return_inverse=True, return_counts=True)
+    cand = np.flatnonzero(cnt[inv.reshape(-1)] == 1)
+    out = np.zeros(T * 4, dtype=bool)
+    for q in cand:
+        t, i = divmod(int(q), 4)
+        P = nod_cor[tet_vex[t, IND_TRI[i]] - 1]
+        t1, t2 = P[1] - P[0], P[2] - P[0]
+        nrm = np.array([t1[1] * t2[2] - t1[2] * t2[1], -(t1[0] * t2[2] - t1[2] * t2[0]), t1[0] * t2[1] - t1[1] * t2[0]])
+        dd = -(nrm @ P[0])
+        tv = nod_cor @ nrm + dd
+        out[q] = not ((tv > 0.0).any() and (tv < 0.0).any())
+    return out.reshape(T, 4)
+
+
+def surface_integral(nod_cor, tet_vex, faces) -> np.ndarray:
+    """First-order ABC term per tet, (T,6,6): the face integrals of the
+    boundary faces on the tet's local edges, times sqrt(1.257e-6 / 8.85e-12)
+    (src/FETD_FWD.f90:914-959)."""
+    T = tet_vex.shape[0]
+    W = np.zeros((T, 6, 6))
+    for t, i in zip(*np.nonzero(faces)):
+        P = nod_cor[tet_vex[t, IND_TRI[i]] - 1]
+        f = triangle_int(P)
+        for j in range(3):
+            for k in range(3):
+                W[t, IND_EDG[i, j], IND_EDG[i, k]] += IND_DIR[i, j] * IND_DIR[i, k] * f[j, k]
+    return W * math.sqrt(1.257e-6 / 8.85e-12)
 
 
 def assemble_upper(n_edges: int, tet_edg, tet_drc, emat) -> sp.csr_matrix:
@@ -450,19 +586,39 @@ def build_model(mesh: Dict[str, np.ndarray], ctl: Control,
     edg_vex, tet_edg, tet_drc = build_topology(tet_vex)
     a, b, c, d, vol, tet_len = geometry(nod_cor, tet_vex)
     edg_len = np.sqrt(((nod_cor[edg_vex[:, 0] - 1] - nod_cor[edg_vex[:, 1] - 1]) ** 2).sum(axis=1))
-    # per-tet media, src/FETD_FWD.f90:347-364
-    sig = np.empty(tet_vex.shape[0]); mag = np.empty(tet_vex.shape[0])
-    found = np.zeros(tet_vex.shape[0], dtype=bool)
-    for j, dom in enumerate(ctl.dom_ind):
-        m = tet_phy == dom
-        sig[m] = ctl.sig_dom[j]; mag[m] = ctl.mag_dom[j]; found |= m
-    if not found.all():
-        raise ValueError("error - physical domain not found!")
-    if ctl.bound_cond != 0:
-        raise NotImplementedError("first-order ABC is outside the restated path")
+    T = tet_vex.shape[0]
+    sig = np.empty(T); mag = np.empty(T)
+    found = np.zeros(T, dtype=bool)
     n = edg_vex.shape[0]
-    Bm = assemble_upper(n, tet_edg, tet_drc, f_kind_iso(b, c, d, vol, tet_len, sig))
-    Cm = assemble_upper(n, tet_edg, tet_drc, e_kind_iso(b, c, d, vol, tet_len, 1.0 / mag))
+    if not ctl.aniso:
+        # per-tet media, src/FETD_FWD.f90:347-364
+        for j, dom in enumerate(ctl.dom_ind):
+            m = tet_phy == dom
+            sig[m] = ctl.sig_dom[j]; mag[m] = ctl.mag_dom[j]; found |= m
+        if not found.all():
+            raise ValueError("error - physical domain not found!")
+        Bt = f_kind_iso(b, c, d, vol, tet_len, sig)
+        Ct = e_kind_iso(b, c, d, vol, tet_len, 1.0 / mag)
+    else:
+        # tensors per tet (src/FETD_FWD.f90:381-409), element matrices (:621-634)
+        S = np.empty((T, 3, 3)); Mt = np.empty((T, 3, 3))
+        for j, dom in enumerate(ctl.dom_ind):
+            m = tet_phy == dom
+            S[m] = media_tensor(ctl.sig_ani[j], ctl.sig_ang[j])
+            Mt[m] = media_tensor(ctl.mag_ani[j], ctl.mag_ang[j]) * MU0
+            found |= m
+        if not found.all():
+            raise ValueError("error - physical domain not found!")
+        Tm = np.where(Mt == 0.0, 0.0, 1.0 / np.where(Mt == 0.0, 1.0, Mt))
+        Bt = f_kind_ani(b, c, d, vol, tet_len, S)
+        Ct = e_kind_ani(b, c, d, vol, tet_len, Tm)
+        sig = np.trace(S, axis1=1, axis2=2) / 3.0   # scalar summary; the adjoint is isotropic only
+        mag = np.trace(Mt, axis1=1, axis2=2) / 3.0
+    if ctl.bound_cond != 0:
+        # first-order absorbing boundary: b_mat += w_mat (src/FETD_FWD.f90:635-640)
+        Bt = Bt + surface_integral(nod_cor, tet_vex, boundary_faces(nod_cor, tet_vex))
+    Bm = assemble_upper(n, tet_edg, tet_drc, Bt)
+    Cm = assemble_upper(n, tet_edg, tet_drc, Ct)
     if src_edg is None:
         src_edg, src_drc = source_edges(edg_vex, mesh["src_vex"])
     if rec_tet is None:

@@ -51,6 +51,8 @@ SIGNATURES = {
     "temf_analysis_stats": (_i, [_p, _dp]),
     "temf_symbolic_host": (_i, [_i, C.POINTER(C.c_longlong), _ip, _dp, _ip, _dp]),
     "temf_adjoint_record": (_i, [_p, _i]),
+    "temf_set_media_tensor": (_i, [_p, _dp, _dp]),
+    "temf_set_boundary": (_i, [_p, _i, C.POINTER(C.c_ubyte)]),
     "temf_set_analysis_options": (_i, [_p, _i, _i]),
     "temf_tune_solve": (_i, [_p, _i, _i, _ip, _ip, _ip, _dp]),
     "temf_solve_schedule": (_i, [_p, _i, _ip, _ip]),

@@ -117,6 +117,7 @@ void run_adjoint(temf_ctx& c, const double* dJ, int rows, const int* tet_cell, i
                  double* grad_tet, AdjointResult& res) {
   AdjointRecord& A = c.adj;
   if (!A.valid) throw StateError("no recorded run: enable recording before temf_run");
+  if (c.aniso) throw StateError("the adjoint gradient covers isotropic conductivities");
   if ((int)A.row_node.size() != rows) throw ArgError("dJ has a different number of rows than the recorded run");
   res = AdjointResult();
   cudaStream_t st = c.stream;

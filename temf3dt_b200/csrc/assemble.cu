@@ -52,6 +52,91 @@ __global__ void __launch_bounds__(128) k_element_matrices(
   }
 }
 
+// The same for anisotropic media: per tet the conductivity tensor S and the
+// curl-curl tensor Tm (row-major, 9 doubles each).
+__global__ void __launch_bounds__(128) k_element_matrices_aniso(
+    int n_tets, const double* __restrict__ xyz, const int* __restrict__ tet_vex,
+    const int* __restrict__ tet_drc, const double* __restrict__ sig9, const double* __restrict__ tm9,
+    double* __restrict__ elemM, double* __restrict__ elemK) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_tets) return;
+  double X[4][3], S[9], Tm[9];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int v = tet_vex[4 * (int64_t)t + k];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[k][a] = xyz[3 * (int64_t)v + a];
+  }
+#pragma unroll
+  for (int a = 0; a < 9; ++a) {
+    S[a] = sig9[9 * (int64_t)t + a];
+    Tm[a] = tm9[9 * (int64_t)t + a];
+  }
+  double M21[21], K21[21];
+  aniso_elements(X, S, Tm, M21, K21);
+  double s[6];
+#pragma unroll
+  for (int j = 0; j < 6; ++j) s[j] = (double)tet_drc[6 * (int64_t)t + j];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+#pragma unroll
+    for (int j = i; j < 6; ++j) {
+      const int k = packed_upper(i, j);
+      const double sgn = s[i] * s[j];
+      elemM[(int64_t)k * n_tets + t] = sgn * M21[k];
+      elemK[(int64_t)k * n_tets + t] = sgn * K21[k];
+    }
+  }
+}
+
+// First-order absorbing boundary: for each tet with boundary faces (bits of
+// face_mask), add the faces' integrals (times sqrt(1.257e-6 / 8.85e-12),
+// orientation signs folded in) to its sigma-mass entries -- b_mat + w_mat of
+// mesh_process (src/FETD_FWD.f90:635-640).
+__global__ void __launch_bounds__(128) k_boundary_terms(int n_tets, const double* __restrict__ xyz,
+                                                        const int* __restrict__ tet_vex,
+                                                        const int* __restrict__ tet_drc,
+                                                        const unsigned char* __restrict__ face_mask,
+                                                        double* __restrict__ elemM) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_tets) return;
+  const unsigned mask = face_mask[t];
+  if (!mask) return;
+  double X[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int v = tet_vex[4 * (int64_t)t + k];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[k][a] = xyz[3 * (int64_t)v + a];
+  }
+  double W[6][6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int j = 0; j < 6; ++j) W[i][j] = 0.0;
+  for (int f = 0; f < 4; ++f) {
+    if (!(mask & (1u << f))) continue;
+    double P[3][3], F[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) P[k][a] = X[face_vertex(f, k)][a];
+    face_integral(P, F);
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) W[face_edge(f, j)][face_edge(f, k)] += face_dir(f, j) * face_dir(f, k) * F[j][k];
+  }
+  const double z0 = sqrt(1.257e-6 / 8.85e-12);
+  double s[6];
+#pragma unroll
+  for (int j = 0; j < 6; ++j) s[j] = (double)tet_drc[6 * (int64_t)t + j];
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int j = i; j < 6; ++j) elemM[(int64_t)packed_upper(i, j) * n_tets + t] += s[i] * s[j] * (W[i][j] * z0);
+}
+
 __global__ void __launch_bounds__(256) k_gather_nonzeros(
     int64_t nnz, const int* __restrict__ cptr, const int* __restrict__ cidx,
     const double* __restrict__ elemM, const double* __restrict__ elemK,
@@ -163,8 +248,41 @@ void upload_mesh(temf_ctx& c) {
 }
 
 void upload_media(temf_ctx& c) {
-  c.d_sig.upload(c.sig.data(), c.sig.size(), c.stream);
-  c.d_mu.upload(c.mu.data(), c.mu.size(), c.stream);
+  if (c.aniso) {
+    c.d_sig9.upload(c.sig9.data(), c.sig9.size(), c.stream);
+    c.d_tm9.upload(c.tm9.data(), c.tm9.size(), c.stream);
+  } else {
+    c.d_sig.upload(c.sig.data(), c.sig.size(), c.stream);
+    c.d_mu.upload(c.mu.data(), c.mu.size(), c.stream);
+  }
+}
+
+void boundary_face_mask(const temf_ctx& c, std::vector<unsigned char>& mask) {
+  // faces that belong to one tet; on a convex mesh these are the faces
+  // surface_integral's plane test finds (src/FETD_FWD.f90:928-950)
+  static const int fv[4][3] = {{0, 2, 1}, {3, 1, 2}, {0, 3, 2}, {0, 1, 3}};
+  const int T = c.n_tets;
+  struct Face {
+    int a, b, c;
+    int64_t q;  // 4 * tet + local face
+  };
+  std::vector<Face> faces((size_t)4 * T);
+  for (int t = 0; t < T; ++t)
+    for (int f = 0; f < 4; ++f) {
+      int v[3] = {c.tet_vex[4LL * t + fv[f][0]], c.tet_vex[4LL * t + fv[f][1]], c.tet_vex[4LL * t + fv[f][2]]};
+      std::sort(v, v + 3);
+      faces[4LL * t + f] = {v[0], v[1], v[2], 4LL * t + f};
+    }
+  std::sort(faces.begin(), faces.end(), [](const Face& x, const Face& y) {
+    return x.a != y.a ? x.a < y.a : (x.b != y.b ? x.b < y.b : x.c < y.c);
+  });
+  mask.assign(T, 0);
+  for (size_t i = 0; i < faces.size();) {
+    size_t j = i + 1;
+    while (j < faces.size() && faces[j].a == faces[i].a && faces[j].b == faces[i].b && faces[j].c == faces[i].c) ++j;
+    if (j - i == 1) mask[faces[i].q / 4] |= (unsigned char)(1u << (faces[i].q % 4));
+    i = j;
+  }
 }
 
 void upload_pattern(temf_ctx& c) {
@@ -181,9 +299,19 @@ void upload_pattern(temf_ctx& c) {
 
 void launch_assembly(temf_ctx& c) {
   const int T = c.n_tets;
-  k_element_matrices<<<ceil_div(T, 128), 128, 0, c.stream>>>(T, c.d_xyz.p, c.d_tet_vex.p, c.d_tet_drc.p,
-                                                             c.d_sig.p, c.d_mu.p, c.d_elemM.p, c.d_elemK.p);
+  if (c.aniso) {
+    k_element_matrices_aniso<<<ceil_div(T, 128), 128, 0, c.stream>>>(T, c.d_xyz.p, c.d_tet_vex.p, c.d_tet_drc.p,
+                                                                     c.d_sig9.p, c.d_tm9.p, c.d_elemM.p, c.d_elemK.p);
+  } else {
+    k_element_matrices<<<ceil_div(T, 128), 128, 0, c.stream>>>(T, c.d_xyz.p, c.d_tet_vex.p, c.d_tet_drc.p,
+                                                               c.d_sig.p, c.d_mu.p, c.d_elemM.p, c.d_elemK.p);
+  }
   TEMF_CHECK_LAUNCH();
+  if (c.bound_cond != 0) {
+    k_boundary_terms<<<ceil_div(T, 128), 128, 0, c.stream>>>(T, c.d_xyz.p, c.d_tet_vex.p, c.d_tet_drc.p,
+                                                             c.d_face_mask.p, c.d_elemM.p);
+    TEMF_CHECK_LAUNCH();
+  }
   const int64_t nnz = c.pat.nnz;
   k_gather_nonzeros<<<ceil_div(nnz, 256), 256, 0, c.stream>>>(nnz, c.d_contrib_ptr.p, c.d_contrib_idx.p,
                                                               c.d_elemM.p, c.d_elemK.p, c.d_M.p, c.d_K.p);

@@ -8,4 +8,6 @@ void upload_mesh(temf_ctx& c);
 void upload_media(temf_ctx& c);
 void upload_pattern(temf_ctx& c);
 void launch_assembly(temf_ctx& c);
+// bit f of mask[t] set when local face f of tet t lies on the mesh boundary
+void boundary_face_mask(const temf_ctx& c, std::vector<unsigned char>& mask);
 }  // namespace temf

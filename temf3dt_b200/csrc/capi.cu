@@ -384,6 +384,7 @@ int temf_set_media(temf_ctx* c, const double* sig, const double* mu) {
   return guarded(c, [&] {
     need(c->have_mesh, "temf_set_media: set the mesh first");
     if (!sig || !mu) throw ArgError("temf_set_media: NULL array");
+    c->aniso = false;
     c->sig.assign(sig, sig + c->n_tets);
     c->mu.assign(mu, mu + c->n_tets);
     for (int t = 0; t < c->n_tets; ++t)
@@ -394,6 +395,55 @@ int temf_set_media(temf_ctx* c, const double* sig, const double* mu) {
     c->slots[0].valid = c->slots[1].valid = false;
     upload_media(*c);
     TEMF_CUDA(cudaStreamSynchronize(c->stream));
+    return TEMF_OK;
+  });
+}
+
+int temf_set_media_tensor(temf_ctx* c, const double* sig9, const double* mu9) {
+  return guarded(c, [&] {
+    need(c->have_mesh, "temf_set_media_tensor: set the mesh first");
+    if (!sig9 || !mu9) throw ArgError("temf_set_media_tensor: NULL array");
+    const size_t m = 9 * (size_t)c->n_tets;
+    c->sig9.assign(sig9, sig9 + m);
+    c->tm9.resize(m);
+    for (size_t q = 0; q < m; ++q) {
+      if (!std::isfinite(sig9[q]) || !std::isfinite(mu9[q])) throw ArgError("media tensors must be finite");
+      c->tm9[q] = mu9[q] == 0.0 ? 0.0 : 1.0 / mu9[q];  // mesh_process's elementwise reciprocal (:624-633)
+    }
+    // scalar summaries (trace / 3) for the callers that read sigma per tet
+    c->sig.assign(c->n_tets, 0.0);
+    c->mu.assign(c->n_tets, 0.0);
+    for (int t = 0; t < c->n_tets; ++t) {
+      c->sig[t] = (sig9[9LL * t] + sig9[9LL * t + 4] + sig9[9LL * t + 8]) / 3.0;
+      c->mu[t] = (mu9[9LL * t] + mu9[9LL * t + 4] + mu9[9LL * t + 8]) / 3.0;
+    }
+    c->aniso = true;
+    c->have_media = true;
+    c->assembled = false;
+    c->adj.valid = false;
+    c->slots[0].valid = c->slots[1].valid = false;
+    upload_media(*c);
+    TEMF_CUDA(cudaStreamSynchronize(c->stream));
+    return TEMF_OK;
+  });
+}
+
+int temf_set_boundary(temf_ctx* c, int bound_cond, const unsigned char* face_mask) {
+  return guarded(c, [&] {
+    need(c->have_mesh, "temf_set_boundary: set the mesh first");
+    if (bound_cond != 0 && bound_cond != 1) throw ArgError("boundary condition must be 0 (PEC) or 1 (first-order ABC)");
+    c->bound_cond = bound_cond;
+    if (bound_cond) {
+      if (face_mask) c->face_mask.assign(face_mask, face_mask + c->n_tets);
+      else boundary_face_mask(*c, c->face_mask);
+      for (unsigned char v : c->face_mask)
+        if (v > 15) throw ArgError("face mask: 4 bits per tet");
+      c->d_face_mask.upload(c->face_mask.data(), c->face_mask.size(), c->stream);
+      TEMF_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    c->assembled = false;
+    c->adj.valid = false;
+    c->slots[0].valid = c->slots[1].valid = false;
     return TEMF_OK;
   });
 }

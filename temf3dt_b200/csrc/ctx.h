@@ -162,6 +162,13 @@ struct temf_ctx {
   std::vector<int> tet_edg;      // n_tets*6
   std::vector<int> tet_drc;      // n_tets*6
   std::vector<double> sig, mu;   // per tet
+  // anisotropic media: per tet row-major 3 x 3 conductivity tensor and the
+  // curl-curl tensor (elementwise reciprocal of the permeability tensor)
+  bool aniso = false;
+  std::vector<double> sig9, tm9;
+  // first-order absorbing boundary: 4 face bits per tet (0: PEC, no term)
+  int bound_cond = 0;
+  std::vector<unsigned char> face_mask;
   bool have_mesh = false, have_media = false;
   // symbolic + pattern
   temf::SymbolicOptions sym_opt;
@@ -169,7 +176,8 @@ struct temf_ctx {
   temf::Pattern pat;
   bool analysed = false;
   // device mesh / matrices
-  temf::DBuf<double> d_xyz, d_sig, d_mu;
+  temf::DBuf<double> d_xyz, d_sig, d_mu, d_sig9, d_tm9;
+  temf::DBuf<unsigned char> d_face_mask;
   temf::DBuf<int> d_tet_vex, d_tet_drc;
   temf::DBuf<int> d_rowptr, d_col, d_contrib_ptr, d_contrib_idx;
   temf::DBuf<double> d_elemM, d_elemK, d_M, d_K;

@@ -85,4 +85,100 @@ __device__ inline void unit_elements(const double X[4][3], double* M21, double* 
   }
 }
 
+// Anisotropic media (f_kind_ani, src/FETD_FWD.f90:884-912; e_kind_ani,
+// :853-882): the mass bracket with g_k . S g_l in place of g_k . g_l, and the
+// curl-curl term (curl N_i) . Tm (curl N_j) V, where S is the conductivity
+// tensor and Tm the tensor mesh_process passes for mu (the elementwise
+// reciprocal of the permeability tensor, :624-633).  Row-major 3 x 3 inputs;
+// 21 packed upper entries out, without orientation signs.
+__device__ inline void aniso_elements(const double X[4][3], const double* S, const double* Tm, double* M21,
+                                      double* K21) {
+  double g[4][3], vol;
+  tet_gradients(X, g, vol);
+  double len[6], cr[6][3];
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const int p = ind_tet(j, 0), q = ind_tet(j, 1);
+    const double dx = X[p][0] - X[q][0], dy = X[p][1] - X[q][1], dz = X[p][2] - X[q][2];
+    len[j] = sqrt(dx * dx + dy * dy + dz * dz);
+    cr[j][0] = g[p][1] * g[q][2] - g[q][1] * g[p][2];
+    cr[j][1] = g[q][0] * g[p][2] - g[p][0] * g[q][2];
+    cr[j][2] = g[p][0] * g[q][1] - g[q][0] * g[p][1];
+  }
+  double H[4][4];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    double sg[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) sg[a] = S[3 * a] * g[l][0] + S[3 * a + 1] * g[l][1] + S[3 * a + 2] * g[l][2];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) H[k][l] = g[k][0] * sg[0] + g[k][1] * sg[1] + g[k][2] * sg[2];
+  }
+  double tc[6][3];
+#pragma unroll
+  for (int j = 0; j < 6; ++j)
+#pragma unroll
+    for (int a = 0; a < 3; ++a) tc[j][a] = Tm[3 * a] * cr[j][0] + Tm[3 * a + 1] * cr[j][1] + Tm[3 * a + 2] * cr[j][2];
+  const double v6 = 6.0 * vol;
+  const double fM = 1.0 / (vol * 720.0);
+  const double fK = 4.0 * vol / (v6 * v6 * v6 * v6);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+#pragma unroll
+    for (int j = i; j < 6; ++j) {
+      const int pi = ind_tet(i, 0), qi = ind_tet(i, 1);
+      const int pj = ind_tet(j, 0), qj = ind_tet(j, 1);
+      const double br = H[qi][qj] * (1.0 + (pi == pj)) - H[pi][qj] * (1.0 + (qi == pj)) -
+                        H[qi][pj] * (1.0 + (pi == qj)) + H[pi][pj] * (1.0 + (qi == qj));
+      const double ll = len[i] * len[j];
+      const double dots = cr[i][0] * tc[j][0] + cr[i][1] * tc[j][1] + cr[i][2] * tc[j][2];
+      const int k = packed_upper(i, j);
+      M21[k] = ll * fM * br;
+      K21[k] = ll * fK * dots;
+    }
+  }
+}
+
+// First-order absorbing boundary (surface_integral, src/FETD_FWD.f90:914-1007):
+// local face f of a tet has vertices face_vertex(f, 0..2) and edges
+// face_edge(f, 0..2) with directions face_dir(f, 0..2) (ind_tri, ind_edg,
+// ind_dir, :24-26).  face_integral is triangle_int + f_int_2d as written.
+__device__ __forceinline__ int face_vertex(int f, int k) {
+  const int t[4][3] = {{0, 2, 1}, {3, 1, 2}, {0, 3, 2}, {0, 1, 3}};
+  return t[f][k];
+}
+__device__ __forceinline__ int face_edge(int f, int k) {
+  const int t[4][3] = {{3, 0, 1}, {3, 5, 4}, {5, 1, 2}, {4, 2, 0}};
+  return t[f][k];
+}
+__device__ __forceinline__ double face_dir(int f, int k) { return (k == 2 || f == 1) ? 1.0 : -1.0; }
+
+__device__ inline void face_integral(const double P[3][3], double F[3][3]) {
+  double d21[3], d31[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    d21[a] = P[1][a] - P[0][a];
+    d31[a] = P[2][a] - P[0][a];
+  }
+  const double u2 = sqrt(d21[0] * d21[0] + d21[1] * d21[1] + d21[2] * d21[2]);
+  const double u3 = (d31[0] * d21[0] + d31[1] * d21[1] + d31[2] * d21[2]) / u2;
+  const double l31 = sqrt(d31[0] * d31[0] + d31[1] * d31[1] + d31[2] * d31[2]);
+  const double r = u3 / l31;
+  const double v3 = sqrt(1.0 - r * r) * l31;
+  const double x[3] = {0.0, u2, u3}, y[3] = {0.0, 0.0, v3};
+  const double len[3] = {hypot(x[0] - x[1], y[0] - y[1]), hypot(x[1] - x[2], y[1] - y[2]),
+                         hypot(x[2] - x[0], y[2] - y[0])};
+  const double area = 0.5 * (x[0] * (y[1] - y[2]) - y[0] * (x[1] - x[2]) + 1.0 * (x[1] * y[2] - x[2] * y[1]));
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const double v = 6.0 * (y[i] - y[2]) * (y[j] - y[2]) - 2.0 * (y[i] + y[j] - 2.0 * y[2]) * (y[0] + y[1] - 2.0 * y[2]) +
+                       (y[0] - y[2]) * (y[0] - y[2]) + (y[1] - y[2]) * (y[1] - y[2]) + (y[0] - y[2]) * (y[1] - y[2]) +
+                       6.0 * (x[i] - x[2]) * (x[j] - x[2]) - 2.0 * (x[i] + x[j] - 2.0 * x[2]) * (x[0] + x[1] - 2.0 * x[2]) +
+                       (x[0] - x[2]) * (x[0] - x[2]) + (x[1] - x[2]) * (x[1] - x[2]) + (x[0] - x[2]) * (x[1] - x[2]);
+      F[i][j] = v * len[i] * len[j] / 24.0 / area;
+    }
+}
+
 }  // namespace temf

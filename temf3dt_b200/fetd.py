@@ -131,6 +131,23 @@ class FetdGPU:
         self._ck(self._L.temf_set_analysis_options(self._h, int(leaf_size), int(amalg_level)),
                  "temf_set_analysis_options")
 
+    def set_media_tensor(self, sig9, mu9) -> None:
+        """Anisotropic media: per tet row-major 3 x 3 conductivity and
+        (absolute) permeability tensors, shape (n_tets, 9)."""
+        s = as_f64(np.asarray(sig9, dtype=np.float64).reshape(-1))
+        m = as_f64(np.asarray(mu9, dtype=np.float64).reshape(-1))
+        self._ck(self._L.temf_set_media_tensor(self._h, dptr(s), dptr(m)), "temf_set_media_tensor")
+
+    def set_boundary(self, bound_cond: int, face_mask=None) -> None:
+        """0 = PEC, 1 = first-order absorbing boundary (face_mask: 4 bits per
+        tet; None = the faces that belong to one tet)."""
+        fm = None
+        if face_mask is not None:
+            fm = np.ascontiguousarray(face_mask, dtype=np.uint8)
+        self._ck(self._L.temf_set_boundary(self._h, int(bound_cond),
+                                           fm.ctypes.data_as(C.POINTER(C.c_ubyte)) if fm is not None else None),
+                 "temf_set_boundary")
+
     def analyse(self) -> None:
         self._ck(self._L.temf_analyse(self._h), "temf_analyse")
 
@@ -388,12 +405,15 @@ class FetdBatch:
 
 def load_case(gpu: FetdGPU, mesh: meshio.Mesh, ctl: meshio.Control, rec_tet: Optional[np.ndarray] = None):
     """model_mesh + model_ctl + mesh_process for one ``.mesh``/``.cntl`` pair."""
-    if ctl.bound_cond != 0:
-        raise NotImplementedError("only the PEC boundary (boundary condition: 0) is on the GPU path")
     edg_vex, tet_edg, tet_drc = mesh_topology(mesh.tet_vex)
     gpu.set_mesh(mesh.nod_cor, mesh.tet_vex, edg_vex, tet_edg, tet_drc)
-    sig, mu = meshio.media_per_tet(mesh.tet_phy, ctl)
-    gpu.set_media(sig, mu)
+    if ctl.aniso_domains:
+        sig, mu = meshio.media_tensors_per_tet(mesh.tet_phy, ctl)
+        gpu.set_media_tensor(sig, mu)
+    else:
+        sig, mu = meshio.media_per_tet(mesh.tet_phy, ctl)
+        gpu.set_media(sig, mu)
+    gpu.set_boundary(ctl.bound_cond)
     gpu.analyse()
     gpu.assemble()
     src_edg, src_drc = source_edges(edg_vex, mesh.src_vex)

@@ -95,6 +95,9 @@ class Control:
     output: np.ndarray = field(default_factory=lambda: np.zeros(9, dtype=bool))
     time_points: Optional[np.ndarray] = None
     vtkout: int = 0
+    # anisotropic media (src/FETD_FWD.f90:368-410): per domain
+    # (phys, (s1, s2, s3), (a1, a2, a3) degrees) for sigma, eps_r and mu_r
+    aniso_domains: List[tuple] = field(default_factory=list)
 
 
 def _parse(line: str):
@@ -135,7 +138,13 @@ def read_cntl(path: str) -> Control:
                 c.domains.append((int(t[0]), _num(t[1]), _num(t[2]), _num(t[3])))
             i += n
         elif k == "anisotropic":
-            raise NotImplementedError("anisotropic media are not part of the GPU path")
+            n = int(v.split()[0])
+            rows = [[_num(t) for t in L[i + q].split()[:7]] for q in range(3 * n)]
+            i += 3 * n
+            for q in range(n):
+                s, e, m = rows[3 * q], rows[3 * q + 1], rows[3 * q + 2]
+                c.aniso_domains.append((int(s[0]), (tuple(s[1:4]), tuple(s[4:7])), (tuple(e[1:4]), tuple(e[4:7])),
+                                        (tuple(m[1:4]), tuple(m[4:7]))))
         elif k == "boundary condition":
             c.bound_cond = int(v.split()[0])
         elif k == "source":
@@ -158,7 +167,8 @@ def read_cntl(path: str) -> Control:
             n = int(v.split()[0]); c.time_points = np.array([_num(L[i + q].split()[0]) for q in range(n)]); i += n
         elif k == "vtkout":
             c.vtkout = int(v.split()[0]); i += max(c.vtkout, 0)
-    if c.rec_cor is None or not len(c.rec_cor) or not c.domains or not c.src_num or not c.sp_mthd \
+    if c.rec_cor is None or not len(c.rec_cor) or not (c.domains or c.aniso_domains) or not c.src_num \
+            or not c.sp_mthd \
             or not c.sp_division or abs(c.time_maximum) < 1e-20 or not c.sp_double or not c.output.any():
         raise ValueError("%s: incomplete control file (src/FETD_FWD.f90:490-497)" % path)
     return c
@@ -170,9 +180,16 @@ def write_cntl(path: str, c: Control) -> None:
         for p in c.rec_cor:
             fh.write("%.10g %.10g %.10g\n" % tuple(p))
         fh.write("\nrec_charac: %.10g\n" % c.rec_charac)
-        fh.write("\nisotropic: %d\n" % len(c.domains))
-        for d in c.domains:
-            fh.write("%d %.10g %.10g %.10g\n" % d)
+        if c.aniso_domains:
+            fh.write("\nanisotropic: %d\n" % len(c.aniso_domains))
+            for phys, *parts in c.aniso_domains:
+                for vals, ang in parts:  # sigma, eps_r, mu_r lines
+                    fh.write("%d %s %s\n" % (phys, " ".join("%.10g" % v for v in vals),
+                                              " ".join("%.10g" % a for a in ang)))
+        else:
+            fh.write("\nisotropic: %d\n" % len(c.domains))
+            for d in c.domains:
+                fh.write("%d %.10g %.10g %.10g\n" % d)
         fh.write("\nboundary condition: %d\n" % c.bound_cond)
         fh.write("\n! TYPE 1 - STEPON / TYPE 2 - IMPULSE / TYPE 3 - STEPOFF\nsource: 1\n")
         fh.write("%d %d %.10g %.10g\n" % (c.source_type, c.pulse_type, c.t0, c.current))
@@ -184,6 +201,34 @@ def write_cntl(path: str, c: Control) -> None:
             for t in c.time_points:
                 fh.write("%.10g\n" % t)
         fh.write("\nvtkout: 0\n")
+
+
+def rotation(ang_deg) -> np.ndarray:
+    """dm = dx dy dz of the anisotropic media (src/FETD_FWD.f90:387-390),
+    angles in degrees.  The reference's z factor carries cos of the second
+    angle at its (2,2) entry, and so does this one (same tensors as the
+    reference)."""
+    a1, a2, a3 = np.radians(np.asarray(ang_deg, dtype=np.float64))
+    dx = np.array([[1.0, 0.0, 0.0], [0.0, np.cos(a1), -np.sin(a1)], [0.0, np.sin(a1), np.cos(a1)]])
+    dy = np.array([[np.cos(a2), 0.0, np.sin(a2)], [0.0, 1.0, 0.0], [-np.sin(a2), 0.0, np.cos(a2)]])
+    dz = np.array([[np.cos(a3), -np.sin(a3), 0.0], [np.sin(a3), np.cos(a2), 0.0], [0.0, 0.0, 1.0]])
+    return dx @ dy @ dz
+
+
+def media_tensors_per_tet(tet_phy: np.ndarray, ctl: Control):
+    """sig_a3d and mag_a3d per tet as (n_tets, 9) row-major arrays
+    (src/FETD_FWD.f90:381-409; mag includes mu0)."""
+    sig = np.full((len(tet_phy), 9), np.nan)
+    mu = np.full((len(tet_phy), 9), np.nan)
+    for phys, (sv, sa), _eps, (mv, ma) in ctl.aniso_domains:
+        m = tet_phy == phys
+        dm = rotation(sa)
+        sig[m] = (dm @ np.diag(sv) @ dm.T).reshape(9)
+        dm = rotation(ma)
+        mu[m] = (dm @ np.diag(mv) @ dm.T).reshape(9) * MU0
+    if np.isnan(sig).any():
+        raise ValueError("error - physical domain not found!")
+    return sig, mu
 
 
 def media_per_tet(tet_phy: np.ndarray, ctl: Control):

@@ -143,3 +143,57 @@ def adjoint_misfit_case(rows, seed: int = 0):
     mask = np.zeros_like(d_obs)
     mask[:, :, 3:9] = 1.0 / np.maximum(np.abs(rows[:, :, 3:9]).max(axis=0), 1e-300) ** 2
     return d_obs, mask
+
+
+# anisotropic variant of the tiny model: the earth gets a rotated conductivity
+# tensor and unequal (unrotated) relative permeabilities; air stays isotropic
+ANISO_EARTH = ((1e-3, 2e-3, 5e-4), (10.0, 20.0, 30.0))
+ANISO_EARTH_MU = ((1.0, 1.2, 0.9), (0.0, 0.0, 0.0))
+
+
+def aniso_controls(model, bound_cond: int = 1):
+    """(host Control, oracle Control) of a synthetic model with anisotropic
+    media in the earth and the given boundary condition."""
+    import copy
+    import math
+    from temf3dt_b200 import meshio as MI
+    hc = copy.deepcopy(model.ctl)
+    hc.aniso_domains = []
+    for phys, sig, epsr, mur in hc.domains:
+        if sig > 1e-6:
+            hc.aniso_domains.append((phys, ANISO_EARTH, ((1.0,) * 3, (0.0,) * 3), ANISO_EARTH_MU))
+        else:
+            hc.aniso_domains.append((phys, ((sig,) * 3, (0.0,) * 3), ((epsr,) * 3, (0.0,) * 3), ((mur,) * 3, (0.0,) * 3)))
+    hc.domains = []
+    hc.bound_cond = bound_cond
+    oc = copy.copy(synth_oracle_model_control(model))
+    oc.aniso = True
+    oc.bound_cond = bound_cond
+    d2r = math.pi / 180.0
+    oc.dom_ind = np.array([d[0] for d in hc.aniso_domains])
+    oc.sig_ani = np.array([d[1][0] for d in hc.aniso_domains])
+    oc.sig_ang = np.array([d[1][1] for d in hc.aniso_domains]) * d2r
+    oc.per_ani = np.array([d[2][0] for d in hc.aniso_domains])
+    oc.per_ang = np.array([d[2][1] for d in hc.aniso_domains]) * d2r
+    oc.mag_ani = np.array([d[3][0] for d in hc.aniso_domains])
+    oc.mag_ang = np.array([d[3][1] for d in hc.aniso_domains]) * d2r
+    assert isinstance(MI.Control(), type(hc))
+    return hc, oc
+
+
+def synth_oracle_model_control(model) -> O.Control:
+    """The oracle Control of a synthetic model (isotropic, as built)."""
+    c = model.ctl
+    return O.Control(rec_cor=c.rec_cor, rec_charac=c.rec_charac,
+                     dom_ind=np.array([d[0] for d in c.domains]), sig_dom=np.array([d[1] for d in c.domains]),
+                     per_dom=np.array([d[2] for d in c.domains]) * O.EPS0,
+                     mag_dom=np.array([d[3] for d in c.domains]) * O.MU0,
+                     src_num=1, src_sourcetype=c.source_type, src_pulsetype=c.pulse_type, src_pulsewidth=c.t0,
+                     src_current=c.current, step_mthd=2, step_dvsi=c.sp_division, time_maxm=c.time_maximum,
+                     step_dble=c.sp_double, step_dblesize=c.sp_dblesize, o_f=c.output, time_channels=c.time_points)
+
+
+def oracle_model_with(model, oc):
+    mesh = dict(nod_cor=model.mesh.nod_cor, tet_vex=model.mesh.tet_vex, tet_phy=model.mesh.tet_phy,
+                src_vex=model.mesh.src_vex, src_phy=model.mesh.src_phy)
+    return O.build_model(mesh, oc)
