@@ -152,14 +152,20 @@ def test_field_roundtrip(tmp_path):
     assert np.allclose(r[:, 2:].reshape(4, 2, 2), f[:, :, [3, 5]], rtol=1e-5)
 
 
-@pytest.mark.parametrize("kind", ["halfspace", "multiloop"])
+@pytest.mark.parametrize("kind", ["halfspace", "multiloop", "layered"])
 def test_synth_models(kind):
-    kw = dict(h_core=250, ratio=2.5, h_z=50, z_core=150) if kind == "halfspace" else \
-        dict(n_loops=3, h_core=60, ratio=2.2, h_z=60, scale=1.0)
+    kw = {"halfspace": dict(h_core=250, ratio=2.5, h_z=50, z_core=150),
+          "multiloop": dict(n_loops=3, h_core=60, ratio=2.2, h_z=60, scale=1.0),
+          "layered": dict(scale=0.2, ratio=2.5, seed=4)}[kind]
     m = synth.build_model(kind, **kw)
     P = m.mesh.nod_cor[m.mesh.tet_vex - 1]
     d = np.einsum("ti,ti->t", P[:, 1] - P[:, 0], np.cross(P[:, 2] - P[:, 0], P[:, 3] - P[:, 0]))
     assert (d > 0).all()
+    if kind == "layered":
+        # 3-6 layers with conductivities in [1e-4, 1e-1] S/m under air
+        sig = [dom[1] for dom in m.ctl.domains[1:]]
+        assert 3 <= len(sig) <= 6 and all(1e-4 <= v <= 1e-1 for v in sig)
+        assert set(np.unique(m.mesh.tet_phy)) <= {dom[0] for dom in m.ctl.domains}
     ev, _, _ = fetd.mesh_topology(m.mesh.tet_vex)
     cols = m.source_columns(ev)
     se, sd = fetd.source_edges(ev, m.mesh.src_vex)
