@@ -289,8 +289,10 @@ int temf_analysis_stats(temf_ctx* ctx, double* stats);
 int temf_symbolic_host(int n, const long long* xadj, const int* adj, const double* xyz, int* perm_out,
                        double* stats);
 
-/* Host-only check of the triangular-solve schedules built from the same
- * analysis (no GPU needed; no reference counterpart): replays both sweeps,
+/* Host-only check of an analysis (no GPU needed; for the factor structure
+ * the analogue of pardiso_checker, src/FETD_UTILITY.f90:993-1027): the
+ * supernode row lists (ascending, below the diagonal block, every child row
+ * inside its parent's panel), then the triangular-solve schedules replayed,
  * claimed in order and through the ready queue, for both chunk heights.
  * Returns 0, or 1 with the first violation in msg. */
 int temf_schedule_check(int n, const long long* xadj, const int* adj, const double* xyz, char* msg, int msg_len);

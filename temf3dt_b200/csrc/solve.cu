@@ -1606,7 +1606,44 @@ void solve_timeline(temf_ctx& c, int slot, const double* b_perm, int64_t cap, un
   }
 }
 
+// Structure of the supernodal partition (the analogue of pardiso_checker,
+// src/FETD_UTILITY.f90:993-1027, for the factor): row lists ascending and
+// below the diagonal block, the parent owning the first row, and every row
+// of a child either a column or a row of its parent (the Schur update of
+// the child lands inside the parent's panel).
+static std::string check_structure(const Symbolic& S) {
+  for (int s = 0; s < S.nsn; ++s) {
+    const int f = S.sn_first[s], l = S.sn_first[s + 1];
+    if (l <= f) return "empty supernode";
+    const int* b = S.sn_rows.data() + S.sn_rows_ptr[s];
+    const int* e = S.sn_rows.data() + S.sn_rows_ptr[s + 1];
+    for (const int* q = b; q < e; ++q) {
+      if (*q < l || *q >= S.n) return "row list outside the lower triangle";
+      if (q > b && q[-1] >= *q) return "row list not ascending";
+    }
+    const int p = S.sn_parent[s];
+    if (b == e) {
+      if (p >= 0) return "supernode without rows has a parent";
+      continue;
+    }
+    if (p != S.col2sn[*b]) return "parent does not own the first row";
+    const int fp = S.sn_first[p], lp = S.sn_first[p + 1];
+    const int* pb = S.sn_rows.data() + S.sn_rows_ptr[p];
+    const int* pe = S.sn_rows.data() + S.sn_rows_ptr[p + 1];
+    for (const int* q = b; q < e; ++q) {
+      if (*q >= fp && *q < lp) continue;
+      if (!std::binary_search(pb, pe, *q)) return "child row missing from its parent";
+    }
+    if (S.sn_level[p] <= S.sn_level[s]) return "parent not on a higher level";
+  }
+  return std::string();
+}
+
 std::string check_schedules(const Symbolic& S) {
+  {
+    const std::string w = check_structure(S);
+    if (!w.empty()) return "supernode structure: " + w;
+  }
   const int splits[5] = {0, level_below_width(S, 2048), default_split(S), level_below_width(S, 64), S.nlevels};
   for (int sp : splits) {
     std::string w = check_schedule(S, kChunkRows, sp);

@@ -39,8 +39,9 @@ struct SweepView {
 };
 
 void build_solve_plan(temf_ctx& c);
-// Host replay of the sweep schedules of a symbolic analysis (both chunk
-// heights; claim order and ready queue).  Empty string, or the violation.
+// Host check of a symbolic analysis: supernode structure, then the sweep
+// schedules replayed (both chunk heights; claim order and ready queue).
+// Empty string, or the violation.
 std::string check_schedules(const Symbolic& S);
 void ensure_update_buffer(temf_ctx& c, int nrhs);
 
