@@ -289,9 +289,7 @@ int temf_analysis_stats(temf_ctx* ctx, double* stats);
 int temf_symbolic_host(int n, const long long* xadj, const int* adj, const double* xyz, int* perm_out,
                        double* stats);
 
-/* Host-only check of an analysis (no GPU needed; for the factor structure
- * the analogue of pardiso_checker, src/FETD_UTILITY.f90:993-1027): the
- * supernode row lists (ascending, below the diagonal block, every child row
+/* Host-only check of an analysis (no GPU needed): the supernode row lists (ascending, below the diagonal block, every child row
  * inside its parent's panel), then the triangular-solve schedules replayed,
  * claimed in order and through the ready queue, for both chunk heights.
  * Returns 0, or 1 with the first violation in msg. */
@@ -303,6 +301,15 @@ int temf_schedule_check(int n, const long long* xadj, const int* adj, const doub
  * direct_1 takes the 1-based upper CSR (ia, ja, va) of A; its pattern must be
  * the assembled step-matrix pattern of the mesh set on the context (the
  * pattern mkl_add_3 produces), which is checked. */
+/* pardiso_checker (src/FETD_UTILITY.f90:993-1027), host only: the CSR
+ * structure checks the reference asks of MKL's sparse matrix checker (ia(1) =
+ * 1, ia(n+1)-1 = nnz, ia non-decreasing, ja in 1..n and strictly ascending per
+ * row, upper triangle when symm != 0).  *checker = 1 if the structure is
+ * valid, else 0 with the first violation in msg; returns 0, or TEMF_EARG for
+ * null pointers.  temf_pardiso_direct_1 runs the same checks and fails with
+ * TEMF_EARG where the reference stops with "matrix error!". */
+int temf_pardiso_checker(int symm, int n, int nnz, const int* ia, const int* ja, int* checker, char* msg,
+                         int msg_len);
 int temf_pardiso_alloc(temf_ctx* ctx, int max_matrix);
 int temf_pardiso_direct_1(temf_ctx* ctx, int num_m, int symm, int n, int nnz, const int* ia, const int* ja,
                           const double* va);

@@ -67,6 +67,7 @@ SIGNATURES = {
     "temf_batch_set_tuning": (_i, [_p, _i, _i]),
     "temf_adjoint": (_i, [_p, _dp, _i, _ip, _dp, _dp]),
     "temf_adjoint_timing": (_i, [_p, _dp, C.POINTER(C.c_longlong)]),
+    "temf_pardiso_checker": (_i, [_i, _i, _i, _ip, _ip, _ip, C.c_char_p, _i]),
     "temf_pardiso_alloc": (_i, [_p, _i]),
     "temf_pardiso_direct_1": (_i, [_p, _i, _i, _i, _i, _ip, _ip, _dp]),
     "temf_pardiso_direct_2": (_i, [_p, _i, _dp, _dp]),

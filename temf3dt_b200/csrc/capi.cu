@@ -2,8 +2,10 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <string>
 
 #include "../../include/temf_b200.h"
 #include "adjoint.h"
@@ -1141,6 +1143,63 @@ int temf_schedule_check(int n, const long long* xadj, const int* adj, const doub
 }
 
 // ---- PARDISO shim -----------------------------------------------------------
+}  // extern "C"
+
+// The structure checks of MKL's sparse matrix checker as pardiso_checker
+// (src/FETD_UTILITY.f90:993-1027) configures it: 1-based CSR, ia(1) = 1,
+// ia(n+1) - 1 = nnz, ia non-decreasing, column indices in 1..n and strictly
+// ascending within a row, and for the symmetric case only the upper
+// triangle.  Empty string, or the first violation with its row and position.
+static std::string check_user_csr(int symm, int n, int nnz, const int* ia, const int* ja) {
+  char buf[160];
+  if (n <= 0 || nnz < 0) return "n must be positive and nnz non-negative";
+  if (ia[0] != 1) return "ia(1) must be 1 (one-based indexing)";
+  if ((long long)ia[n] - 1 != nnz) {
+    std::snprintf(buf, sizeof buf, "ia(n+1)-1 = %d differs from nnz = %d", ia[n] - 1, nnz);
+    return buf;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (ia[i + 1] < ia[i]) {
+      std::snprintf(buf, sizeof buf, "ia decreases at row %d", i + 1);
+      return buf;
+    }
+    for (int q = ia[i] - 1; q < ia[i + 1] - 1; ++q) {
+      const int j = ja[q];
+      if (j < 1 || j > n) {
+        std::snprintf(buf, sizeof buf, "column index %d out of range in row %d (position %d)", j, i + 1, q + 1);
+        return buf;
+      }
+      if (symm && j < i + 1) {
+        std::snprintf(buf, sizeof buf, "entry (%d,%d) below the diagonal of an upper-triangular matrix", i + 1, j);
+        return buf;
+      }
+      if (q > ia[i] - 1 && j <= ja[q - 1]) {
+        std::snprintf(buf, sizeof buf, "column indices not strictly ascending in row %d (position %d)", i + 1, q + 1);
+        return buf;
+      }
+    }
+  }
+  return std::string();
+}
+
+extern "C" {
+
+int temf_pardiso_checker(int symm, int n, int nnz, const int* ia, const int* ja, int* checker, char* msg,
+                         int msg_len) {
+  if (!ia || !checker || (nnz > 0 && !ja)) return TEMF_EARG;
+  try {
+    const std::string w = check_user_csr(symm, n, nnz, ia, ja);
+    *checker = w.empty() ? 1 : 0;
+    if (msg && msg_len > 0) {
+      std::strncpy(msg, w.c_str(), msg_len - 1);
+      msg[msg_len - 1] = 0;
+    }
+    return TEMF_OK;
+  } catch (...) {
+    return TEMF_EINTERNAL;
+  }
+}
+
 int temf_pardiso_alloc(temf_ctx* c, int max_matrix) {
   return guarded(c, [&] {
     if (max_matrix < 1 || max_matrix > 2) throw ArgError("maximum number of matrix error (1 or 2 slots)");
@@ -1158,16 +1217,17 @@ int temf_pardiso_direct_1(temf_ctx* c, int num_m, int symm, int n, int nnz, cons
     if (!symm) throw ArgError("only the symmetric (mtype 2) path of the reference is supported");
     need(c->analysed, "temf_pardiso_direct_1: the mesh pattern must be analysed (temf_analyse)");
     if (n != c->n_edges || !ia || !ja || !va || nnz <= 0) throw ArgError("matrix size differs from the mesh");
-    if (ia[0] != 1 || ia[n] - 1 != nnz) throw ArgError("matrix error: ia must be 1-based with ia(n+1)-1 = nnz");
+    {
+      const std::string w = check_user_csr(symm, n, nnz, ia, ja);
+      if (!w.empty()) throw ArgError("matrix error: " + w);
+    }
     if (X.shim_n != n || X.shim_nnz != nnz || X.shim_map.size() != (size_t)nnz) {
       // map each user entry (upper, 1-based) onto the permuted lower pattern
       const Pattern& P = c->pat;
       X.shim_map.assign(nnz, -1);
       for (int i = 0; i < n; ++i) {
-        if (ia[i + 1] < ia[i]) throw ArgError("matrix error: ia not monotone");
         for (int q = ia[i] - 1; q < ia[i + 1] - 1; ++q) {
           const int j = ja[q] - 1;
-          if (j < i || j >= n) throw ArgError("matrix error: entries must be in the upper triangle");
           int pi = c->sym.iperm[i], pj = c->sym.iperm[j];
           if (pi < pj) std::swap(pi, pj);  // lower triangle of the permuted matrix: row pi, col pj
           const int* b = P.col.data() + P.rowptr[pi];

@@ -54,6 +54,18 @@ def source_edges(edg_vex: np.ndarray, src_vex: np.ndarray):
     return (pos + 1).astype(np.int32), drc
 
 
+def pardiso_checker(symm: bool, ia, ja) -> Tuple[bool, str]:
+    """Structure check of a 1-based CSR matrix (pardiso_checker,
+    src/FETD_UTILITY.f90:993-1027): (valid, first violation or "")."""
+    ia, ja = as_i32(ia), as_i32(ja)
+    ok = np.zeros(1, dtype=np.int32)
+    msg = C.create_string_buffer(256)
+    rc = lib().temf_pardiso_checker(1 if symm else 0, len(ia) - 1, len(ja), iptr(ia), iptr(ja), iptr(ok), msg, 256)
+    if rc != 0:
+        raise TemfError(rc, "temf_pardiso_checker")
+    return bool(ok[0]), msg.value.decode()
+
+
 @dataclass
 class RunOutput:
     steps: np.ndarray

@@ -52,3 +52,47 @@ def test_host_entry_points_return_error_codes():
     # empty or NULL input to the host-only analysis
     assert L.temf_symbolic_host(0, None, None, None, None, None) < 0
     assert L.temf_schedule_check(0, None, None, None, None, 0) < 0
+
+
+def _upper_csr_of_mesh():
+    """1-based upper CSR of the edge-adjacency pattern (with the diagonal) of
+    the small synthetic mesh: the structure adap_euler hands to
+    pardiso_direct_1."""
+    import scipy.sparse as sp
+    from temf3dt_b200 import fetd
+    m = tiny_synth()
+    ev, te, _ = fetd.mesh_topology(m.mesh.tet_vex)
+    n, T = ev.shape[0], te.shape[0]
+    I = sp.csr_matrix((np.ones(6 * T), (np.repeat(np.arange(T), 6), (te - 1).reshape(-1))), shape=(T, n))
+    A = sp.triu((I.T @ I).tocsr()).tocsr()
+    A.sort_indices()
+    return (A.indptr + 1).astype(np.int32), (A.indices + 1).astype(np.int32)
+
+
+def test_pardiso_checker_accepts_the_step_pattern_and_rejects_planted_errors():
+    from temf3dt_b200 import fetd
+    ia, ja = _upper_csr_of_mesh()
+    assert fetd.pardiso_checker(True, ia, ja) == (True, "")
+    assert fetd.pardiso_checker(False, ia, ja)[0]
+    r = 5                       # a row with several entries
+    q0, q1 = ia[r] - 1, ia[r + 1] - 1
+    assert q1 - q0 >= 3
+    bad = ja.copy(); bad[q0 + 1], bad[q0 + 2] = bad[q0 + 2], bad[q0 + 1]
+    ok, msg = fetd.pardiso_checker(True, ia, bad)
+    assert not ok and "ascending" in msg and "row %d" % (r + 1) in msg
+    bad = ja.copy(); bad[q0 + 2] = bad[q0 + 1]          # duplicate entry
+    assert not fetd.pardiso_checker(True, ia, bad)[0]
+    bad = ja.copy(); bad[q0] = r                         # (r+1, r) is below the diagonal
+    ok, msg = fetd.pardiso_checker(True, ia, bad)
+    assert not ok and "below the diagonal" in msg
+    assert fetd.pardiso_checker(False, ia, bad)[0]       # a general matrix may hold it
+    bad = ja.copy(); bad[-1] = len(ia)                   # column n + 1
+    ok, msg = fetd.pardiso_checker(True, ia, bad)
+    assert not ok and "out of range" in msg
+    ok, msg = fetd.pardiso_checker(True, ia - 1, ja)     # zero-based row pointers
+    assert not ok and "one-based" in msg
+    ok, msg = fetd.pardiso_checker(True, ia, ja[:-1])    # nnz disagrees with ia(n+1)
+    assert not ok and "nnz" in msg
+    L = _lib.lib()
+    ck = np.zeros(1, dtype=np.int32)
+    assert L.temf_pardiso_checker(1, len(ia) - 1, len(ja), None, _lib.iptr(ja), _lib.iptr(ck), None, 0) < 0
