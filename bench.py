@@ -25,7 +25,8 @@ traces copied back.
 --impl reference: the reference's CPU path is Intel Fortran + MKL PARDISO,
 which cannot be built or run here; its CPU restatement (oracle/, SuperLU
 factorisation) is timed instead on a bounded sample of the same model family
-(reduced resolution, a fixed number of leading time steps).
+(reduced resolution, a fixed number of leading time steps), one
+single-threaded sample per host core, all started together.
 """
 from __future__ import annotations
 
@@ -48,8 +49,10 @@ CONFIGS = {
     2: dict(kind="multiloop", kw=dict(), label="block3d-64-loops-64rhs"),
 }
 COMMON = dict(t0=1e-6, sp_division=10, sp_double=100, time_maximum=1e-2)
-# the CPU restatement factors and solves with SuperLU, which runs on one thread
-CPU_THREADS = 1
+# the CPU restatement factors and solves with SuperLU, which runs on one
+# thread; the host's cores are used by one independent sample per core
+# (steps*RHS/s is a throughput: a CPU job runs its sources side by side)
+CPU_WORKER_BYTES = 1.5e9   # peak RSS of one reduced-model sample is ~0.8 GB
 
 
 def model_for(cfg: int, reduced: bool = False):
@@ -124,18 +127,106 @@ def measured_dgemm_tflops(torch) -> float:
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_sample(cfg: int, max_steps: int):
-    """The oracle on a bounded sample: reduced-resolution model, leading steps."""
-    from oracle import fetd_oracle as O
-    from tests.golden_cases import synth_oracle_model
-    m = model_for(cfg, reduced=True)
-    om = synth_oracle_model(m)
-    t = time.perf_counter()
-    res = O.run_fetd(om, max_steps=max_steps)
-    dt = time.perf_counter() - t
-    nrhs = 1
-    steps = len(res.steps) - 1
-    return steps * nrhs / dt, dict(n_edges=om.n, steps=steps, seconds=dt)
+def cpu_sample_text(info) -> str:
+    return ("CPU restatement (oracle/, SuperLU) on the %d-edge reduced-resolution model, first %d time steps, "
+            "%d single-threaded samples side by side (one per core, %.1f s each); MKL PARDISO reference not "
+            "buildable here" % (info["n_edges"], info["steps"], info["workers"], info["sample_seconds"]))
+
+
+def cpu_workers() -> int:
+    """Host threads the CPU arm may use: the cores this process may run on,
+    bounded by the free memory at CPU_WORKER_BYTES per sample."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    try:
+        import psutil
+        n = min(n, int(psutil.virtual_memory().available // CPU_WORKER_BYTES))
+    except ImportError:
+        pass
+    return max(1, n)
+
+
+def _cpu_worker(cfg: int, max_steps: int, starts, out):
+    """One single-threaded sample process: build the reduced model once, then
+    run the oracle's leading time steps once per round, released together."""
+    try:
+        from oracle import fetd_oracle as O
+        from tests.golden_cases import synth_oracle_model
+        om = synth_oracle_model(model_for(cfg, reduced=True))
+        out.put(("ready",))
+        for ev in starts:
+            ev.wait()
+            t = time.perf_counter()
+            res = O.run_fetd(om, max_steps=max_steps)
+            out.put(("done", len(res.steps) - 1, time.perf_counter() - t, om.n))
+    except Exception as e:  # noqa: BLE001 - reported to the parent
+        out.put(("error", repr(e)))
+
+
+def _collect(q, procs, count: int, kind: str, limit_s: float):
+    """`count` messages of `kind` from the workers; a worker that failed or
+    exited, or the time limit, ends the wait with an error."""
+    import queue
+    got, t_end = [], time.monotonic() + limit_s
+    while len(got) < count:
+        try:
+            msg = q.get(timeout=2.0)
+        except queue.Empty:
+            dead = [p.exitcode for p in procs if p.exitcode not in (None, 0)]
+            if dead:
+                raise RuntimeError("CPU sample worker exited with code %s" % dead[0])
+            if time.monotonic() > t_end:
+                raise RuntimeError("CPU sample workers did not finish within %.0f s" % limit_s)
+            continue
+        if msg[0] == "error":
+            raise RuntimeError("CPU sample worker failed: %s" % msg[1])
+        if msg[0] == kind:
+            got.append(msg)
+    return got
+
+
+def cpu_parallel(cfg: int, max_steps: int, rounds: int, workers: int):
+    """The oracle on `workers` cores at once (spawned processes, one BLAS
+    thread each).  Per round: steps of all samples / wall time from the
+    common start to the last sample's end."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    keys = ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")
+    saved = {k: os.environ.get(k) for k in keys}
+    for k in keys:
+        os.environ[k] = "1"
+    starts = [ctx.Event() for _ in range(rounds)]
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_cpu_worker, args=(cfg, max_steps, starts, q), daemon=True) for _ in range(workers)]
+    try:
+        for p in procs:
+            p.start()
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    vals, info = [], None
+    try:
+        _collect(q, procs, workers, "ready", 1800)
+        for ev in starts:
+            t = time.perf_counter()
+            ev.set()
+            got = _collect(q, procs, workers, "done", 3600)
+            wall = time.perf_counter() - t
+            vals.append(sum(g[1] for g in got) / wall)
+            info = dict(n_edges=got[0][3], steps=got[0][1], seconds=wall, workers=workers,
+                        sample_seconds=float(np.mean([g[2] for g in got])))
+    finally:
+        for p in procs:
+            p.join(timeout=5 if vals and len(vals) == rounds else 0.1)
+            if p.is_alive():
+                p.terminate()
+                p.join(timeout=10)
+    return vals, info
 
 
 def inversion_cells(m, shape=(32, 32, 16), box=((-640.0, 640.0), (-640.0, 640.0), (0.0, 400.0))):
@@ -262,14 +353,9 @@ def reference_arm(args):
     if rank != 0:
         return 0
     cfg = args.config
-    vals = []
-    info = None
-    for k in range(args.warmup + args.steps):
-        v, info = cpu_sample(cfg, args.sample_steps)
-        if k >= args.warmup:
-            vals.append(v)
-    value = float(np.mean(vals))
-    cores = CPU_THREADS
+    cores = cpu_workers()
+    vals, info = cpu_parallel(cfg, args.sample_steps, args.warmup + args.steps, cores)
+    value = float(np.mean(vals[args.warmup:]))
     line = {
         "impl": "reference", "metric": "FETD steps*RHS/s", "value": value, "unit": "steps*RHS/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -278,8 +364,7 @@ def reference_arm(args):
         "config": {"workload": CONFIGS[cfg]["label"], "sample": "reduced-resolution model, first %d time steps"
                    % args.sample_steps},
         "cpu_baseline": {"value": value, "unit": "steps*RHS/s", "cores": cores, "kind": "port",
-                         "sample": "CPU restatement (oracle/, single-threaded SuperLU) on the %d-edge reduced model, "
-                                   "%d steps; MKL PARDISO reference not buildable here" % (info["n_edges"], info["steps"])},
+                         "sample": cpu_sample_text(info)},
         "e2e": {"value": value, "unit": "steps*RHS/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -419,10 +504,9 @@ def ours(args):
                 "factor": {"achieved_tflops": factor_rate, "peak_dgemm_tflops": dgemm, "frac": factor_rate / dgemm}}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, inf = cpu_sample(cfg, args.sample_steps)
-        cpu = {"value": v, "unit": "steps*RHS/s", "cores": CPU_THREADS,
-               "kind": "port", "sample": "CPU restatement (oracle/, single-threaded SuperLU) on the %d-edge reduced-resolution model, "
-                                         "first %d time steps" % (inf["n_edges"], inf["steps"])}
+        nw = cpu_workers()
+        vs, inf = cpu_parallel(cfg, args.sample_steps, 1, nw)
+        cpu = {"value": vs[0], "unit": "steps*RHS/s", "cores": nw, "kind": "port", "sample": cpu_sample_text(inf)}
     line = {
         "metric": "FETD steps*RHS/s", "value": value, "unit": "steps*RHS/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
