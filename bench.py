@@ -135,11 +135,19 @@ def cpu_sample_text(info) -> str:
 
 def cpu_workers() -> int:
     """Host threads the CPU arm may use: the cores this process may run on,
-    bounded by the free memory at CPU_WORKER_BYTES per sample."""
+    bounded by the container's CPU quota and by the free memory at
+    CPU_WORKER_BYTES per sample."""
     try:
         n = len(os.sched_getaffinity(0))
     except AttributeError:
         n = os.cpu_count() or 1
+    try:
+        with open("/sys/fs/cgroup/cpu.max") as fh:
+            quota, period = fh.read().split()[:2]
+        if quota != "max":
+            n = min(n, max(1, int(float(quota) / float(period))))
+    except (OSError, ValueError):
+        pass
     try:
         import psutil
         n = min(n, int(psutil.virtual_memory().available // CPU_WORKER_BYTES))
@@ -505,8 +513,12 @@ def ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nw = cpu_workers()
-        vs, inf = cpu_parallel(cfg, args.sample_steps, 1, nw)
-        cpu = {"value": vs[0], "unit": "steps*RHS/s", "cores": nw, "kind": "port", "sample": cpu_sample_text(inf)}
+        try:
+            vs, inf = cpu_parallel(cfg, args.sample_steps, 1, nw)
+            cpu = {"value": vs[0], "unit": "steps*RHS/s", "cores": nw, "kind": "port",
+                   "sample": cpu_sample_text(inf)}
+        except RuntimeError as e:
+            cpu = {"value": None, "unit": "steps*RHS/s", "cores": nw, "kind": "port", "error": str(e)}
     line = {
         "metric": "FETD steps*RHS/s", "value": value, "unit": "steps*RHS/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
