@@ -3,10 +3,14 @@
 #include "symbolic.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
+#include <exception>
 #include <numeric>
 #include <stdexcept>
+#include <thread>
 
 namespace temf {
 
@@ -28,7 +32,15 @@ double now_s() {
 // counts for all k.  The split with the smallest boundary among balanced ones
 // (35-65 %) wins; the smaller-side boundary becomes the separator.  Each
 // subset is ordered: left part, right part, separator (separators are
-// eliminated last, forming the top of the elimination tree).
+// eliminated last, forming the top of the elimination tree).  The ordering
+// is built in place: a subset's range of the vertex array ends as its order.
+//
+// The two halves of a split are ordered by separate threads when both are
+// large.  They share no edge (the separator covers every cut edge), so a
+// thread writes stamp/rank only for its own vertices and reads them only for
+// its own vertices and finished separators; subset ids come from one atomic
+// counter, so they are unique and the result does not depend on the number
+// of threads.
 // ---------------------------------------------------------------------------
 struct NDState {
   int n;
@@ -38,9 +50,12 @@ struct NDState {
   int leaf;
   std::vector<int> stamp;   // subset id a vertex currently belongs to
   std::vector<int> rank;    // rank along the axis being evaluated
-  std::vector<int> order;   // output: new -> old
-  int next_id = 1;
+  std::atomic<int> next_id{1};
+  std::atomic<int> spare_threads{0};
 };
+
+constexpr int kNdParallelMin = 20000;       // smallest half handed to another thread
+constexpr int kNdAxisParallelMin = 200000;  // smallest subset whose three axes run in parallel
 
 struct Split {
   int axis = -1;
@@ -50,13 +65,25 @@ struct Split {
   double cost = 0;
 };
 
-// Evaluate all split positions along `axis`; leaves v sorted along the axis.
-void eval_axis(NDState& S, int* v, int m, int axis, int id, Split& best) {
-  std::sort(v, v + m, [&](int a, int b) {
-    double ka = S.xyz[3 * (int64_t)a + axis], kb = S.xyz[3 * (int64_t)b + axis];
-    return ka < kb || (ka == kb && a < b);
-  });
-  for (int i = 0; i < m; ++i) { S.rank[v[i]] = i; S.stamp[v[i]] = id; }
+// v sorted along `axis`, ties by vertex id (keys gathered once, not per comparison).
+void sort_along(const NDState& S, int* v, int m, int axis) {
+  std::vector<std::pair<double, int>> key(m);
+  for (int i = 0; i < m; ++i) key[i] = {S.xyz[3 * (int64_t)v[i] + axis], v[i]};
+  std::sort(key.begin(), key.end());
+  for (int i = 0; i < m; ++i) v[i] = key[i].second;
+}
+
+int take_threads(NDState& S, int want) {
+  int k = S.spare_threads.load();
+  while (k > 0 && !S.spare_threads.compare_exchange_weak(k, k - std::min(k, want))) {}
+  return std::min(k, want);
+}
+
+// Evaluate all split positions along `axis` for the subset stamped `id`;
+// leaves v sorted along the axis and rank[v[i]] = i.
+void eval_axis(const NDState& S, int* v, int m, int axis, int id, int* rank, Split& best) {
+  sort_along(S, v, m, axis);
+  for (int i = 0; i < m; ++i) rank[v[i]] = i;
   std::vector<int> dl(m + 2, 0), dr(m + 2, 0);
   for (int i = 0; i < m; ++i) {
     const int u = v[i];
@@ -64,7 +91,7 @@ void eval_axis(NDState& S, int* v, int m, int axis, int id, Split& best) {
     for (int64_t p = S.xadj[u]; p < S.xadj[u + 1]; ++p) {
       const int w = S.adj[p];
       if (S.stamp[w] != id) continue;
-      const int rw = S.rank[w];
+      const int rw = rank[w];
       mx = std::max(mx, rw);
       mn = std::min(mn, rw);
     }
@@ -85,32 +112,70 @@ void eval_axis(NDState& S, int* v, int m, int axis, int id, Split& best) {
   }
 }
 
-void nd_rec(NDState& S, int* v, int m) {
-  if (m <= S.leaf) {
-    for (int i = 0; i < m; ++i) S.order.push_back(v[i]);
-    return;
-  }
+// The best split of the three axes; the first axis wins ties.  Large subsets
+// evaluate the axes on copies of v in parallel (private rank arrays).
+Split best_split(NDState& S, int* v, int m) {
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   for (int i = 0; i < m; ++i)
     for (int a = 0; a < 3; ++a) {
       double x = S.xyz[3 * (int64_t)v[i] + a];
       lo[a] = std::min(lo[a], x); hi[a] = std::max(hi[a], x);
     }
-  Split best;
-  for (int axis = 0; axis < 3; ++axis) {
-    if (hi[axis] <= lo[axis]) continue;
-    eval_axis(S, v, m, axis, S.next_id++, best);
-  }
-  if (best.axis < 0) {  // all points coincide: give up splitting
-    for (int i = 0; i < m; ++i) S.order.push_back(v[i]);
-    return;
-  }
-  // re-sort along the chosen axis (v holds the order of the last axis tried)
   const int id = S.next_id++;
-  std::sort(v, v + m, [&](int a, int b) {
-    double ka = S.xyz[3 * (int64_t)a + best.axis], kb = S.xyz[3 * (int64_t)b + best.axis];
-    return ka < kb || (ka == kb && a < b);
-  });
+  for (int i = 0; i < m; ++i) S.stamp[v[i]] = id;
+  Split cand[3];
+  const int extra = m >= kNdAxisParallelMin ? take_threads(S, 2) : 0;
+  if (extra == 0) {
+    for (int a = 0; a < 3; ++a)
+      if (hi[a] > lo[a]) eval_axis(S, v, m, a, id, S.rank.data(), cand[a]);
+  } else {
+    // axis 0 here; axes 1 and 2 on one or two other threads
+    std::vector<int> va(v, v + m), vb(extra == 2 ? m : 0);
+    std::vector<int> ra(S.n), rb(extra == 2 ? S.n : 0);
+    if (extra == 2) std::copy(v, v + m, vb.begin());
+    std::exception_ptr fa, fb;
+    std::thread ta([&] {
+      try {
+        if (hi[1] > lo[1]) eval_axis(S, va.data(), m, 1, id, ra.data(), cand[1]);
+        if (extra == 1 && hi[2] > lo[2]) eval_axis(S, va.data(), m, 2, id, ra.data(), cand[2]);
+      } catch (...) {
+        fa = std::current_exception();
+      }
+    });
+    std::thread tb;
+    if (extra == 2)
+      tb = std::thread([&] {
+        try {
+          if (hi[2] > lo[2]) eval_axis(S, vb.data(), m, 2, id, rb.data(), cand[2]);
+        } catch (...) {
+          fb = std::current_exception();
+        }
+      });
+    std::exception_ptr f0;
+    try {
+      if (hi[0] > lo[0]) eval_axis(S, v, m, 0, id, S.rank.data(), cand[0]);
+    } catch (...) {
+      f0 = std::current_exception();
+    }
+    ta.join();
+    if (tb.joinable()) tb.join();
+    S.spare_threads.fetch_add(extra);
+    for (const std::exception_ptr& e : {f0, fa, fb})
+      if (e) std::rethrow_exception(e);
+  }
+  Split best;
+  for (int a = 0; a < 3; ++a)
+    if (cand[a].sep >= 0 && (best.sep < 0 || cand[a].cost < best.cost)) best = cand[a];
+  return best;
+}
+
+void nd_rec(NDState& S, int* v, int m) {
+  if (m <= S.leaf) return;
+  const Split best = best_split(S, v, m);
+  if (best.axis < 0) return;  // all points coincide: give up splitting
+  // re-sort along the chosen axis (v holds the order of an axis tried)
+  const int id = S.next_id++;
+  sort_along(S, v, m, best.axis);
   for (int i = 0; i < m; ++i) { S.rank[v[i]] = i; S.stamp[v[i]] = id; }
   // Minimum vertex cover of the bipartite graph of cut edges (Koenig): maximum
   // matching between the left boundary BL and the right boundary BR, then the
@@ -219,27 +284,106 @@ void nd_rec(NDState& S, int* v, int m) {
   std::copy(L.begin(), L.end(), v);
   std::copy(R.begin(), R.end(), v + L.size());
   std::copy(Sp.begin(), Sp.end(), v + L.size() + R.size());
-  const int nl = (int)L.size(), nr = (int)R.size(), ns = (int)Sp.size();
+  const int nl = (int)L.size(), nr = (int)R.size();
   { std::vector<int>().swap(L); std::vector<int>().swap(R); std::vector<int>().swap(Sp); }
-  nd_rec(S, v, nl);
-  nd_rec(S, v + nl, nr);
-  for (int i = 0; i < ns; ++i) S.order.push_back(v[nl + nr + i]);
+  const bool fork = std::min(nl, nr) >= kNdParallelMin && take_threads(S, 1) == 1;
+  if (!fork) {
+    nd_rec(S, v, nl);
+    nd_rec(S, v + nl, nr);
+    return;
+  }
+  std::exception_ptr failed;
+  std::thread left([&] {
+    try {
+      nd_rec(S, v, nl);
+    } catch (...) {
+      failed = std::current_exception();
+    }
+  });
+  std::exception_ptr failed_right;
+  try {
+    nd_rec(S, v + nl, nr);
+  } catch (...) {
+    failed_right = std::current_exception();
+  }
+  left.join();
+  S.spare_threads.fetch_add(1);
+  if (failed) std::rethrow_exception(failed);
+  if (failed_right) std::rethrow_exception(failed_right);
+}
+
+// Column counts of L for a postordered elimination tree (children before
+// parents, every subtree a contiguous index range), by the method of
+// Gilbert, Ng & Peyton, "An efficient algorithm to compute row and column
+// counts for sparse Cholesky factorization" (SIAM J. Matrix Anal. Appl.
+// 15(4), 1994).  cc[j] = #{i : L(i,j) != 0} = #{i : j in T_i}, where the row
+// subtree T_i is the union of the tree paths from every k < i with
+// A(i,k) != 0 (and from i itself) up to i.  With weights w and
+// cc[j] = sum of w over the subtree of j, one row subtree contributes
+//   +1 at each of its leaves k_1 < ... < k_m,
+//   -1 at lca(k_{t-1}, k_t) for t >= 2, and -1 at parent(i):
+// every node of T_i then sums to 1 and every other node to 0.  Columns are
+// visited in increasing order; k is a leaf of T_i iff no earlier column of
+// row i lies in k's subtree, i.e. the last one seen is below first(k); the
+// lca of the previous leaf and k is the lowest ancestor of the previous
+// leaf not yet finished (a column is finished, and its set joined to its
+// parent's, once all its entries are visited), found with path compression.
+std::vector<int64_t> column_counts(int n, const int64_t* xadj, const int* adj, const std::vector<int>& perm,
+                                   const std::vector<int>& iperm, const std::vector<int>& parent) {
+  std::vector<int64_t> w(n, 0);
+  std::vector<int> first(n), size(n, 1);
+  for (int j = 0; j < n; ++j)
+    if (parent[j] >= 0) size[parent[j]] += size[j];
+  for (int j = 0; j < n; ++j) first[j] = j - size[j] + 1;
+  std::vector<int> last_seen(n, -1), prev_leaf(n, -1), anc(n);
+  std::iota(anc.begin(), anc.end(), 0);
+  for (int k = 0; k < n; ++k) {
+    if (first[k] == k) w[k] += 1;           // an etree leaf: T_k = {k}
+    if (parent[k] >= 0) w[parent[k]] -= 1;  // the root correction of T_k
+    const int ok = perm[k];
+    for (int64_t p = xadj[ok]; p < xadj[ok + 1]; ++p) {
+      const int i = iperm[adj[p]];
+      if (i <= k) continue;
+      const bool leaf = last_seen[i] < first[k];
+      last_seen[i] = k;
+      if (!leaf) continue;
+      w[k] += 1;
+      const int pl = prev_leaf[i];
+      prev_leaf[i] = k;
+      if (pl < 0) continue;
+      int q = pl;
+      while (anc[q] != q) q = anc[q];
+      for (int x = pl; x != q;) {
+        const int nx = anc[x];
+        anc[x] = q;
+        x = nx;
+      }
+      w[q] -= 1;
+    }
+    if (parent[k] >= 0) anc[k] = parent[k];
+  }
+  for (int j = 0; j < n; ++j)
+    if (parent[j] >= 0) w[parent[j]] += w[j];
+  return w;
 }
 
 }  // namespace
 
 std::vector<int> nested_dissection(int n, const int64_t* xadj, const int* adj,
-                                   const double* xyz, int leaf_size) {
+                                   const double* xyz, int leaf_size, int threads) {
   NDState S;
   S.n = n; S.xadj = xadj; S.adj = adj; S.xyz = xyz; S.leaf = std::max(leaf_size, 4);
   S.stamp.assign(n, 0);
   S.rank.assign(n, 0);
-  S.order.reserve(n);
+  if (threads <= 0) {
+    const char* env = std::getenv("TEMF_HOST_THREADS");
+    threads = env && std::atoi(env) > 0 ? std::atoi(env) : (int)std::max(1u, std::thread::hardware_concurrency());
+  }
+  S.spare_threads = std::max(0, threads - 1);
   std::vector<int> v(n);
   std::iota(v.begin(), v.end(), 0);
   nd_rec(S, v.data(), n);
-  if ((int)S.order.size() != n) throw std::runtime_error("nested dissection lost vertices");
-  return S.order;
+  return v;
 }
 
 void analyse(int n, const int64_t* xadj, const int* adj, const double* xyz,
@@ -247,7 +391,7 @@ void analyse(int n, const int64_t* xadj, const int* adj, const double* xyz,
   out = Symbolic();
   out.n = n;
   double t0 = now_s();
-  std::vector<int> perm = nested_dissection(n, xadj, adj, xyz, opt.leaf_size);
+  std::vector<int> perm = nested_dissection(n, xadj, adj, xyz, opt.leaf_size, opt.threads);
   std::vector<int> iperm(n);
   for (int i = 0; i < n; ++i) iperm[perm[i]] = i;
   double t1 = now_s();
@@ -302,25 +446,8 @@ void analyse(int n, const int64_t* xadj, const int* adj, const double* xyz,
   double t2 = now_s();
   out.t_etree = t2 - t1;
 
-  // --- column counts by row subtrees (O(nnz(L))) ---
-  std::vector<int64_t> cc(n, 0);
-  {
-    std::vector<int> mark(n, -1);
-    for (int i = 0; i < n; ++i) {
-      mark[i] = i;
-      cc[i] += 1;
-      int oi = perm[i];
-      for (int64_t p = xadj[oi]; p < xadj[oi + 1]; ++p) {
-        int k = iperm[adj[p]];
-        if (k >= i) continue;
-        while (mark[k] != i) {
-          mark[k] = i;
-          cc[k] += 1;
-          k = parent[k];
-        }
-      }
-    }
-  }
+  // --- column counts (Gilbert, Ng & Peyton 1994, near-linear in nnz(A)) ---
+  std::vector<int64_t> cc = column_counts(n, xadj, adj, perm, iperm, parent);
   double t3 = now_s();
   out.t_colcount = t3 - t2;
   out.nnzL_exact = 0;

@@ -19,6 +19,8 @@ struct SymbolicOptions {
   int max_sn_cols = 64;        // supernodes are split into column blocks of at most this width
   bool amalgamate = true;      // relaxed supernode amalgamation
   int amalg_level = 2;         // 1: merge while the zero fraction stays small; 2: merge small supernodes harder
+  int threads = 0;             // host threads for the ordering (0: $TEMF_HOST_THREADS, else all cores);
+                               // the result does not depend on it
 };
 
 struct Symbolic {
@@ -47,9 +49,11 @@ struct Symbolic {
 
 // Nested-dissection ordering on the symmetric graph (xadj/adj without the
 // diagonal) using recursive coordinate bisection with vertex separators.
-// Returns perm[new] = old.
+// Returns perm[new] = old.  Independent halves are ordered by up to
+// `threads` host threads (0: $TEMF_HOST_THREADS, else all cores); the
+// ordering is the same for any count.
 std::vector<int> nested_dissection(int n, const int64_t* xadj, const int* adj,
-                                   const double* xyz, int leaf_size);
+                                   const double* xyz, int leaf_size, int threads = 0);
 
 // Full symbolic analysis.  (xadj, adj) is the symmetric pattern of A in the
 // original numbering without the diagonal; xyz gives a point per unknown

@@ -215,3 +215,17 @@ def test_solve_schedules_replay(kind):
     rc = _lib.lib().temf_schedule_check(n, xadj.ctypes.data_as(C.POINTER(C.c_longlong)), _lib.iptr(adj),
                                         _lib.dptr(xyz), msg, 256)
     assert rc == 0, msg.value.decode()
+
+
+def test_ordering_does_not_depend_on_host_threads(monkeypatch):
+    """The nested-dissection halves and the three axis evaluations of large
+    subsets run on separate host threads; the permutation and the symbolic
+    statistics are the same for one thread and for several."""
+    n, xadj, adj, xyz = _grid_pattern(64, 60, 56)   # 215k unknowns: both threading thresholds reached
+    out = {}
+    for t in ("1", "3", "8"):
+        monkeypatch.setenv("TEMF_HOST_THREADS", t)
+        out[t] = _symbolic(n, xadj, adj, xyz)
+    for t in ("3", "8"):
+        assert np.array_equal(out[t][0], out["1"][0])
+        assert np.array_equal(out[t][1][[0, 1, 2, 3, 4, 5, 8]], out["1"][1][[0, 1, 2, 3, 4, 5, 8]])
