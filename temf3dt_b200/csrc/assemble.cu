@@ -14,7 +14,10 @@
 // entries listed for that nonzero in a fixed order -- the COO duplicate sum
 // without atomics, so the assembled matrices are bitwise reproducible.
 #include <algorithm>
+#include <climits>
+#include <exception>
 #include <numeric>
+#include <thread>
 
 #include "assemble.h"
 #include "element.cuh"
@@ -188,56 +191,107 @@ void build_adjacency(const temf_ctx& c, std::vector<int64_t>& xadj, std::vector<
   }
 }
 
+// Rows of the permuted pattern are independent: each host thread builds a
+// contiguous row range into its own arrays, which are then concatenated, so
+// the result is the same for any thread count.
 void build_pattern(const temf_ctx& c, const std::vector<int>& perm, const std::vector<int>& iperm,
                    Pattern& P) {
   const int n = c.n_edges, T = c.n_tets;
   std::vector<int64_t> iptr;
   std::vector<int> inc;
   edge_incidence(c, iptr, inc);
+  struct Part {
+    std::vector<int> rowlen, col, cnt, idx;  // per row: entries; per entry: contributions
+    std::exception_ptr failed;
+  };
+  auto rows = [&](int r0, int r1, Part& out) {
+    std::vector<int> slot(n, -1);  // new column -> local entry index within the current row
+    std::vector<int> cols;
+    std::vector<std::vector<int>> contr;
+    std::vector<int> order;
+    for (int r = r0; r < r1; ++r) {
+      const int e = perm[r];
+      cols.clear();
+      for (auto& v : contr) v.clear();
+      int m = 0;
+      for (int64_t q = iptr[e]; q < iptr[e + 1]; ++q) {
+        const int t = inc[q] / 6, a = inc[q] % 6;
+        for (int b = 0; b < 6; ++b) {
+          const int cn = iperm[c.tet_edg[6LL * t + b]];
+          int k = slot[cn];
+          if (k < 0) {
+            k = m++;
+            slot[cn] = k;
+            cols.push_back(cn);
+            if ((int)contr.size() < m) contr.emplace_back();
+          }
+          const int i = std::min(a, b), j = std::max(a, b);
+          contr[k].push_back(packed_upper(i, j) * T + t);
+        }
+      }
+      order.resize(m);
+      std::iota(order.begin(), order.end(), 0);
+      std::sort(order.begin(), order.end(), [&](int x, int y) { return cols[x] < cols[y]; });
+      for (int k : order) {
+        out.col.push_back(cols[k]);
+        out.cnt.push_back((int)contr[k].size());
+        out.idx.insert(out.idx.end(), contr[k].begin(), contr[k].end());
+      }
+      for (int k = 0; k < m; ++k) slot[cols[k]] = -1;
+      out.rowlen.push_back(m);
+    }
+  };
+  const int nt = std::max(1, std::min(host_threads(0), n / 50000));
+  std::vector<Part> parts(nt);
+  {
+    std::vector<std::thread> pool;
+    for (int k = 1; k < nt; ++k)
+      pool.emplace_back([&, k] {
+        try {
+          rows((int)((int64_t)n * k / nt), (int)((int64_t)n * (k + 1) / nt), parts[k]);
+        } catch (...) {
+          parts[k].failed = std::current_exception();
+        }
+      });
+    try {
+      rows(0, (int)((int64_t)n / nt), parts[0]);
+    } catch (...) {
+      parts[0].failed = std::current_exception();
+    }
+    for (std::thread& t : pool) t.join();
+    for (const Part& q : parts)
+      if (q.failed) std::rethrow_exception(q.failed);
+  }
+  int64_t nnz = 0, ncontr = 0;
+  for (const Part& q : parts) {
+    nnz += (int64_t)q.col.size();
+    ncontr += (int64_t)q.idx.size();
+  }
+  if (nnz > (int64_t)INT32_MAX - 64 || ncontr > (int64_t)INT32_MAX - 64)
+    throw ArgError("matrix too large for int32 CSR");
   P.n = n;
+  P.nnz = nnz;
   P.rowptr.assign(n + 1, 0);
   P.col.clear();
-  P.contrib_ptr.clear();
+  P.col.reserve(nnz);
+  P.contrib_ptr.assign(1, 0);
+  P.contrib_ptr.reserve(nnz + 1);
   P.contrib_idx.clear();
-  P.contrib_ptr.push_back(0);
-  std::vector<int> slot(n, -1);  // new column -> local entry index within the current row
-  struct Ent { int col; std::vector<int> c; };
-  std::vector<int> cols;
-  std::vector<std::vector<int>> contr;
-  std::vector<int> order;
-  for (int r = 0; r < n; ++r) {
-    const int e = perm[r];
-    cols.clear();
-    for (auto& v : contr) v.clear();
-    int m = 0;
-    for (int64_t q = iptr[e]; q < iptr[e + 1]; ++q) {
-      const int t = inc[q] / 6, a = inc[q] % 6;
-      for (int b = 0; b < 6; ++b) {
-        const int cn = iperm[c.tet_edg[6LL * t + b]];
-        int k = slot[cn];
-        if (k < 0) {
-          k = m++;
-          slot[cn] = k;
-          cols.push_back(cn);
-          if ((int)contr.size() < m) contr.emplace_back();
-        }
-        const int i = std::min(a, b), j = std::max(a, b);
-        contr[k].push_back(packed_upper(i, j) * T + t);
-      }
+  P.contrib_idx.reserve(ncontr);
+  int r = 0;
+  for (Part& q : parts) {
+    for (int len : q.rowlen) {
+      P.rowptr[r + 1] = P.rowptr[r] + len;
+      ++r;
     }
-    order.resize(m);
-    std::iota(order.begin(), order.end(), 0);
-    std::sort(order.begin(), order.end(), [&](int x, int y) { return cols[x] < cols[y]; });
-    for (int k : order) {
-      P.col.push_back(cols[k]);
-      for (int v : contr[k]) P.contrib_idx.push_back(v);
-      P.contrib_ptr.push_back((int)P.contrib_idx.size());
-    }
-    for (int k = 0; k < m; ++k) slot[cols[k]] = -1;
-    P.rowptr[r + 1] = (int)P.col.size();
-    if ((int64_t)P.col.size() > (int64_t)INT32_MAX - 64) throw ArgError("matrix too large for int32 CSR");
+    P.col.insert(P.col.end(), q.col.begin(), q.col.end());
+    for (int k : q.cnt) P.contrib_ptr.push_back(P.contrib_ptr.back() + k);
+    P.contrib_idx.insert(P.contrib_idx.end(), q.idx.begin(), q.idx.end());
+    std::vector<int>().swap(q.rowlen);
+    std::vector<int>().swap(q.col);
+    std::vector<int>().swap(q.cnt);
+    std::vector<int>().swap(q.idx);
   }
-  P.nnz = (int64_t)P.col.size();
 }
 
 void upload_mesh(temf_ctx& c) {

@@ -252,6 +252,73 @@ void need(bool cond, const char* msg) {
 
 }  // namespace
 
+namespace {
+
+// Edge keys of every (tet, local edge) of a 1-based tet_vex(n_tets, 4)
+// (column-major): key = min vertex << bits | max vertex, local edges joining
+// the vertex pairs ind_tet (src/FETD_FWD.f90:23), sorted ascending: a
+// counting sort by the smaller vertex, then an insertion sort by the larger
+// one inside each (short) bucket.  Both are stable, so equal keys stay in
+// (tet, local edge) order.  slot[p] = 6 * tet + local edge of the p-th key.
+struct EdgeKeys {
+  std::vector<uint64_t> key;
+  std::vector<int64_t> slot;
+  int bits = 0;
+};
+
+bool edge_keys(int n_tets, const int* tet_vex, EdgeKeys& K) {
+  static const int it[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {3, 1}, {2, 3}};
+  const int64_t m = 6LL * n_tets;
+  int64_t vmax = 0;
+  for (int64_t q = 0; q < 4LL * n_tets; ++q) {
+    if (tet_vex[q] < 0) return false;
+    vmax = std::max<int64_t>(vmax, tet_vex[q]);
+  }
+  int bits = 1;
+  while ((1LL << bits) <= vmax) ++bits;
+  K.bits = bits;
+  auto lo_hi = [&](int64_t q, uint64_t& a, uint64_t& b) {
+    const int64_t t = q / 6, j = q % 6;
+    a = (uint64_t)tet_vex[it[j][0] * (int64_t)n_tets + t];
+    b = (uint64_t)tet_vex[it[j][1] * (int64_t)n_tets + t];
+    if (a > b) std::swap(a, b);
+  };
+  std::vector<int64_t> start(vmax + 2, 0);
+  for (int64_t q = 0; q < m; ++q) {
+    uint64_t a, b;
+    lo_hi(q, a, b);
+    ++start[a + 1];
+  }
+  for (int64_t v = 0; v <= vmax; ++v) start[v + 1] += start[v];
+  K.key.resize(m);
+  K.slot.resize(m);
+  {
+    std::vector<int64_t> fill(start.begin(), start.end() - 1);
+    for (int64_t q = 0; q < m; ++q) {
+      uint64_t a, b;
+      lo_hi(q, a, b);
+      const int64_t d = fill[a]++;
+      K.key[d] = (a << bits) | b;
+      K.slot[d] = q;
+    }
+  }
+  for (int64_t v = 0; v <= vmax; ++v)
+    for (int64_t p = start[v] + 1; p < start[v + 1]; ++p) {
+      const uint64_t k = K.key[p];
+      const int64_t sl = K.slot[p];
+      int64_t r = p;
+      for (; r > start[v] && K.key[r - 1] > k; --r) {
+        K.key[r] = K.key[r - 1];
+        K.slot[r] = K.slot[r - 1];
+      }
+      K.key[r] = k;
+      K.slot[r] = sl;
+    }
+  return true;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* temf_version(void) { return "temf_b200 0.1 (sm_100a, FP64)"; }
@@ -292,48 +359,50 @@ const char* temf_last_error(const temf_ctx* c) { return c ? c->err.c_str() : "nu
 
 int temf_mesh_count_edges(int n_tets, const int* tet_vex, int* n_edges) {
   if (n_tets <= 0 || !tet_vex || !n_edges) return TEMF_EARG;
-  std::vector<int64_t> keys;
-  keys.reserve(6LL * n_tets);
-  static const int it[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {3, 1}, {2, 3}};
-  for (int t = 0; t < n_tets; ++t)
-    for (int j = 0; j < 6; ++j) {
-      int64_t a = tet_vex[(int64_t)it[j][0] * n_tets + t], b = tet_vex[(int64_t)it[j][1] * n_tets + t];
-      if (a > b) std::swap(a, b);
-      keys.push_back((a << 32) | b);
-    }
-  std::sort(keys.begin(), keys.end());
-  *n_edges = (int)(std::unique(keys.begin(), keys.end()) - keys.begin());
-  return TEMF_OK;
+  try {
+    EdgeKeys K;
+    if (!edge_keys(n_tets, tet_vex, K)) return TEMF_EARG;
+    int64_t count = 0;
+    for (size_t p = 0; p < K.key.size(); ++p)
+      if (p == 0 || K.key[p] != K.key[p - 1]) ++count;
+    if (count > INT32_MAX) return TEMF_EARG;
+    *n_edges = (int)count;
+    return TEMF_OK;
+  } catch (...) {
+    return TEMF_EINTERNAL;
+  }
 }
 
 int temf_mesh_topology(int n_tets, const int* tet_vex, int n_edges, int* edg_vex, int* tet_edg, int* tet_drc) {
   if (n_tets <= 0 || !tet_vex || !edg_vex || !tet_edg || !tet_drc) return TEMF_EARG;
-  std::vector<int64_t> keys;
-  keys.reserve(6LL * n_tets);
-  static const int it[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {3, 1}, {2, 3}};
-  for (int t = 0; t < n_tets; ++t)
-    for (int j = 0; j < 6; ++j) {
-      int64_t a = tet_vex[(int64_t)it[j][0] * n_tets + t], b = tet_vex[(int64_t)it[j][1] * n_tets + t];
-      if (a > b) std::swap(a, b);
-      keys.push_back((a << 32) | b);
+  try {
+    EdgeKeys K;
+    if (!edge_keys(n_tets, tet_vex, K)) return TEMF_EARG;
+    int64_t count = 0;
+    for (size_t p = 0; p < K.key.size(); ++p)
+      if (p == 0 || K.key[p] != K.key[p - 1]) ++count;
+    if (count != n_edges) return TEMF_EARG;
+    // edges in ascending (min, max) order; every (tet, local edge) gets its edge's 1-based index
+    int64_t e = -1;
+    for (size_t p = 0; p < K.key.size(); ++p) {
+      if (p == 0 || K.key[p] != K.key[p - 1]) {
+        ++e;
+        edg_vex[e] = (int)(K.key[p] >> K.bits);
+        edg_vex[(int64_t)n_edges + e] = (int)(K.key[p] & ((1ULL << K.bits) - 1));
+      }
+      const int64_t q = K.slot[p], t = q / 6, j = q % 6;
+      tet_edg[j * n_tets + t] = (int)e + 1;
     }
-  std::vector<int64_t> u(keys);
-  std::sort(u.begin(), u.end());
-  u.erase(std::unique(u.begin(), u.end()), u.end());
-  if ((int)u.size() != n_edges) return TEMF_EARG;
-  for (int e = 0; e < n_edges; ++e) {
-    edg_vex[e] = (int)(u[e] >> 32);
-    edg_vex[(int64_t)n_edges + e] = (int)(u[e] & 0xffffffffLL);
+    static const int it[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {3, 1}, {2, 3}};
+    for (int t = 0; t < n_tets; ++t)
+      for (int j = 0; j < 6; ++j) {
+        const int a = tet_vex[(int64_t)it[j][0] * n_tets + t], b = tet_vex[(int64_t)it[j][1] * n_tets + t];
+        tet_drc[(int64_t)j * n_tets + t] = a < b ? 1 : -1;
+      }
+    return TEMF_OK;
+  } catch (...) {
+    return TEMF_EINTERNAL;
   }
-  for (int t = 0; t < n_tets; ++t)
-    for (int j = 0; j < 6; ++j) {
-      const int64_t key = keys[6LL * t + j];
-      const int64_t pos = std::lower_bound(u.begin(), u.end(), key) - u.begin();
-      tet_edg[(int64_t)j * n_tets + t] = (int)pos + 1;
-      const int a = tet_vex[(int64_t)it[j][0] * n_tets + t], b = tet_vex[(int64_t)it[j][1] * n_tets + t];
-      tet_drc[(int64_t)j * n_tets + t] = a < b ? 1 : -1;
-    }
-  return TEMF_OK;
 }
 
 int temf_set_mesh(temf_ctx* c, int n_nodes, const double* nod_cor, int n_tets, const int* tet_vex, int n_edges,

@@ -276,46 +276,17 @@ void build_factor_plan(temf_ctx& c) {
     F.a2l_src.upload(src.data(), src.size(), st);
     F.a2l_dst.upload(dst.data(), dst.size(), st);
   }
-  // update groups + relative indices
+  // update groups + relative indices (host threads; see symbolic.h)
   {
-    std::vector<int> row_grp(S.sn_rows.size());
-    std::vector<int> gt, gj;
-    std::vector<int64_t> gr;
-    std::vector<int> rel;
-    for (int s = 0; s < nsn; ++s) {
-      const int64_t rp = S.sn_rows_ptr[s];
-      const int r = (int)nrows(s);
-      int j = 0;
-      while (j < r) {
-        const int t = S.col2sn[S.sn_rows[rp + j]];
-        int j2 = j;
-        while (j2 < r && S.col2sn[S.sn_rows[rp + j2]] == t) ++j2;
-        const int grp = (int)gt.size();
-        gt.push_back(t);
-        gj.push_back(j);
-        gr.push_back((int64_t)rel.size());
-        for (int jj = j; jj < j2; ++jj) row_grp[rp + jj] = grp;
-        // relative positions of rows j..r-1 inside t's panel (merge of sorted lists)
-        const int ft = S.sn_first[t], ct = width(t);
-        const int* tb = S.sn_rows.data() + S.sn_rows_ptr[t];
-        const int64_t tr = nrows(t);
-        int64_t k = 0;
-        for (int i = j; i < r; ++i) {
-          const int gi = S.sn_rows[rp + i];
-          if (gi < ft + ct) { rel.push_back(gi - ft); continue; }
-          while (k < tr && tb[k] < gi) ++k;
-          if (k >= tr || tb[k] != gi) throw StateError("symbolic structure inconsistent (update row)");
-          rel.push_back((int)(ct + k));
-        }
-        j = j2;
-      }
-    }
-    F.n_relind = (int64_t)rel.size();
-    F.row_grp.upload(row_grp.data(), row_grp.size(), st);
-    F.grp_target.upload(gt.data(), gt.size(), st);
-    F.grp_jfirst.upload(gj.data(), gj.size(), st);
-    F.grp_relind.upload(gr.data(), gr.size(), st);
-    F.relind.upload(rel.data(), rel.size(), st);
+    UpdateGroups G;
+    update_groups(S, G);
+    F.n_relind = G.n_rel;
+    F.row_grp.upload(G.row_grp.data(), G.row_grp.size(), st);
+    F.grp_target.upload(G.grp_target.data(), G.grp_target.size(), st);
+    F.grp_jfirst.upload(G.grp_jfirst.data(), G.grp_jfirst.size(), st);
+    F.grp_relind.upload(G.grp_rel.data(), G.grp_rel.size(), st);
+    F.relind.upload(G.rel.get(), (size_t)G.n_rel, st);
+    TEMF_CUDA(cudaStreamSynchronize(st));  // G's host arrays go out of scope
   }
   // row chunks of the triangular solves per level
   {

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <exception>
@@ -369,16 +370,111 @@ std::vector<int64_t> column_counts(int n, const int64_t* xadj, const int* adj, c
 
 }  // namespace
 
+int host_threads(int requested) {
+  if (requested > 0) return requested;
+  const char* env = std::getenv("TEMF_HOST_THREADS");
+  if (env && std::atoi(env) > 0) return std::atoi(env);
+  return (int)std::max(1u, std::thread::hardware_concurrency());
+}
+
+void update_groups(const Symbolic& S, UpdateGroups& G, int threads) {
+  const int nsn = S.nsn;
+  // pass 1: groups and relative positions per supernode
+  std::vector<int64_t> goff(nsn + 1, 0), roff(nsn + 1, 0);
+  for (int s = 0; s < nsn; ++s) {
+    const int64_t rp = S.sn_rows_ptr[s], r = S.sn_rows_ptr[s + 1] - rp;
+    int64_t ng = 0, nr = 0;
+    for (int64_t j = 0; j < r;) {
+      const int t = S.col2sn[S.sn_rows[rp + j]];
+      int64_t j2 = j;
+      while (j2 < r && S.col2sn[S.sn_rows[rp + j2]] == t) ++j2;
+      ++ng;
+      nr += r - j;
+      j = j2;
+    }
+    goff[s + 1] = goff[s] + ng;
+    roff[s + 1] = roff[s] + nr;
+  }
+  const int64_t ngrp = goff[nsn];
+  if (ngrp > INT32_MAX) throw std::runtime_error("too many update groups for int32 indices");
+  G.row_grp.assign(S.sn_rows.size(), 0);
+  G.grp_target.assign(ngrp, 0);
+  G.grp_jfirst.assign(ngrp, 0);
+  G.grp_rel.assign(ngrp, 0);
+  G.n_rel = roff[nsn];
+  G.rel.reset(new int[std::max<int64_t>(G.n_rel, 1)]);
+  // pass 2: fill, supernode ranges of about equal work per thread
+  auto fill = [&](int s0, int s1) {
+    for (int s = s0; s < s1; ++s) {
+      const int64_t rp = S.sn_rows_ptr[s], r = S.sn_rows_ptr[s + 1] - rp;
+      int64_t g = goff[s], q = roff[s];
+      for (int64_t j = 0; j < r;) {
+        const int t = S.col2sn[S.sn_rows[rp + j]];
+        int64_t j2 = j;
+        while (j2 < r && S.col2sn[S.sn_rows[rp + j2]] == t) ++j2;
+        G.grp_target[g] = t;
+        G.grp_jfirst[g] = (int)j;
+        G.grp_rel[g] = q;
+        for (int64_t jj = j; jj < j2; ++jj) G.row_grp[rp + jj] = (int)g;
+        // relative positions of rows j..r-1 inside t's panel (merge of sorted lists)
+        const int ft = S.sn_first[t], ct = S.sn_first[t + 1] - ft;
+        const int* tb = S.sn_rows.data() + S.sn_rows_ptr[t];
+        const int64_t tr = S.sn_rows_ptr[t + 1] - S.sn_rows_ptr[t];
+        int64_t k = 0;
+        for (int64_t i = j; i < r; ++i) {
+          const int gi = S.sn_rows[rp + i];
+          if (gi < ft + ct) {
+            G.rel[q++] = gi - ft;
+            continue;
+          }
+          while (k < tr && tb[k] < gi) ++k;
+          if (k >= tr || tb[k] != gi) throw std::runtime_error("symbolic structure inconsistent (update row)");
+          G.rel[q++] = (int)(ct + k);
+        }
+        ++g;
+        j = j2;
+      }
+    }
+  };
+  const int nt = (int)std::min<int64_t>(host_threads(threads), std::max<int64_t>(1, G.n_rel / 4000000));
+  if (nt <= 1) {
+    fill(0, nsn);
+    return;
+  }
+  std::vector<int> cut(nt + 1, nsn);
+  cut[0] = 0;
+  for (int k = 1, s = 0; k < nt; ++k) {
+    const int64_t target = G.n_rel * k / nt;
+    while (s < nsn && roff[s] < target) ++s;
+    cut[k] = s;
+  }
+  std::vector<std::exception_ptr> failed(nt);
+  std::vector<std::thread> pool;
+  for (int k = 1; k < nt; ++k)
+    pool.emplace_back([&, k] {
+      try {
+        fill(cut[k], cut[k + 1]);
+      } catch (...) {
+        failed[k] = std::current_exception();
+      }
+    });
+  try {
+    fill(cut[0], cut[1]);
+  } catch (...) {
+    failed[0] = std::current_exception();
+  }
+  for (std::thread& t : pool) t.join();
+  for (const std::exception_ptr& e : failed)
+    if (e) std::rethrow_exception(e);
+}
+
 std::vector<int> nested_dissection(int n, const int64_t* xadj, const int* adj,
                                    const double* xyz, int leaf_size, int threads) {
   NDState S;
   S.n = n; S.xadj = xadj; S.adj = adj; S.xyz = xyz; S.leaf = std::max(leaf_size, 4);
   S.stamp.assign(n, 0);
   S.rank.assign(n, 0);
-  if (threads <= 0) {
-    const char* env = std::getenv("TEMF_HOST_THREADS");
-    threads = env && std::atoi(env) > 0 ? std::atoi(env) : (int)std::max(1u, std::thread::hardware_concurrency());
-  }
+  threads = host_threads(threads);
   S.spare_threads = std::max(0, threads - 1);
   std::vector<int> v(n);
   std::iota(v.begin(), v.end(), 0);

@@ -9,6 +9,7 @@
 // default (iparm = 0, :909-910).
 #pragma once
 #include <cstdint>
+#include <memory>
 #include <vector>
 #include <string>
 
@@ -54,6 +55,29 @@ struct Symbolic {
 // ordering is the same for any count.
 std::vector<int> nested_dissection(int n, const int64_t* xadj, const int* adj,
                                    const double* xyz, int leaf_size, int threads = 0);
+
+// Update groups of the numeric factorisation.  The below-diagonal rows of a
+// supernode s fall into runs owned by one ancestor t each (a group); the
+// update of s scatters its rows j.. (j = the group's first row) into t's
+// panel at relative positions rel[grp_rel[g] + (i - j)]: the column offset
+// for rows inside t's columns, c_t + (position in t's row list) for rows
+// below them.
+struct UpdateGroups {
+  std::vector<int> row_grp;      // per entry of Symbolic::sn_rows: its group
+  std::vector<int> grp_target;   // per group: t
+  std::vector<int> grp_jfirst;   // per group: j
+  std::vector<int64_t> grp_rel;  // per group: offset into rel
+  std::unique_ptr<int[]> rel;    // relative positions (uninitialised storage, all written)
+  int64_t n_rel = 0;
+};
+
+// Builds the update groups with up to `threads` host threads (0:
+// $TEMF_HOST_THREADS, else all cores); the result does not depend on the
+// count.  Throws if a row of s is missing from its ancestor's structure.
+void update_groups(const Symbolic& S, UpdateGroups& G, int threads = 0);
+
+// Host threads to use for a request (0: $TEMF_HOST_THREADS, else all cores).
+int host_threads(int requested);
 
 // Full symbolic analysis.  (xadj, adj) is the symmetric pattern of A in the
 // original numbering without the diagonal; xyz gives a point per unknown
