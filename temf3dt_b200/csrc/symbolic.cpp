@@ -2,6 +2,8 @@
 // See symbolic.h for what this replaces in the reference.
 #include "symbolic.h"
 
+#include <sched.h>
+
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -374,7 +376,10 @@ int host_threads(int requested) {
   if (requested > 0) return requested;
   const char* env = std::getenv("TEMF_HOST_THREADS");
   if (env && std::atoi(env) > 0) return std::atoi(env);
-  return (int)std::max(1u, std::thread::hardware_concurrency());
+  int n = (int)std::max(1u, std::thread::hardware_concurrency());
+  cpu_set_t set;
+  if (sched_getaffinity(0, sizeof(set), &set) == 0) n = std::max(1, CPU_COUNT(&set));
+  return std::min(n, 64);
 }
 
 void update_groups(const Symbolic& S, UpdateGroups& G, int threads) {

@@ -76,7 +76,8 @@ struct UpdateGroups {
 // count.  Throws if a row of s is missing from its ancestor's structure.
 void update_groups(const Symbolic& S, UpdateGroups& G, int threads = 0);
 
-// Host threads to use for a request (0: $TEMF_HOST_THREADS, else all cores).
+// Host threads to use for a request (0: $TEMF_HOST_THREADS, else the cores
+// this process may run on, at most 64).
 int host_threads(int requested);
 
 // Full symbolic analysis.  (xadj, adj) is the symmetric pattern of A in the
