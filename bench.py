@@ -23,10 +23,12 @@ host->device, the matrices re-assembled, the loop run and the receiver
 traces copied back.
 
 --impl reference: the reference's CPU path is Intel Fortran + MKL PARDISO,
-which cannot be built or run here; its CPU restatement (oracle/, SuperLU
-factorisation) is timed instead on a bounded sample of the same model family
-(reduced resolution, a fixed number of leading time steps), one
-single-threaded sample per host core, all started together.
+which cannot be built or run here; its CPU restatement is timed instead: the
+oracle's adaptive BDF2 loop on a multithreaded supernodal Cholesky
+(oracle/supernodal_cpu.cpp, the same ordering as the GPU path, OpenMP +
+OpenBLAS on all host cores), on the full-resolution model, each bench step
+one run from rest over a doubling period (sp_double time steps) including
+its factorisation.
 """
 from __future__ import annotations
 
@@ -49,10 +51,6 @@ CONFIGS = {
     2: dict(kind="multiloop", kw=dict(), label="block3d-64-loops-64rhs"),
 }
 COMMON = dict(t0=1e-6, sp_division=10, sp_double=100, time_maximum=1e-2)
-# the CPU restatement factors and solves with SuperLU, which runs on one
-# thread; the host's cores are used by one independent sample per core
-# (steps*RHS/s is a throughput: a CPU job runs its sources side by side)
-CPU_WORKER_BYTES = 1.5e9   # peak RSS of one reduced-model sample is ~0.8 GB
 
 
 def model_for(cfg: int, reduced: bool = False):
@@ -127,16 +125,10 @@ def measured_dgemm_tflops(torch) -> float:
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_sample_text(info) -> str:
-    return ("CPU restatement (oracle/, SuperLU) on the %d-edge reduced-resolution model, first %d time steps, "
-            "%d single-threaded samples side by side (one per core, %.1f s each); MKL PARDISO reference not "
-            "buildable here" % (info["n_edges"], info["steps"], info["workers"], info["sample_seconds"]))
-
-
-def cpu_workers() -> int:
+def host_cores() -> int:
     """Host threads the CPU arm may use: the cores this process may run on,
-    bounded by the container's CPU quota and by the free memory at
-    CPU_WORKER_BYTES per sample."""
+    bounded by the container's CPU quota, at most 64 (the OpenBLAS build's
+    limit)."""
     try:
         n = len(os.sched_getaffinity(0))
     except AttributeError:
@@ -148,93 +140,52 @@ def cpu_workers() -> int:
             n = min(n, max(1, int(float(quota) / float(period))))
     except (OSError, ValueError):
         pass
+    return max(1, min(n, 64))
+
+
+def cpu_arm(cfg: int, steps: int, warmup: int, sample_steps: int = 0):
+    """The reference's CPU path restated (oracle/): the adaptive BDF2 loop of
+    fetd_oracle on the CPU supernodal Cholesky (oracle/supernodal_cpu.cpp,
+    OpenMP + OpenBLAS, all host cores), on the full-resolution model of the
+    config.  One bench step = one run of the loop from rest over its first
+    `sample_steps` time steps (default: one doubling period, sp_double),
+    including its factorisation.  Warm-up steps run one time step each.
+    Falls back to the reduced-resolution model when two factor slots do not
+    fit in free host memory."""
+    from oracle import fetd_oracle as O
+    from oracle import supernodal_cpu as SN
+    from tests.golden_cases import synth_oracle_model
+    threads = host_cores()
+    SN.build()
+    reduced = False
+    om = synth_oracle_model(model_for(cfg))
+    slots = SN.SupernodalSlots(om, threads=threads)
     try:
         import psutil
-        n = min(n, int(psutil.virtual_memory().available // CPU_WORKER_BYTES))
+        if 2 * 8 * slots.stats[2] + 4e9 > psutil.virtual_memory().available:
+            del slots
+            reduced = True
+            om = synth_oracle_model(model_for(cfg, reduced=True))
+            slots = SN.SupernodalSlots(om, threads=threads)
     except ImportError:
         pass
-    return max(1, n)
-
-
-def _cpu_worker(cfg: int, max_steps: int, starts, out):
-    """One single-threaded sample process: build the reduced model once, then
-    run the oracle's leading time steps once per round, released together."""
-    try:
-        from oracle import fetd_oracle as O
-        from tests.golden_cases import synth_oracle_model
-        om = synth_oracle_model(model_for(cfg, reduced=True))
-        out.put(("ready",))
-        for ev in starts:
-            ev.wait()
-            t = time.perf_counter()
-            res = O.run_fetd(om, max_steps=max_steps)
-            out.put(("done", len(res.steps) - 1, time.perf_counter() - t, om.n))
-    except Exception as e:  # noqa: BLE001 - reported to the parent
-        out.put(("error", repr(e)))
-
-
-def _collect(q, procs, count: int, kind: str, limit_s: float):
-    """`count` messages of `kind` from the workers; a worker that failed or
-    exited, or the time limit, ends the wait with an error."""
-    import queue
-    got, t_end = [], time.monotonic() + limit_s
-    while len(got) < count:
-        try:
-            msg = q.get(timeout=2.0)
-        except queue.Empty:
-            dead = [p.exitcode for p in procs if p.exitcode not in (None, 0)]
-            if dead:
-                raise RuntimeError("CPU sample worker exited with code %s" % dead[0])
-            if time.monotonic() > t_end:
-                raise RuntimeError("CPU sample workers did not finish within %.0f s" % limit_s)
-            continue
-        if msg[0] == "error":
-            raise RuntimeError("CPU sample worker failed: %s" % msg[1])
-        if msg[0] == kind:
-            got.append(msg)
-    return got
-
-
-def cpu_parallel(cfg: int, max_steps: int, rounds: int, workers: int):
-    """The oracle on `workers` cores at once (spawned processes, one BLAS
-    thread each).  Per round: steps of all samples / wall time from the
-    common start to the last sample's end."""
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    keys = ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")
-    saved = {k: os.environ.get(k) for k in keys}
-    for k in keys:
-        os.environ[k] = "1"
-    starts = [ctx.Event() for _ in range(rounds)]
-    q = ctx.Queue()
-    procs = [ctx.Process(target=_cpu_worker, args=(cfg, max_steps, starts, q), daemon=True) for _ in range(workers)]
-    try:
-        for p in procs:
-            p.start()
-    finally:
-        for k, v in saved.items():
-            if v is None:
-                os.environ.pop(k, None)
-            else:
-                os.environ[k] = v
-    vals, info = [], None
-    try:
-        _collect(q, procs, workers, "ready", 1800)
-        for ev in starts:
-            t = time.perf_counter()
-            ev.set()
-            got = _collect(q, procs, workers, "done", 3600)
-            wall = time.perf_counter() - t
-            vals.append(sum(g[1] for g in got) / wall)
-            info = dict(n_edges=got[0][3], steps=got[0][1], seconds=wall, workers=workers,
-                        sample_seconds=float(np.mean([g[2] for g in got])))
-    finally:
-        for p in procs:
-            p.join(timeout=5 if vals and len(vals) == rounds else 0.1)
-            if p.is_alive():
-                p.terminate()
-                p.join(timeout=10)
-    return vals, info
+    S = sample_steps or int(om.ctl.step_dble)
+    for _ in range(warmup):
+        O.run_fetd(om, max_steps=1, slots=slots)
+    vals, secs = [], []
+    for _ in range(steps):
+        t = time.perf_counter()
+        res = O.run_fetd(om, max_steps=S, slots=slots)
+        dt = time.perf_counter() - t
+        vals.append((len(res.steps) - 1) / dt)
+        secs.append(dt)
+    info = dict(n_edges=om.n, steps=S, seconds=float(np.mean(secs)), threads=threads, reduced=reduced,
+                factorisations=slots.n_factor, stored=float(slots.stats[2]))
+    text = ("CPU restatement (oracle/: fetd_oracle's adaptive BDF2 loop on a supernodal Cholesky with the same "
+            "ordering, OpenMP + OpenBLAS on %d threads) on the %s %d-edge model: %d time steps from rest incl. "
+            "the factorisation, %.1f s per sample; not MKL PARDISO, which cannot be built here"
+            % (threads, "reduced-resolution" if reduced else "full-resolution", om.n, S, info["seconds"]))
+    return float(np.mean(vals)), info, text
 
 
 def inversion_cells(m, shape=(32, 32, 16), box=((-640.0, 640.0), (-640.0, 640.0), (0.0, 400.0))):
@@ -361,18 +312,17 @@ def reference_arm(args):
     if rank != 0:
         return 0
     cfg = args.config
-    cores = cpu_workers()
-    vals, info = cpu_parallel(cfg, args.sample_steps, args.warmup + args.steps, cores)
-    value = float(np.mean(vals[args.warmup:]))
+    value, info, text = cpu_arm(cfg, args.steps, args.warmup, args.sample_steps)
     line = {
         "impl": "reference", "metric": "FETD steps*RHS/s", "value": value, "unit": "steps*RHS/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": 1e3 * info["seconds"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": CONFIGS[cfg]["label"], "sample": "reduced-resolution model, first %d time steps"
-                   % args.sample_steps},
-        "cpu_baseline": {"value": value, "unit": "steps*RHS/s", "cores": cores, "kind": "port",
-                         "sample": cpu_sample_text(info)},
+        "config": {"workload": CONFIGS[cfg]["label"], "n_edges": info["n_edges"],
+                   "sample": "first %d time steps from rest per step" % info["steps"],
+                   "reduced_model": info["reduced"]},
+        "cpu_baseline": {"value": value, "unit": "steps*RHS/s", "cores": info["threads"], "kind": "port",
+                         "sample": text},
         "e2e": {"value": value, "unit": "steps*RHS/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -512,13 +462,17 @@ def ours(args):
                 "factor": {"achieved_tflops": factor_rate, "peak_dgemm_tflops": dgemm, "frac": factor_rate / dgemm}}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        nw = cpu_workers()
+        # the reference arm's measurement, one sample, in a fresh process (no CUDA, no torch threads)
+        env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+        cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--config", str(cfg), "--steps", "1",
+               "--warmup", "0", "--sample-steps", str(args.sample_steps)]
         try:
-            vs, inf = cpu_parallel(cfg, args.sample_steps, 1, nw)
-            cpu = {"value": vs[0], "unit": "steps*RHS/s", "cores": nw, "kind": "port",
-                   "sample": cpu_sample_text(inf)}
-        except RuntimeError as e:
-            cpu = {"value": None, "unit": "steps*RHS/s", "cores": nw, "kind": "port", "error": str(e)}
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800, env=env)
+            ref = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+            cpu = ref[-1]["cpu_baseline"] if r.returncode == 0 and ref else {
+                "value": None, "error": "CPU arm exited %d: %s" % (r.returncode, r.stderr[-300:])}
+        except subprocess.TimeoutExpired:
+            cpu = {"value": None, "error": "CPU arm did not finish in 1800 s"}
     line = {
         "metric": "FETD steps*RHS/s", "value": value, "unit": "steps*RHS/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,
@@ -555,7 +509,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2])
-    ap.add_argument("--sample-steps", type=int, default=40)
+    ap.add_argument("--sample-steps", type=int, default=0,
+                    help="CPU arm: time steps per sample (0: one doubling period, sp_double)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--adjoint", type=int, default=1, help="1: also time one adjoint gradient (single-RHS configs)")
     ap.add_argument("--models", type=int, default=16,

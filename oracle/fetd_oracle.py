@@ -509,6 +509,35 @@ def p_in_tet(nod_cor, tet_vex, p, rec_charac: float) -> int:
     return 0
 
 
+def locate_receivers(nod_cor, tet_vex, rec_cor, rec_charac: float) -> np.ndarray:
+    """p_in_tet for every receiver with the candidate tets' determinants
+    evaluated as one stack: the same test, the same first tet in index order.
+    Candidates whose bounding box (widened by a relative 1e-9) misses the
+    point are dropped first: the test only passes for a closed tet holding
+    the point, so no first hit is lost."""
+    X = nod_cor[tet_vex - 1]
+    mid = X.mean(axis=1)
+    lo, hi = X.min(axis=1), X.max(axis=1)
+    pad = 1e-9 * (hi - lo).max(axis=1, keepdims=True) + 1e-12
+    out = np.zeros(len(rec_cor), dtype=np.int64)
+    for r, p in enumerate(rec_cor):
+        inbox = ((lo - pad <= p) & (p <= hi + pad)).all(axis=1)
+        cand = np.nonzero(inbox & (np.sqrt(((mid - p) ** 2).sum(axis=1)) <= rec_charac))[0]
+        if len(cand) == 0:
+            continue
+        M = np.concatenate([X[cand], np.ones((len(cand), 4, 1))], axis=2)
+        dets = [np.linalg.det(M)]
+        for k in range(4):
+            Mk = M.copy()
+            Mk[:, k, :3] = p
+            dets.append(np.linalg.det(Mk))
+        D = np.stack(dets, axis=1)
+        ok = np.nonzero((D >= 0).all(axis=1) | (D <= 0).all(axis=1))[0]
+        if len(ok):
+            out[r] = int(cand[ok[0]]) + 1
+    return out
+
+
 # --------------------------------------------------------------------------
 # Source waveforms (source_mod)
 # --------------------------------------------------------------------------
@@ -622,7 +651,7 @@ def build_model(mesh: Dict[str, np.ndarray], ctl: Control,
     if src_edg is None:
         src_edg, src_drc = source_edges(edg_vex, mesh["src_vex"])
     if rec_tet is None:
-        rec_tet = np.array([p_in_tet(nod_cor, tet_vex, p, ctl.rec_charac) for p in ctl.rec_cor])
+        rec_tet = locate_receivers(nod_cor, tet_vex, ctl.rec_cor, ctl.rec_charac)
         if (rec_tet == 0).any():
             raise ValueError("no rec tet No. %d" % (int(np.argmin(rec_tet)) + 1))
     n_arr, d_arr = receiver_operators(a, b, c, d, vol, tet_len, rec_tet, ctl.rec_cor)
@@ -832,9 +861,11 @@ def adap_euler(model: OracleModel, slots: SuperLUSlots, out: Optional[_Output],
 
 
 def run_fetd(model: OracleModel, max_steps: Optional[int] = None, time_maximum: Optional[float] = None,
-             legacy_linux: bool = False) -> FetdResult:
-    """``time_solver`` (src/FETD_FWD.f90:1174-1227) with MKL replaced by SuperLU."""
-    slots = SuperLUSlots(model)
+             legacy_linux: bool = False, slots=None) -> FetdResult:
+    """``time_solver`` (src/FETD_FWD.f90:1174-1227) with MKL replaced by SuperLU
+    (or by other factor slots with the SuperLUSlots interface)."""
+    if slots is None:
+        slots = SuperLUSlots(model)
     out = _Output(model)
     ctl = model.ctl
     if ctl.step_mthd != 2:

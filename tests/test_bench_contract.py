@@ -1,5 +1,6 @@
-"""The bench's reference arm (CPU restatement on a bounded sample) prints
-one JSON line with the contract's keys; runs without a GPU."""
+"""The bench's reference arm (the CPU restatement on the host cores, on a
+bounded sample) prints one JSON line with the contract's keys; runs without a
+GPU (here on the 150k-edge model)."""
 import json
 import os
 import subprocess
@@ -9,8 +10,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def test_reference_arm_prints_one_json_line():
-    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "0", "--sample-steps", "4"], capture_output=True, text=True, timeout=600)
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--config", "0",
+                        "--steps", "1", "--warmup", "1", "--sample-steps", "4"], capture_output=True, text=True,
+                       timeout=600)
     assert r.returncode == 0, r.stderr
     lines = [ln for ln in r.stdout.splitlines() if ln.strip().startswith("{")]
     assert len(lines) == 1

@@ -147,3 +147,20 @@ def test_linux_golden_time_column_legacy_schedule():
     steps_t = np.array(steps_t)
     ok = g[:, 1] > 0
     assert np.allclose(steps_t[ok], g[ok, 1], rtol=6e-4)
+
+
+def test_stacked_receiver_location_matches_the_scan():
+    """locate_receivers (all candidate determinants at once) picks the same
+    tet as the restated linear scan p_in_tet (src/FETD_FWD.f90:1009-1049),
+    including points on shared vertices, edges and faces, where the first tet
+    in index order wins."""
+    from tests.golden_cases import tiny_synth
+    m = tiny_synth()
+    X, T = m.mesh.nod_cor, m.mesh.tet_vex
+    rng = np.random.default_rng(5)
+    pts = [X[T[k] - 1].mean(axis=0) for k in rng.integers(0, len(T), 6)]
+    pts += [X[T[3, 0] - 1], 0.5 * (X[T[7, 0] - 1] + X[T[7, 1] - 1]), X[T[11, :3] - 1].mean(axis=0)]
+    pts = np.array(pts)
+    got = O.locate_receivers(X, T, pts, 1e6)
+    want = np.array([O.p_in_tet(X, T, p, 1e6) for p in pts])
+    assert np.array_equal(got, want) and (got > 0).all()
