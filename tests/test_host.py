@@ -229,3 +229,18 @@ def test_ordering_does_not_depend_on_host_threads(monkeypatch):
     for t in ("3", "8"):
         assert np.array_equal(out[t][0], out["1"][0])
         assert np.array_equal(out[t][1][[0, 1, 2, 3, 4, 5, 8]], out["1"][1][[0, 1, 2, 3, 4, 5, 8]])
+
+
+def test_topology_on_renumbered_mesh_matches_oracle():
+    """Edge numbering, tet->edge map and signs of the library (counting sort
+    by the smaller vertex) against the oracle's restatement, on a synthetic
+    mesh whose vertices are renumbered and whose tets are shuffled, so that
+    vertex indices and tet order carry no structure."""
+    m = tiny_synth()
+    rng = np.random.default_rng(11)
+    nv = m.mesh.nod_cor.shape[0]
+    relabel = rng.permutation(nv) + 1
+    tv = relabel[m.mesh.tet_vex - 1][rng.permutation(m.mesh.tet_vex.shape[0])]
+    ev, te, td = fetd.mesh_topology(tv)
+    e2, t2, d2 = O.build_topology(tv.astype(np.int64))
+    assert np.array_equal(ev, e2) and np.array_equal(te, t2) and np.array_equal(td, d2)
