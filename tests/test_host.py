@@ -244,3 +244,21 @@ def test_topology_on_renumbered_mesh_matches_oracle():
     ev, te, td = fetd.mesh_topology(tv)
     e2, t2, d2 = O.build_topology(tv.astype(np.int64))
     assert np.array_equal(ev, e2) and np.array_equal(te, t2) and np.array_equal(td, d2)
+
+
+def test_fortran_interfaces_cover_the_header():
+    """INTEGRATION.md's ISO_C_BINDING module declares every entry point of
+    include/temf_b200.h with the same number of arguments."""
+    with open(os.path.join(ROOT, "include", "temf_b200.h")) as fh:
+        txt = re.sub(r"/\*.*?\*/", "", fh.read(), flags=re.S)
+    header = {}
+    for m in re.finditer(r"\b(temf_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", txt, flags=re.S):
+        args = m.group(2).strip()
+        header[m.group(1)] = 0 if args in ("", "void") else len(args.split(","))
+    with open(os.path.join(ROOT, "INTEGRATION.md")) as fh:
+        doc = fh.read()
+    fortran = {m.group(1): (0 if not m.group(2).strip() else len(m.group(2).split(",")))
+               for m in re.finditer(r"function (temf_[a-z0-9_]+)\(([^)]*)\)", doc)}
+    assert set(header) <= set(fortran), sorted(set(header) - set(fortran))
+    for name, n in header.items():
+        assert fortran[name] == n, name
