@@ -197,6 +197,7 @@ void build_adjacency(const temf_ctx& c, std::vector<int64_t>& xadj, std::vector<
 void build_pattern(const temf_ctx& c, const std::vector<int>& perm, const std::vector<int>& iperm,
                    Pattern& P) {
   const int n = c.n_edges, T = c.n_tets;
+  if (21LL * T > (int64_t)INT32_MAX) throw ArgError("mesh too large: element entries k * n_tets + t exceed int32");
   std::vector<int64_t> iptr;
   std::vector<int> inc;
   edge_incidence(c, iptr, inc);
