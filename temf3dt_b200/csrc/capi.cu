@@ -1144,7 +1144,7 @@ int temf_adjoint_timing(temf_ctx* c, double* ms, long long* counts) {
 int temf_set_analysis_options(temf_ctx* c, int leaf_size, int amalg_level) {
   return guarded(c, [&] {
     if (leaf_size < 8 || leaf_size > 100000) throw ArgError("leaf_size must be in [8, 100000]");
-    if (amalg_level < 0 || amalg_level > 2) throw ArgError("amalg_level must be 0, 1 or 2");
+    if (amalg_level < 0 || amalg_level > 3) throw ArgError("amalg_level must be 0, 1, 2 or 3");
     c->sym_opt.leaf_size = leaf_size;
     c->sym_opt.amalgamate = amalg_level > 0;
     c->sym_opt.amalg_level = amalg_level;

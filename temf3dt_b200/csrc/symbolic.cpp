@@ -611,7 +611,9 @@ void analyse(int n, const int64_t* xadj, const int* adj, const double* xyz,
         int64_t nz_m = c * (c + 1) / 2 + c * r2;
         int64_t zeros = nz_m - nz_s - nz_p + rep_zeros[s] + rep_zeros[p];
         double zf = (double)zeros / (double)nz_m;
-        bool ok = opt.amalg_level >= 2
+        bool ok = opt.amalg_level >= 3
+                      ? (c <= 16) || (c <= 32 && zf < 0.4) || (c <= 64 && zf < 0.25) || (c <= 256 && zf < 0.05)
+                  : opt.amalg_level == 2
                       ? (c <= 16) || (c <= 32 && zf < 0.3) || (c <= 64 && zf < 0.15) || (c <= 256 && zf < 0.05)
                       : (c <= 4) || (c <= 16 && zf < 0.8) || (c <= 48 && zf < 0.1) || (c <= 256 && zf < 0.05);
         if (!ok) break;

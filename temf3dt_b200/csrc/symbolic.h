@@ -19,7 +19,8 @@ struct SymbolicOptions {
   int leaf_size = 96;          // nested-dissection leaf size
   int max_sn_cols = 64;        // supernodes are split into column blocks of at most this width
   bool amalgamate = true;      // relaxed supernode amalgamation
-  int amalg_level = 2;         // 1: merge while the zero fraction stays small; 2: merge small supernodes harder
+  int amalg_level = 2;         // 1: merge while the zero fraction stays small; 2: merge small supernodes harder;
+                               // 3: also merge up to 64 columns at 25 % zeros (fewer bottom tasks)
   int threads = 0;             // host threads for the ordering (0: $TEMF_HOST_THREADS, else all cores);
                                // the result does not depend on it
 };

@@ -139,7 +139,8 @@ class FetdGPU:
 
     def set_analysis_options(self, leaf_size: int = 96, amalg_level: int = 2) -> None:
         """Options of the next analyse(): nested-dissection leaf size and
-        supernode amalgamation (0 none, 1 light, 2 harder: the default)."""
+        supernode amalgamation (0 none, 1 light, 2 harder: the default,
+        3 hardest: up to 64 columns at 25 % explicit zeros)."""
         self._ck(self._L.temf_set_analysis_options(self._h, int(leaf_size), int(amalg_level)),
                  "temf_set_analysis_options")
 
