@@ -27,8 +27,8 @@ which cannot be built or run here; its CPU restatement is timed instead: the
 oracle's adaptive BDF2 loop on a multithreaded supernodal Cholesky
 (oracle/supernodal_cpu.cpp, the same ordering as the GPU path, OpenMP +
 OpenBLAS on all host cores), on the full-resolution model, each bench step
-one run from rest over a doubling period (sp_double time steps) including
-its factorisation.
+one run from rest up to the first doubling trial (sp_double - 1 time
+steps) including its factorisation.
 """
 from __future__ import annotations
 
@@ -148,8 +148,8 @@ def cpu_arm(cfg: int, steps: int, warmup: int, sample_steps: int = 0, scaled: bo
     fetd_oracle on the CPU supernodal Cholesky (oracle/supernodal_cpu.cpp,
     OpenMP + OpenBLAS, all host cores), on the full-resolution model of the
     config.  One bench step = one run of the loop from rest over its first
-    `sample_steps` time steps (default: one doubling period, sp_double),
-    including its factorisation.  Warm-up steps run one time step each.
+    `sample_steps` time steps (default: sp_double - 1, up to the first
+    doubling trial), including its factorisation.  Warm-up steps run one time step each.
     `scaled`: a shorter sample whose factorisation time is amortised over a
     doubling period (one factorisation per sp_double steps, as in the full
     run): steps/s = 1 / (seconds per time step + factorisation / sp_double).
@@ -173,7 +173,9 @@ def cpu_arm(cfg: int, steps: int, warmup: int, sample_steps: int = 0, scaled: bo
     except ImportError:
         pass
     period = int(om.ctl.step_dble)
-    S = sample_steps or period
+    # the default sample stops before the first doubling trial (step sp_double), whose extra
+    # factorisation would give it two factorisations per period instead of the run's one
+    S = sample_steps or period - 1
     fac_s = [0.0]
     factor = slots.factor
 
@@ -532,7 +534,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2])
     ap.add_argument("--sample-steps", type=int, default=0,
-                    help="CPU arm: time steps per sample (0: one doubling period, sp_double)")
+                    help="CPU arm: time steps per sample (0: sp_double - 1, up to the first doubling trial)")
     ap.add_argument("--cpu-scaled", type=int, default=0,
                     help="CPU arm: amortise the sample's factorisation over a doubling period")
     ap.add_argument("--no-cpu", action="store_true")
