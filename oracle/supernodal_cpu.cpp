@@ -290,6 +290,7 @@ int factor_panel_tiled(Solver& S, double* L, int s) {
 }
 
 int factor(Solver& S, int slot, double dt) {
+  omp_set_num_threads(S.threads);  // the thread count is per process; another handle may have changed it
   double* L = S.L[slot].get();
   std::memset(L, 0, sizeof(double) * S.stored);
   const int64_t nb = (int64_t)S.posB.size(), nc = (int64_t)S.posC.size();
@@ -356,6 +357,7 @@ void par_gemv_t(const Solver& S, int m, int n, double alpha, const double* A, in
 // matrix-vector products in between split over the threads; other levels
 // run their supernodes on the threads.  BLAS stays single-threaded.
 void solve(Solver& S, int slot, const double* b, double* x) {
+  omp_set_num_threads(S.threads);
   const double* L = S.L[slot].get();
   std::vector<double> y(S.n), z;
   for (int i = 0; i < S.n; ++i) y[i] = b[S.perm[i]];
