@@ -203,7 +203,6 @@ void build_pattern(const temf_ctx& c, const std::vector<int>& perm, const std::v
   edge_incidence(c, iptr, inc);
   struct Part {
     std::vector<int> rowlen, col, cnt, idx;  // per row: entries; per entry: contributions
-    std::exception_ptr failed;
   };
   auto rows = [&](int r0, int r1, Part& out) {
     std::vector<int> slot(n, -1);  // new column -> local entry index within the current row
@@ -244,25 +243,7 @@ void build_pattern(const temf_ctx& c, const std::vector<int>& perm, const std::v
   };
   const int nt = std::max(1, std::min(host_threads(0), n / 50000));
   std::vector<Part> parts(nt);
-  {
-    std::vector<std::thread> pool;
-    for (int k = 1; k < nt; ++k)
-      pool.emplace_back([&, k] {
-        try {
-          rows((int)((int64_t)n * k / nt), (int)((int64_t)n * (k + 1) / nt), parts[k]);
-        } catch (...) {
-          parts[k].failed = std::current_exception();
-        }
-      });
-    try {
-      rows(0, (int)((int64_t)n / nt), parts[0]);
-    } catch (...) {
-      parts[0].failed = std::current_exception();
-    }
-    for (std::thread& t : pool) t.join();
-    for (const Part& q : parts)
-      if (q.failed) std::rethrow_exception(q.failed);
-  }
+  parallel_for_each(nt, [&](int k) { rows((int)((int64_t)n * k / nt), (int)((int64_t)n * (k + 1) / nt), parts[k]); });
   int64_t nnz = 0, ncontr = 0;
   for (const Part& q : parts) {
     nnz += (int64_t)q.col.size();

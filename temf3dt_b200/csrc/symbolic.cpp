@@ -136,35 +136,22 @@ Split best_split(NDState& S, int* v, int m) {
     std::vector<int> va(v, v + m), vb(extra == 2 ? m : 0);
     std::vector<int> ra(S.n), rb(extra == 2 ? S.n : 0);
     if (extra == 2) std::copy(v, v + m, vb.begin());
-    std::exception_ptr fa, fb;
-    std::thread ta([&] {
-      try {
-        if (hi[1] > lo[1]) eval_axis(S, va.data(), m, 1, id, ra.data(), cand[1]);
-        if (extra == 1 && hi[2] > lo[2]) eval_axis(S, va.data(), m, 2, id, ra.data(), cand[2]);
-      } catch (...) {
-        fa = std::current_exception();
-      }
-    });
-    std::thread tb;
-    if (extra == 2)
-      tb = std::thread([&] {
-        try {
-          if (hi[2] > lo[2]) eval_axis(S, vb.data(), m, 2, id, rb.data(), cand[2]);
-        } catch (...) {
-          fb = std::current_exception();
+    try {
+      parallel_for_each(1 + extra, [&](int k) {
+        if (k == 0) {
+          if (hi[0] > lo[0]) eval_axis(S, v, m, 0, id, S.rank.data(), cand[0]);
+        } else if (k == 1) {
+          if (hi[1] > lo[1]) eval_axis(S, va.data(), m, 1, id, ra.data(), cand[1]);
+          if (extra == 1 && hi[2] > lo[2]) eval_axis(S, va.data(), m, 2, id, ra.data(), cand[2]);
+        } else if (hi[2] > lo[2]) {
+          eval_axis(S, vb.data(), m, 2, id, rb.data(), cand[2]);
         }
       });
-    std::exception_ptr f0;
-    try {
-      if (hi[0] > lo[0]) eval_axis(S, v, m, 0, id, S.rank.data(), cand[0]);
     } catch (...) {
-      f0 = std::current_exception();
+      S.spare_threads.fetch_add(extra);
+      throw;
     }
-    ta.join();
-    if (tb.joinable()) tb.join();
     S.spare_threads.fetch_add(extra);
-    for (const std::exception_ptr& e : {f0, fa, fb})
-      if (e) std::rethrow_exception(e);
   }
   Split best;
   for (int a = 0; a < 3; ++a)
@@ -295,24 +282,16 @@ void nd_rec(NDState& S, int* v, int m) {
     nd_rec(S, v + nl, nr);
     return;
   }
-  std::exception_ptr failed;
-  std::thread left([&] {
-    try {
-      nd_rec(S, v, nl);
-    } catch (...) {
-      failed = std::current_exception();
-    }
-  });
-  std::exception_ptr failed_right;
   try {
-    nd_rec(S, v + nl, nr);
+    parallel_for_each(2, [&](int k) {
+      if (k == 0) nd_rec(S, v + nl, nr);
+      else nd_rec(S, v, nl);
+    });
   } catch (...) {
-    failed_right = std::current_exception();
+    S.spare_threads.fetch_add(1);
+    throw;
   }
-  left.join();
   S.spare_threads.fetch_add(1);
-  if (failed) std::rethrow_exception(failed);
-  if (failed_right) std::rethrow_exception(failed_right);
 }
 
 // Column counts of L for a postordered elimination tree (children before
@@ -453,24 +432,7 @@ void update_groups(const Symbolic& S, UpdateGroups& G, int threads) {
     while (s < nsn && roff[s] < target) ++s;
     cut[k] = s;
   }
-  std::vector<std::exception_ptr> failed(nt);
-  std::vector<std::thread> pool;
-  for (int k = 1; k < nt; ++k)
-    pool.emplace_back([&, k] {
-      try {
-        fill(cut[k], cut[k + 1]);
-      } catch (...) {
-        failed[k] = std::current_exception();
-      }
-    });
-  try {
-    fill(cut[0], cut[1]);
-  } catch (...) {
-    failed[0] = std::current_exception();
-  }
-  for (std::thread& t : pool) t.join();
-  for (const std::exception_ptr& e : failed)
-    if (e) std::rethrow_exception(e);
+  parallel_for_each(nt, [&](int k) { fill(cut[k], cut[k + 1]); });
 }
 
 std::vector<int> nested_dissection(int n, const int64_t* xadj, const int* adj,

@@ -8,8 +8,12 @@
 // (src/FETD_UTILITY.f90:912-917) whose ordering the reference leaves at MKL's
 // default (iparm = 0, :909-910).
 #pragma once
+#include <algorithm>
 #include <cstdint>
+#include <exception>
 #include <memory>
+#include <system_error>
+#include <thread>
 #include <vector>
 #include <string>
 
@@ -80,6 +84,41 @@ void update_groups(const Symbolic& S, UpdateGroups& G, int threads = 0);
 // Host threads to use for a request (0: $TEMF_HOST_THREADS, else the cores
 // this process may run on, at most 64).
 int host_threads(int requested);
+
+// Runs work(k) for k = 0 .. n-1: k >= 1 on new threads where one can be
+// created, the rest on the calling thread; rethrows the first exception
+// after all have finished.
+template <class F>
+void parallel_for_each(int n, F&& work) {
+  std::vector<std::exception_ptr> failed(std::max(n, 1));
+  std::vector<std::thread> pool;
+  pool.reserve(std::max(n - 1, 0));
+  std::vector<int> here{0};
+  for (int k = 1; k < n; ++k) {
+    try {
+      pool.emplace_back([&work, &failed, k] {
+        try {
+          work(k);
+        } catch (...) {
+          failed[k] = std::current_exception();
+        }
+      });
+    } catch (const std::system_error&) {
+      here.push_back(k);
+    }
+  }
+  for (int k : here) {
+    if (k >= n) break;
+    try {
+      work(k);
+    } catch (...) {
+      failed[k] = std::current_exception();
+    }
+  }
+  for (std::thread& t : pool) t.join();
+  for (const std::exception_ptr& e : failed)
+    if (e) std::rethrow_exception(e);
+}
 
 // Full symbolic analysis.  (xadj, adj) is the symmetric pattern of A in the
 // original numbering without the diagonal; xyz gives a point per unknown
