@@ -502,8 +502,11 @@ def ours(args):
         try:
             r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800, env=env)
             ref = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
-            cpu = ref[-1]["cpu_baseline"] if r.returncode == 0 and ref else {
-                "value": None, "error": "CPU arm exited %d: %s" % (r.returncode, r.stderr[-300:])}
+            if r.returncode == 0 and ref and "cpu_baseline" in ref[-1]:
+                cpu = ref[-1]["cpu_baseline"]
+            else:
+                why = ref[-1].get("unavailable") if ref else "exit %d: %s" % (r.returncode, r.stderr[-300:])
+                cpu = {"value": None, "error": "CPU arm: %s" % why}
         except subprocess.TimeoutExpired:
             cpu = {"value": None, "error": "CPU arm did not finish in 1800 s"}
     line = {
