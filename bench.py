@@ -336,6 +336,23 @@ def models_measure(local: int, n_models: int = 16):
             "merged_solves": tm["merged_solves"], "tuning": tu}
 
 
+def cpu_baseline(cfg: int, sample_steps: int) -> dict:
+    """The GPU line's cpu_baseline: the reference arm's measurement as one
+    scaled sample, run in a fresh process (no CUDA context, no torch threads)."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--config", str(cfg), "--steps", "1",
+           "--warmup", "0", "--sample-steps", str(sample_steps), "--cpu-scaled", "1"]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800, env=env)
+    except subprocess.TimeoutExpired:
+        return {"value": None, "error": "CPU arm did not finish in 1800 s"}
+    ref = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode == 0 and ref and "cpu_baseline" in ref[-1]:
+        return ref[-1]["cpu_baseline"]
+    why = ref[-1].get("unavailable") if ref else "exit %d: %s" % (r.returncode, r.stderr[-300:])
+    return {"value": None, "error": "CPU arm: %s" % why}
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -495,20 +512,7 @@ def ours(args):
                 "factor": {"achieved_tflops": factor_rate, "peak_dgemm_tflops": dgemm, "frac": factor_rate / dgemm}}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        # the reference arm's measurement, one sample, in a fresh process (no CUDA, no torch threads)
-        env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
-        cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--config", str(cfg), "--steps", "1",
-               "--warmup", "0", "--sample-steps", str(args.sample_steps or 10), "--cpu-scaled", "1"]
-        try:
-            r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800, env=env)
-            ref = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
-            if r.returncode == 0 and ref and "cpu_baseline" in ref[-1]:
-                cpu = ref[-1]["cpu_baseline"]
-            else:
-                why = ref[-1].get("unavailable") if ref else "exit %d: %s" % (r.returncode, r.stderr[-300:])
-                cpu = {"value": None, "error": "CPU arm: %s" % why}
-        except subprocess.TimeoutExpired:
-            cpu = {"value": None, "error": "CPU arm did not finish in 1800 s"}
+        cpu = cpu_baseline(cfg, args.sample_steps or 10)
     line = {
         "metric": "FETD steps*RHS/s", "value": value, "unit": "steps*RHS/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_s * 1e3 / args.steps, "higher_is_better": True,

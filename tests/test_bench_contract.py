@@ -24,3 +24,14 @@ def test_reference_arm_prints_one_json_line():
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_gpu_line_cpu_baseline_runs_in_a_fresh_process():
+    """The cpu_baseline object of the GPU arm's line (a scaled sample of the
+    reference arm, run as a subprocess): value, unit, cores, kind, sample."""
+    sys.path.insert(0, ROOT)
+    import bench
+    cpu = bench.cpu_baseline(0, 3)
+    assert cpu.get("value") and cpu["value"] > 0, cpu
+    assert cpu["unit"] == "steps*RHS/s" and cpu["kind"] == "port" and cpu["cores"] >= 1
+    assert "amortised" in cpu["sample"]
