@@ -37,6 +37,7 @@ extern "C" {
 
 typedef struct temf_ctx temf_ctx;
 typedef struct temf_batch temf_batch;
+typedef struct temf_case temf_case;
 
 /* ---- context --------------------------------------------------------- */
 /* Create a context on CUDA device `device`. */
@@ -317,6 +318,49 @@ int temf_pardiso_direct_1(temf_ctx* ctx, int num_m, int symm, int n, int nnz, co
 int temf_pardiso_direct_2(temf_ctx* ctx, int num_m, const double* b, double* x);
 int temf_pardiso_direct_3(temf_ctx* ctx, int num_m);
 int temf_pardiso_dealloc(temf_ctx* ctx);
+
+/* ---- the reference's file front end (./FETD -f ROOT) --------------------------
+ * Host only, except temf_case_load / temf_case_run, which drive a context.
+ *
+ * temf_case_read: ROOT.mesh (model_mesh, MEDIT sections Vertices / Edges
+ * (tagged edges = source segments) / Tetrahedra, src/FETD_FWD.f90:112-166) and
+ * ROOT.cntl (model_ctl keywords, :284-497, with its completeness test,
+ * :490-497).  On failure returns TEMF_EARG with the reason in msg. */
+int temf_case_read(const char* root, temf_case** out, char* msg, int msg_len);
+int temf_case_free(temf_case* cs);
+/* sizes[0..6] = nodes, tets, source segments, receivers, isotropic domains,
+ * anisotropic domains, time points (-1 when the cntl has none). */
+int temf_case_sizes(const temf_case* cs, int* sizes);
+/* The mesh in the reference's Fortran layouts: nod_cor(nodes,3),
+ * tet_vex(tets,4), tet_phy(tets), src_vex(segments,2), src_phy(segments);
+ * 1-based vertex numbers.  NULL arrays are skipped. */
+int temf_case_mesh(const temf_case* cs, double* nod_cor, int* tet_vex, int* tet_phy, int* src_vex, int* src_phy);
+/* The control: ints[10] = bound_cond, src_num, source_type, pulse_type,
+ * sp_mthd, sp_division, sp_double, sp_dblesize, vtkout, output mask (bit k =
+ * column k of ex ey ez dx dy dz bx by bz); reals[4] = rec_charac, t0,
+ * current, time_maximum; rec_cor(receivers,3); time_points. */
+int temf_case_control(const temf_case* cs, int* ints, double* reals, double* rec_cor, double* time_points);
+/* Media per tet (src/FETD_FWD.f90:347-409): *aniso = 0: sig(tets) and
+ * mu(tets) = mu_r mu0; *aniso = 1: row-major 3 x 3 tensors (tets,9), the
+ * rotation as the reference builds it.  TEMF_EARG if a tet's physical domain
+ * is not in the cntl. */
+int temf_case_media(const temf_case* cs, double* sig, double* mu, int* aniso);
+/* .field rows as solution_output writes them (src/FETD_FWD.f90:1623,
+ * format i6, e15.5, 2x, nrec(n e15.5, 2x), n = selected columns): steps(rows),
+ * times(rows), fields(9, nrec, rows) as temf_result_get returns them,
+ * output_mask[9] (non-zero = written).  Fortran E15.5 numbers. */
+int temf_case_write_rows(const char* path, int rows, int nrec, const int* steps, const double* times,
+                         const double* fields, const int* output_mask);
+/* mesh_process and the source/receiver set-up on a fresh context: edge
+ * topology, mesh, media, boundary, analysis, assembly, src_edg/src_drc (+1,
+ * last -1, src/FETD_FWD.f90:435-448), receiver location and operators. */
+int temf_case_load(temf_case* cs, temf_ctx* ctx, char* msg, int msg_len);
+/* ROOT.field from the last temf_run of ctx, and ROOT.field2 (the time_points
+ * rows the run reached, numbered from 1) when the cntl has time_points. */
+int temf_case_write(const temf_case* cs, temf_ctx* ctx, const char* root, char* msg, int msg_len);
+/* `./FETD -f ROOT` on GPU `device`: read, load, temf_run (flags as there),
+ * write ROOT.field(2). */
+int temf_case_run(const char* root, int device, int flags, char* msg, int msg_len);
 
 #ifdef __cplusplus
 }

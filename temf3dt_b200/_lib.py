@@ -68,6 +68,16 @@ SIGNATURES = {
     "temf_adjoint": (_i, [_p, _dp, _i, _ip, _dp, _dp]),
     "temf_adjoint_timing": (_i, [_p, _dp, C.POINTER(C.c_longlong)]),
     "temf_pardiso_checker": (_i, [_i, _i, _i, _ip, _ip, _ip, C.c_char_p, _i]),
+    "temf_case_read": (_i, [C.c_char_p, C.POINTER(_p), C.c_char_p, _i]),
+    "temf_case_free": (_i, [_p]),
+    "temf_case_sizes": (_i, [_p, _ip]),
+    "temf_case_mesh": (_i, [_p, _dp, _ip, _ip, _ip, _ip]),
+    "temf_case_control": (_i, [_p, _ip, _dp, _dp, _dp]),
+    "temf_case_media": (_i, [_p, _dp, _dp, _ip]),
+    "temf_case_write_rows": (_i, [C.c_char_p, _i, _i, _ip, _dp, _dp, _ip]),
+    "temf_case_load": (_i, [_p, _p, C.c_char_p, _i]),
+    "temf_case_write": (_i, [_p, _p, C.c_char_p, C.c_char_p, _i]),
+    "temf_case_run": (_i, [C.c_char_p, _i, _i, C.c_char_p, _i]),
     "temf_pardiso_alloc": (_i, [_p, _i]),
     "temf_pardiso_direct_1": (_i, [_p, _i, _i, _i, _i, _ip, _ip, _dp]),
     "temf_pardiso_direct_2": (_i, [_p, _i, _dp, _dp]),

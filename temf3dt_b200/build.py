@@ -15,9 +15,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libtemf_b200.so")
+CLI = os.path.join(HERE, "temf_fetd")
 BUILD = os.path.join(ROOT, "_build")
 
-SOURCES = ["symbolic.cpp", "assemble.cu", "factor.cu", "solve.cu", "fetd.cu", "capi.cu", "noalloc.cu", "adjoint.cu", "batch.cu"]
+SOURCES = ["symbolic.cpp", "assemble.cu", "factor.cu", "solve.cu", "fetd.cu", "capi.cu", "noalloc.cu", "adjoint.cu", "batch.cu",
+           "case.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
           "-I" + CSRC, "-I" + os.path.join(ROOT, "include")]
@@ -59,6 +61,14 @@ def build(verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
+    # the command-line driver (./FETD -f ROOT), linked against the library next to it
+    main = os.path.join(CSRC, "fetd_main.cpp")
+    if not os.path.exists(CLI) or os.path.getmtime(CLI) < max(os.path.getmtime(LIB), os.path.getmtime(main)):
+        cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), "-o", CLI, main, "-L" + HERE,
+               "-ltemf_b200", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("temf_fetd link failed:\n%s\n%s" % (r.stdout, r.stderr))
     return LIB
 
 

@@ -451,6 +451,109 @@ def run_case(root: str, device: int = 0, legacy_linux: bool = False, write: bool
         if write:
             meshio.write_field(root + ".field", out.steps, out.times, out.fields, ctl.output)
             if ctl.time_points is not None:
-                g, _done = gpu.gates(ctl.time_points)
-                meshio.write_field(root + ".field2", np.arange(1, len(g) + 1), ctl.time_points, g, ctl.output)
+                g, done = gpu.gates(ctl.time_points)
+                idx = np.nonzero(done)[0]
+                meshio.write_field(root + ".field2", idx + 1, ctl.time_points[idx], g[idx], ctl.output)
         return out
+
+
+class CaseFile:
+    """ROOT.mesh + ROOT.cntl read by the library's C++ front end
+    (temf_case_read: model_mesh and model_ctl); the arrays in the reference's
+    conventions (1-based vertices), plus loading a context and writing the
+    .field files the way the reference's driver does."""
+
+    def __init__(self, root: str):
+        L = lib()
+        h = C.c_void_p()
+        msg = C.create_string_buffer(512)
+        rc = L.temf_case_read(root.encode(), C.byref(h), msg, 512)
+        if rc != 0:
+            raise ValueError(msg.value.decode() or "temf_case_read failed")
+        self._L, self._h = L, h
+        sz = np.zeros(7, dtype=np.int32)
+        L.temf_case_sizes(h, iptr(sz))
+        N, T, S, R = int(sz[0]), int(sz[1]), int(sz[2]), int(sz[3])
+        nod = np.zeros(3 * N)
+        tv = np.zeros(4 * T, dtype=np.int32)
+        tp = np.zeros(max(T, 1), dtype=np.int32)
+        sv = np.zeros(max(2 * S, 1), dtype=np.int32)
+        spn = np.zeros(max(S, 1), dtype=np.int32)
+        L.temf_case_mesh(h, dptr(nod), iptr(tv), iptr(tp), iptr(sv), iptr(spn))
+        self.nod_cor = nod.reshape(3, N).T.copy()
+        self.tet_vex = tv.reshape(4, T).T.copy()
+        self.tet_phy = tp[:T].copy()
+        self.src_vex = sv[:2 * S].reshape(2, S).T.copy()
+        self.src_phy = spn[:S].copy()
+        ints = np.zeros(10, dtype=np.int32)
+        reals = np.zeros(4)
+        rc_ = np.zeros(max(3 * R, 1))
+        ntp = int(sz[6])
+        tpts = np.zeros(max(ntp, 1))
+        L.temf_case_control(h, iptr(ints), dptr(reals), dptr(rc_), dptr(tpts))
+        (self.bound_cond, self.src_num, self.source_type, self.pulse_type, self.sp_mthd, self.sp_division,
+         self.sp_double, self.sp_dblesize, self.vtkout) = [int(v) for v in ints[:9]]
+        self.output = np.array([(int(ints[9]) >> k) & 1 == 1 for k in range(9)])
+        self.rec_charac, self.t0, self.current, self.time_maximum = [float(v) for v in reals]
+        self.rec_cor = rc_[:3 * R].reshape(3, R).T.copy()
+        self.time_points = tpts[:ntp].copy() if ntp >= 0 else None
+        self.n_iso, self.n_aniso = int(sz[4]), int(sz[5])
+
+    def close(self) -> None:
+        if self._h:
+            self._L.temf_case_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+    def media(self):
+        """(sig, mu, aniso): per tet (n_tets,) or row-major tensors (n_tets, 9)."""
+        T = self.tet_vex.shape[0]
+        a = C.c_int(0)
+        self._L.temf_case_media(self._h, None, None, C.byref(a))
+        k = 9 if a.value else 1
+        sig, mu = np.zeros(k * T), np.zeros(k * T)
+        rc = self._L.temf_case_media(self._h, dptr(sig), dptr(mu), C.byref(a))
+        if rc != 0:
+            raise ValueError("error - physical domain not found!")
+        return (sig.reshape(T, 9), mu.reshape(T, 9), True) if a.value else (sig, mu, False)
+
+    def load(self, gpu: "FetdGPU") -> None:
+        msg = C.create_string_buffer(512)
+        if self._L.temf_case_load(self._h, gpu._h, msg, 512) != 0:
+            raise ValueError(msg.value.decode())
+        self.n_edges = gpu.n_edges = self._edges(gpu)
+        gpu.n_tets = self.tet_vex.shape[0]
+        gpu.nrec = self.rec_cor.shape[0]
+
+    def _edges(self, gpu) -> int:
+        s = np.zeros(10)
+        gpu._ck(self._L.temf_analysis_stats(gpu._h, dptr(s)), "temf_analysis_stats")
+        return int(s[0])
+
+    def write(self, gpu: "FetdGPU", root: str) -> None:
+        msg = C.create_string_buffer(512)
+        if self._L.temf_case_write(self._h, gpu._h, root.encode(), msg, 512) != 0:
+            raise RuntimeError(msg.value.decode())
+
+
+def run_case_native(root: str, device: int = 0, legacy_linux: bool = False) -> None:
+    """``./FETD -f ROOT`` entirely in the library (temf_case_run)."""
+    msg = C.create_string_buffer(512)
+    if lib().temf_case_run(root.encode(), device, 1 if legacy_linux else 0, msg, 512) != 0:
+        raise RuntimeError(msg.value.decode())
+
+
+def write_field_rows(path: str, steps, times, fields: np.ndarray, output_mask) -> None:
+    """The library's .field writer (temf_case_write_rows); fields (rows, nrec, 9)."""
+    st = as_i32(steps)
+    tm = as_f64(times)
+    f = as_f64(np.asarray(fields, dtype=np.float64).reshape(len(st), -1, 9))
+    m = as_i32(np.asarray(output_mask, dtype=bool).astype(np.int32))
+    rc = lib().temf_case_write_rows(path.encode(), len(st), f.shape[1], iptr(st), dptr(tm), dptr(f), iptr(m))
+    if rc != 0:
+        raise TemfError(rc, "temf_case_write_rows")

@@ -244,15 +244,36 @@ def media_per_tet(tet_phy: np.ndarray, ctl: Control):
     return sig, mu
 
 
+def fortran_e(v: float, w: int = 15, d: int = 5) -> str:
+    """Fortran Ew.d: [-]0.ddddd E+ee right-justified in w columns (a
+    three-digit exponent drops the E)."""
+    v = float(v)
+    if v != v:
+        s = "NaN"
+    elif v in (float("inf"), float("-inf")):
+        s = "Infinity" if v > 0 else "-Infinity"
+    elif v == 0.0:
+        s = "0." + "0" * d + "E+00"
+    else:
+        t = "%.*E" % (d - 1, abs(v))
+        mant, ex = t.split("E")
+        e = int(ex) + 1
+        digits = mant.replace(".", "")
+        es = ("E%+03d" % e) if abs(e) < 100 else ("%+04d" % e)
+        s = ("-" if v < 0 else "") + "0." + digits + es
+    return s.rjust(w)
+
+
 def write_field(path: str, steps, times, fields: np.ndarray, output_mask: np.ndarray) -> None:
     """``.field`` rows: step, time, then the selected components per receiver
-    (src/FETD_FWD.f90:1623, format i6, e15.5, 2x, rec*(n e15.5, 2x))."""
+    (src/FETD_FWD.f90:1623, format i6, e15.5, 2x, rec*(n e15.5, 2x)), numbers
+    as Fortran's E15.5 writes them."""
     sel = np.nonzero(output_mask)[0]
     with open(path, "w") as fh:
         for i, (s, t) in enumerate(zip(steps, times)):
-            parts = ["%6d%15.5E  " % (s, t)]
+            parts = ["%6d%s  " % (s, fortran_e(t))]
             for r in range(fields.shape[1]):
-                parts.append("".join("%15.5E" % v for v in fields[i, r, sel]) + "  ")
+                parts.append("".join(fortran_e(v) for v in fields[i, r, sel]) + "  ")
             fh.write("".join(parts).rstrip() + "\n")
 
 
