@@ -34,3 +34,30 @@ def test_native_driver_matches_python_driver(tmp_path):
     assert r.returncode == 0, r.stderr
     _close(meshio.read_field(b + ".field"), meshio.read_field(a + ".field"))
     _close(meshio.read_field(b + ".field2"), meshio.read_field(a + ".field2"))
+
+
+def test_native_driver_reproduces_the_shipped_linux_field(tmp_path):
+    """temf_fetd --legacy-linux on the reference's LINUX/mod_big_sig_0.001
+    files (mesh re-emitted from the fixture, the shipped cntl text) against
+    the shipped .field, as the Python path is checked in test_gpu_parity."""
+    from tests.golden_cases import load_fixture
+    fx = load_fixture("linux_mod_big")
+    root = str(tmp_path / "mod_big")
+    meshio.write_mesh(root + ".mesh", meshio.Mesh(fx["nod_cor"], fx["tet_vex"].astype(np.int64),
+                                                  fx["tet_phy"].astype(np.int64), fx["src_vex"].astype(np.int64),
+                                                  fx["src_phy"].astype(np.int64)))
+    with open(root + ".cntl", "w") as fh:
+        fh.write(str(fx["cntl"]))
+    cli = os.path.join(ROOT, "temf3dt_b200", "temf_fetd")
+    r = subprocess.run([cli, "-f", root, "--legacy-linux"], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stderr
+    out = meshio.read_field(root + ".field")
+    gold = fx["field"]
+    n = min(len(out), len(gold))
+    same = np.isclose(out[:n, 1], gold[:n, 1], rtol=6e-4, atol=0) | (gold[:n, 1] == 0)
+    first_diff = int(np.argmin(same)) if not same.all() else n
+    assert first_diff >= 400, first_diff
+    v, gd = out[:first_diff, 2], gold[:first_diff, 2]
+    big = np.abs(gd) >= 1e-3 * np.abs(gd).max()
+    rel = np.abs(v[big] - gd[big]) / np.abs(gd[big])
+    assert rel.max() < 6e-4, rel.max()
