@@ -263,3 +263,39 @@ def test_fortran_interfaces_cover_the_header():
     assert set(header) <= set(fortran), sorted(set(header) - set(fortran))
     for name, n in header.items():
         assert fortran[name] == n, name
+
+
+@pytest.mark.parametrize("case", ["single", "disconnected", "isolated_and_chain", "coincident_points"])
+def test_analysis_of_degenerate_patterns(case):
+    """Ordering, symbolic analysis and the schedule replay on patterns a mesh
+    can degenerate to: one unknown, no edges, isolated unknowns beside a
+    chain, and unknowns that all sit at one point (no axis can split them)."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(1)
+    n, rows, cols, xyz = {
+        "single": (1, [], [], np.zeros((1, 3))),
+        "disconnected": (40, [], [], rng.random((40, 3))),
+        "isolated_and_chain": (500, list(range(100)), list(range(1, 101)), rng.random((500, 3))),
+        "coincident_points": (300, rng.integers(0, 300, 2000), rng.integers(0, 300, 2000), np.zeros((300, 3))),
+    }[case]
+    A = sp.coo_matrix((np.ones(len(rows)), (rows, cols)), shape=(n, n)).tocsr()
+    A = ((A + A.T) > 0).astype(float).tocsr()
+    A.setdiag(0)
+    A.eliminate_zeros()
+    A.sort_indices()
+    xadj, adj = A.indptr.astype(np.int64), A.indices.astype(np.int32)
+    perm, st = _symbolic(n, xadj, adj, np.ascontiguousarray(xyz))
+    assert np.array_equal(np.sort(perm), np.arange(n)) and st[8] >= n
+    msg = C.create_string_buffer(256)
+    rc = _lib.lib().temf_schedule_check(n, xadj.ctypes.data_as(C.POINTER(C.c_longlong)), _lib.iptr(adj),
+                                        _lib.dptr(np.ascontiguousarray(xyz)), msg, 256)
+    assert rc == 0, msg.value.decode()
+
+
+def test_single_tet_topology_follows_ind_tet():
+    """Local edges (1,2),(1,3),(1,4),(2,3),(4,2),(3,4) of ind_tet
+    (src/FETD_FWD.f90:23): the fifth runs from vertex 4 to 2, against the
+    global (2,4) edge, so its sign is -1."""
+    ev, te, td = fetd.mesh_topology(np.array([[1, 2, 3, 4]]))
+    assert ev.tolist() == [[1, 2], [1, 3], [1, 4], [2, 3], [2, 4], [3, 4]]
+    assert te.tolist() == [[1, 2, 3, 4, 5, 6]] and td.tolist() == [[1, 1, 1, 1, -1, 1]]
