@@ -978,6 +978,8 @@ int temf_batch_run(temf_batch* B, int sp_division, int sp_double, int sp_dblesiz
     for (temf_ctx* c : B->b.models) {
       need(c->assembled, "temf_batch_run: assemble every model first");
       need(c->src.nrhs >= 1, "temf_batch_run: set every model's source first");
+      for (int r = 0; r < c->rec.nrec; ++r)
+        if (c->rec.rec_rhs[r] >= c->src.nrhs) throw ArgError("a receiver samples a RHS column that does not exist");
       extra(c).run.valid = false;
       c->adj.valid = false;
     }
