@@ -132,3 +132,20 @@ def test_command_line_driver_reports_usage_and_missing_files(tmp_path):
     assert r.returncode == 2 and "usage" in r.stderr
     r = subprocess.run([cli, "-f", str(tmp_path / "nothing")], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "cannot open" in r.stderr
+
+
+def test_unknown_physical_domain_and_bad_writer_arguments(tmp_path):
+    m = tiny_synth()
+    ctl = meshio.read_cntl(_write_case(tmp_path, m.mesh, m.ctl) + ".cntl")
+    ctl.domains = ctl.domains[:1]               # drop the earth domains
+    root = _write_case(tmp_path, m.mesh, ctl, name="nodom")
+    cf = fetd.CaseFile(root)
+    with pytest.raises(ValueError, match="physical domain"):
+        cf.media()
+    from temf3dt_b200 import _lib
+    L = _lib.lib()
+    mask = np.ones(9, dtype=np.int32)
+    assert L.temf_case_write_rows(None, 1, 1, None, None, None, _lib.iptr(mask)) < 0
+    assert L.temf_case_write_rows(str(tmp_path / "x").encode(), 1, 1, None, None, None, _lib.iptr(mask)) < 0
+    assert L.temf_case_write_rows(str(tmp_path / "x").encode(), 0, 0, None, None, None, _lib.iptr(mask)) == 0
+    assert open(str(tmp_path / "x")).read() == ""
