@@ -96,3 +96,18 @@ def test_pardiso_checker_accepts_the_step_pattern_and_rejects_planted_errors():
     L = _lib.lib()
     ck = np.zeros(1, dtype=np.int32)
     assert L.temf_pardiso_checker(1, len(ia) - 1, len(ja), None, _lib.iptr(ja), _lib.iptr(ck), None, 0) < 0
+
+
+def test_source_segment_that_is_not_a_mesh_edge_is_rejected():
+    """A source segment must be an edge of the mesh (src_edg of model_ctl,
+    src/FETD_FWD.f90:435-448); two opposite corners of a tet's neighbour are not."""
+    from temf3dt_b200 import fetd
+    m = tiny_synth()
+    ev, _, _ = fetd.mesh_topology(m.mesh.tet_vex)
+    se, sd = fetd.source_edges(ev, m.mesh.src_vex)
+    assert len(se) == len(m.mesh.src_vex) and sd[-1] == -1
+    edges = set(map(tuple, ev.tolist()))
+    n = m.mesh.nod_cor.shape[0]
+    bad = next((a, b) for a in range(1, n + 1) for b in range(a + 1, n + 1) if (a, b) not in edges)
+    with pytest.raises(ValueError, match="not an edge"):
+        fetd.source_edges(ev, np.array([bad]))
