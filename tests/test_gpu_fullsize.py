@@ -29,8 +29,8 @@ def test_block_model_first_steps_match_the_cpu_restatement():
     om = synth_oracle_model(m)
     ref = O.run_fetd(om, max_steps=STEPS, slots=SN.SupernodalSlots(om))
     assert np.array_equal(out.steps, np.array(ref.steps))
-    for lo in (0, 3):                               # E, then dB/dt: scaled per receiver over the three components
+    for lo in (0, 3):                               # E, then dB/dt: relative to the largest value of the group
         a, b = out.fields[:, :, lo:lo + 3], ref.fields[:, :, lo:lo + 3]
-        scale = np.abs(b).max(axis=(0, 2), keepdims=True) + 1e-300
+        scale = np.abs(b).max() + 1e-300
         err = (np.abs(a - b) / scale).max()
         assert err <= 1e-8, (lo, err)
