@@ -292,7 +292,12 @@ int factor_panel_tiled(Solver& S, double* L, int s) {
 int factor(Solver& S, int slot, double dt) {
   omp_set_num_threads(S.threads);  // the thread count is per process; another handle may have changed it
   double* L = S.L[slot].get();
-  std::memset(L, 0, sizeof(double) * S.stored);
+  // zero the panels on all threads: faster, and on a multi-socket host the
+  // pages are spread over the memory nodes of the threads that use them
+  const int64_t chunk = 1 << 17;
+#pragma omp parallel for schedule(static)
+  for (int64_t q = 0; q < (S.stored + chunk - 1) / chunk; ++q)
+    std::memset(L + q * chunk, 0, sizeof(double) * (size_t)std::min(chunk, S.stored - q * chunk));
   const int64_t nb = (int64_t)S.posB.size(), nc = (int64_t)S.posC.size();
 #pragma omp parallel for schedule(static)
   for (int64_t k = 0; k < nb; ++k) L[S.posB[k]] += 3.0 * S.valB[k];
