@@ -552,6 +552,20 @@ int sncpu_solve(void* h, int slot, const double* b, double* x) {
   return 0;
 }
 
+// y = A x for a CSR matrix (int32 row pointers and columns) on the
+// solver's threads: the mkl_sparse_d_mv of the BDF2 right-hand side
+// (src/FETD_FWD.f90:1427), which MKL runs threaded
+void sncpu_spmv(void* h, int n, const int* ptr, const int* col, const double* val, const double* x, double* y) {
+  Solver* S = static_cast<Solver*>(h);
+  if (S) omp_set_num_threads(S->threads);
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < n; ++i) {
+    double a = 0.0;
+    for (int p = ptr[i]; p < ptr[i + 1]; ++p) a += val[p] * x[col[p]];
+    y[i] = a;
+  }
+}
+
 void sncpu_release(void* h, int slot) {
   Solver* S = static_cast<Solver*>(h);
   if (S && slot >= 0 && slot <= 1) S->L[slot].reset();

@@ -53,6 +53,7 @@ def _load():
         L.sncpu_solve.restype = C.c_int
         L.sncpu_solve.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.sncpu_release.argtypes = [C.c_void_p, C.c_int]
+        L.sncpu_spmv.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -131,7 +132,11 @@ class SupernodalSlots:
         if not self.h:
             raise RuntimeError("sncpu_create failed")
         self.n = model.n
-        self.B = full_from_upper(model.B)
+        self.B = full_from_upper(model.B).tocsr()
+        self.B.sort_indices()
+        self._Bp = np.ascontiguousarray(self.B.indptr, dtype=np.int32)
+        self._Bi = np.ascontiguousarray(self.B.indices, dtype=np.int32)
+        self._Bv = np.ascontiguousarray(self.B.data, dtype=np.float64)
         self.slot_of: Dict[int, int] = {}
         self.n_factor = 0
         self.n_solve = 0
@@ -171,4 +176,9 @@ class SupernodalSlots:
             _load().sncpu_release(self.h, s)
 
     def spmv_B(self, x: np.ndarray) -> np.ndarray:
-        return self.B @ x
+        """M_sigma x on the host threads (mkl_sparse_d_mv runs threaded)."""
+        xv = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.n)
+        _load().sncpu_spmv(self.h, self.n, self._Bp.ctypes.data, self._Bi.ctypes.data, self._Bv.ctypes.data,
+                           xv.ctypes.data, y.ctypes.data)
+        return y
