@@ -165,7 +165,7 @@ int temf_locate_points(temf_ctx* ctx, int npts, const double* pts, double rec_ch
 /* ---- the time loop ----------------------------------------------------------
  * Runs time_solver/adap_euler (src/FETD_FWD.f90:1174-1464) on the GPU:
  * sp_division, sp_double, sp_dblesize and time_maximum as in the .cntl file.
- * flags: bit 0 = reproduce the build that wrote the shipped LINUX/*.field
+ * flags: bit 0 = reproduce the build that wrote the shipped LINUX .field
  * files (after an accepted dt-doubling trial it restarted BDF2 from
  * all_e(idx - sp_dblesize) instead of all_e(idx), src/FETD_FWD.f90:1405, and
  * advanced the time by one more old step); bit 1 = disable CUDA graphs.  forced (may be NULL): per trial 1 = accept, 0 = reject, -1 = the
