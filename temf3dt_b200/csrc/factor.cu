@@ -101,7 +101,6 @@ __global__ void __launch_bounds__(kFacThreads) k_trsm(const TrsmChunk* __restric
                                                       const int64_t* __restrict__ Lptr, double* __restrict__ L) {
   constexpr int CB = kSnCols;
   __shared__ double D[CB][CB + 1];
-  __shared__ double inv[CB];
   const TrsmChunk ch = chunks[blockIdx.x];
   const int s = ch.s;
   const int f = sn_first[s];
@@ -129,7 +128,6 @@ __global__ void __launch_bounds__(kFacThreads) k_trsm(const TrsmChunk* __restric
       x[j] = v / D[j][j];
     }
   }
-  (void)inv;
 #pragma unroll
   for (int j = 0; j < CB; ++j)
     if (j < c) P[(int64_t)j * ld + c + i] = x[j];
@@ -235,7 +233,6 @@ void build_factor_plan(temf_ctx& c) {
   const Symbolic& S = c.sym;
   FactorPlan& F = c.fplan;
   cudaStream_t st = c.stream;
-  const int nsn = S.nsn;
   F.sn_first.upload(S.sn_first.data(), S.sn_first.size(), st);
   F.sn_parent.upload(S.sn_parent.data(), S.sn_parent.size(), st);
   F.sn_rows.upload(S.sn_rows.data(), S.sn_rows.size(), st);
