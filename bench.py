@@ -126,21 +126,10 @@ def measured_dgemm_tflops(torch) -> float:
 
 
 def host_cores() -> int:
-    """Host threads the CPU arm may use: the cores this process may run on,
-    bounded by the container's CPU quota, at most 64 (the OpenBLAS build's
-    limit)."""
-    try:
-        n = len(os.sched_getaffinity(0))
-    except AttributeError:
-        n = os.cpu_count() or 1
-    try:
-        with open("/sys/fs/cgroup/cpu.max") as fh:
-            quota, period = fh.read().split()[:2]
-        if quota != "max":
-            n = min(n, max(1, int(float(quota) / float(period))))
-    except (OSError, ValueError):
-        pass
-    return max(1, min(n, 64))
+    """Host threads the CPU arm may use (the process's CPUs, bounded by the
+    container's CPU quota, at most 64)."""
+    from oracle.supernodal_cpu import host_threads
+    return host_threads()
 
 
 def cpu_arm(cfg: int, steps: int, warmup: int, sample_steps: int = 0, scaled: bool = False):

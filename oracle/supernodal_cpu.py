@@ -99,10 +99,20 @@ def blas_table():
 
 
 def host_threads() -> int:
+    """The cores this process may run on, bounded by the container's CPU
+    quota (cgroup cpu.max) and by 64, the OpenBLAS build's thread limit.
+    OpenMP barriers stall badly when threads outnumber the CPUs they get."""
     try:
         n = len(os.sched_getaffinity(0))
     except AttributeError:
         n = os.cpu_count() or 1
+    try:
+        with open("/sys/fs/cgroup/cpu.max") as fh:
+            quota, period = fh.read().split()[:2]
+        if quota != "max":
+            n = min(n, max(1, int(float(quota) / float(period))))
+    except (OSError, ValueError):
+        pass
     return max(1, min(n, 64))
 
 
