@@ -9,7 +9,9 @@
 #include <chrono>
 #include <climits>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <exception>
 #include <numeric>
 #include <stdexcept>
@@ -358,6 +360,14 @@ int host_threads(int requested) {
   int n = (int)std::max(1u, std::thread::hardware_concurrency());
   cpu_set_t set;
   if (sched_getaffinity(0, sizeof(set), &set) == 0) n = std::max(1, CPU_COUNT(&set));
+  // a container's CPU quota (cgroup v2 cpu.max: "quota period" or "max period")
+  if (FILE* f = std::fopen("/sys/fs/cgroup/cpu.max", "r")) {
+    char q[32] = {0};
+    long long period = 0;
+    if (std::fscanf(f, "%31s %lld", q, &period) == 2 && std::strcmp(q, "max") != 0 && period > 0)
+      n = std::min(n, std::max(1, (int)(std::atoll(q) / period)));
+    std::fclose(f);
+  }
   return std::min(n, 64);
 }
 

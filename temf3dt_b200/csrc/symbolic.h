@@ -82,7 +82,7 @@ struct UpdateGroups {
 void update_groups(const Symbolic& S, UpdateGroups& G, int threads = 0);
 
 // Host threads to use for a request (0: $TEMF_HOST_THREADS, else the cores
-// this process may run on, at most 64).
+// this process may run on, bounded by the cgroup CPU quota, at most 64).
 int host_threads(int requested);
 
 // Runs work(k) for k = 0 .. n-1: k >= 1 on new threads where one can be
