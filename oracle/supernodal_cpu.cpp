@@ -155,6 +155,14 @@ void build(Solver& S, const temf::Symbolic& Y) {
   S.level_sn.assign(ns, 0);
   std::vector<int> fill(S.level_ptr.begin(), S.level_ptr.end() - 1);
   for (int k = 0; k < ns; ++k) S.level_sn[fill[level[k]]++] = k;
+  // largest first inside a level, so the dynamic schedule ends on small ones
+  auto work = [&](int k) {
+    const double c = S.sn[k].c, r = (double)S.sn[k].r;
+    return c * c * c / 3.0 + c * c * r + c * r * r;
+  };
+  for (int l = 0; l < nlev; ++l)
+    std::stable_sort(S.level_sn.begin() + S.level_ptr[l], S.level_sn.begin() + S.level_ptr[l + 1],
+                     [&](int a, int b) { return work(a) > work(b); });
 }
 
 // panel offset of the lower-triangle entry (row a, column b) of the permuted matrix, a >= b
