@@ -351,6 +351,20 @@ int temf_case_media(const temf_case* cs, double* sig, double* mu, int* aniso);
  * output_mask[9] (non-zero = written).  Fortran E15.5 numbers. */
 int temf_case_write_rows(const char* path, int rows, int nrec, const int* steps, const double* times,
                          const double* fields, const int* output_mask);
+/* Whole-mesh field dumps (vtkout, src/FETD_FWD.f90:1642-1864), host parts.
+ * temf_case_vtk_times: the vtkout times of the cntl (*n of them; times may
+ * be NULL).  temf_mesh_fields_host: vtk_field_save's E and D of an edge
+ * vector e(n_edges) at every tet's centroid, fields(tets, 6) row-major =
+ * Ex Ey Ez Dx Dy Dz (mesh arrays in the Fortran layouts of temf_set_mesh).
+ * temf_case_write_msh: msh_output -- a copy of the Gmsh 4.1 file src_msh
+ * with one $ElementData block (absolute values, i10 e16.8) per output column
+ * selected in the cntl, from fields(tets, 9) row-major = E, D, B; the tets
+ * are matched to the file's tetrahedron elements in order. */
+int temf_case_vtk_times(const temf_case* cs, int* n, double* times);
+int temf_mesh_fields_host(int n_nodes, const double* nod_cor, int n_tets, const int* tet_vex, const int* tet_edg,
+                          const int* tet_drc, int n_edges, const double* e, double* fields);
+int temf_case_write_msh(const temf_case* cs, const char* src_msh, const char* dst_msh, const double* fields, char* msg,
+                        int msg_len);
 /* mesh_process and the source/receiver set-up on a fresh context: edge
  * topology, mesh, media, boundary, analysis, assembly, src_edg/src_drc (+1,
  * last -1, src/FETD_FWD.f90:435-448), receiver location and operators. */

@@ -139,6 +139,7 @@ class Control:
     o_f: np.ndarray = field(default_factory=lambda: np.zeros(9, dtype=bool))
     time_channels: Optional[np.ndarray] = None
     vtk_num: int = 0
+    vtk_times: Optional[np.ndarray] = None
     # anisotropic media (src/FETD_FWD.f90:368-410): per domain three principal
     # values and three rotation angles (radians) of sigma, eps_r and mu_r
     aniso: bool = False
@@ -215,6 +216,8 @@ def read_cntl(path: str) -> Control:
             c.o_f = np.array([int(x) == 1 for x in t[:9]])
         elif code == "vtkout":
             c.vtk_num = int(val.split()[0])
+            if c.vtk_num > 0:
+                c.vtk_times = np.array([_f(lines[i + q].split()[0]) for q in range(c.vtk_num)])
             i += max(c.vtk_num, 0)
     # src/FETD_FWD.f90:490-497
     if c.rec_cor is None or len(c.rec_cor) == 0:
@@ -491,6 +494,104 @@ def receiver_operators(a, b, c, d, vol, tet_len, rec_tet, rec_cor):
     return n_arr, d_arr
 
 
+def mesh_field_operators(nod_cor, tet_vex, a, b, c, d, vol, tet_len):
+    """n_arr_global / d_arr_global of vtk_field_save (src/FETD_FWD.f90:1670-1695):
+    the E and D operators of the six edge functions at every tet's centroid,
+    (T, 6, 3) each.  D carries +2 here (the receivers' d_arr carries -2)."""
+    X = nod_cor[tet_vex - 1]
+    cp = (X[:, 0] + X[:, 1] + X[:, 2] + X[:, 3]) / 4.0
+    lam = a + b * cp[:, 0:1] + c * cp[:, 1:2] + d * cp[:, 2:3]
+    s = tet_len / (6.0 * vol[:, None]) ** 2
+    T = X.shape[0]
+    N = np.empty((T, 6, 3))
+    D = np.empty((T, 6, 3))
+    for j in range(6):
+        p, q = IND_TET[j]
+        N[:, j, 0] = lam[:, p] * b[:, q] - lam[:, q] * b[:, p]
+        N[:, j, 1] = lam[:, p] * c[:, q] - lam[:, q] * c[:, p]
+        N[:, j, 2] = lam[:, p] * d[:, q] - lam[:, q] * d[:, p]
+        N[:, j] *= s[:, j:j + 1]
+        D[:, j, 0] = c[:, p] * d[:, q] - c[:, q] * d[:, p]
+        D[:, j, 1] = b[:, q] * d[:, p] - b[:, p] * d[:, q]
+        D[:, j, 2] = b[:, p] * c[:, q] - b[:, q] * c[:, p]
+        D[:, j] *= 2.0 * s[:, j:j + 1]
+    return N, D
+
+
+class MeshFields:
+    """vtk_field_save (src/FETD_FWD.f90:1659-1711): at every output row, E and
+    D of the solution at the tet centroids; B accumulates D * dt over the
+    rows, from the first one."""
+
+    def __init__(self, model: "OracleModel"):
+        a, b, c, d, vol, tet_len = geometry(model.nod_cor, model.tet_vex)
+        self.N, self.D = mesh_field_operators(model.nod_cor, model.tet_vex, a, b, c, d, vol, tet_len)
+        self.tet_edg, self.tet_drc = model.tet_edg, model.tet_drc
+        T = model.tet_vex.shape[0]
+        self.e = np.zeros((T, 3))
+        self.d = np.zeros((T, 3))
+        self.b = np.zeros((T, 3))
+
+    def __call__(self, step_cur: float, res_e: np.ndarray) -> None:
+        ev = self.tet_drc * res_e[self.tet_edg - 1]
+        self.e = np.zeros_like(self.e)
+        self.d = np.zeros_like(self.d)
+        for j in range(6):
+            self.e += self.N[:, j] * ev[:, j:j + 1]
+            self.d += self.D[:, j] * ev[:, j:j + 1]
+        self.b = self.b + self.d * step_cur
+
+
+def _fortran_e(v: float, w: int, dd: int) -> str:
+    """Fortran Ew.d: [-]0.ddd E+ee right-justified in w columns."""
+    v = float(v)
+    if v == 0.0:
+        return ("0." + "0" * dd + "E+00").rjust(w)
+    m, ex = ("%.*E" % (dd - 1, abs(v))).split("E")
+    e = int(ex) + 1
+    tail = ("E%+03d" % e) if abs(e) < 100 else ("%+04d" % e)
+    return (("-" if v < 0 else "") + "0." + m.replace(".", "") + tail).rjust(w)
+
+
+def msh_tet_tags(path: str) -> List[int]:
+    """The tetrahedron (type 4) element tags of a Gmsh 4.1 file in file order,
+    as msh_output collects them (src/FETD_FWD.f90:1745-1789)."""
+    with open(path) as fh:
+        lines = fh.read().splitlines()
+    i = next(k for k, ln in enumerate(lines) if ln.startswith("$Elements")) + 1
+    nblk = int(lines[i].split()[0])
+    i += 1
+    tags = []
+    for _ in range(nblk):
+        _dim, _ent, etype, cnt = (int(t) for t in lines[i].split()[:4])
+        i += 1
+        if etype == 4:
+            tags += [int(lines[i + q].split()[0]) for q in range(cnt)]
+        i += cnt
+    return tags
+
+
+MSH_NAMES = ["Ex", "Ey", "Ez", "Dx", "Dy", "Dz", "Bx", "By", "Bz"]
+
+
+def write_msh_fields(src: str, dst: str, fields: np.ndarray, o_f) -> None:
+    """msh_output (src/FETD_FWD.f90:1713-1864): a copy of the model's .msh with
+    one $ElementData block per selected column of fields (T, 9) = E, D, B,
+    absolute values, format (i10, e16.8)."""
+    tags = msh_tet_tags(src)
+    with open(src) as fh:
+        text = fh.read()
+    out = [text if text.endswith("\n") else text + "\n"]
+    for k in range(9):
+        if not o_f[k]:
+            continue
+        out.append('$ElementData\n1\n"%s data"\n1\n0.0\n3\n0\n1\n%12d\n' % (MSH_NAMES[k], len(tags)))
+        out += ["%10d%s\n" % (tags[t], _fortran_e(abs(fields[t, k]), 16, 8)) for t in range(len(tags))]
+        out.append("$EndElementData\n")
+    with open(dst, "w") as fh:
+        fh.write("".join(out))
+
+
 def p_in_tet(nod_cor, tet_vex, p, rec_charac: float) -> int:
     """Receiver point location, src/FETD_FWD.f90:1009-1049 (1-based tet, 0 = none)."""
     X = nod_cor[tet_vex - 1]
@@ -711,6 +812,7 @@ class FetdResult:
     trial_errors: List[float]
     trial_accepted: List[bool]
     final_e: Optional[np.ndarray] = None
+    mesh_fields: Dict[int, np.ndarray] = field(default_factory=dict)   # vtk index -> (T, 9) E D B
 
 
 class _Output:
@@ -726,6 +828,11 @@ class _Output:
         self.chan_t = chan if chan is not None else np.zeros(0)
         self.chan_ok = np.zeros(len(self.chan_t), dtype=bool)
         self.chan_val: Dict[int, np.ndarray] = {}
+        vt = model.ctl.vtk_times
+        self.vtk_t = np.asarray(vt) if vt is not None else np.zeros(0)
+        self.vtk_done = np.zeros(len(self.vtk_t), dtype=bool)
+        self.mesh = MeshFields(model) if len(self.vtk_t) else None
+        self.mesh_fields: Dict[int, np.ndarray] = {}
 
     def __call__(self, step: int, t: float, step_cur: float, e: np.ndarray) -> None:
         m = self.m
@@ -752,6 +859,13 @@ class _Output:
                     break                      # the reference exits the channel loop here
                 self.chan_val[i] = interp_lin(self.times[-2], self.rows[-2], t, row, self.chan_t[i])
                 self.chan_ok[i] = True
+        # whole-mesh fields (src/FETD_FWD.f90:1642-1656)
+        if self.mesh is not None and not self.vtk_done.all():
+            self.mesh(step_cur, e)
+            for i in range(len(self.vtk_t)):
+                if not self.vtk_done[i] and t >= self.vtk_t[i]:
+                    self.mesh_fields[i] = np.concatenate([self.mesh.e, self.mesh.d, self.mesh.b], axis=1)
+                    self.vtk_done[i] = True
 
 
 def adap_euler(model: OracleModel, slots: SuperLUSlots, out: Optional[_Output],
@@ -879,7 +993,8 @@ def run_fetd(model: OracleModel, max_steps: Optional[int] = None, time_maximum: 
     else:
         e_last, errs, acc = adap_euler(model, slots, out, max_steps=max_steps, time_maximum=time_maximum,
                                        legacy_linux=legacy_linux)
-    return FetdResult(out.steps, out.times, out.dts, np.array(out.rows), out.chan_val, errs, acc, e_last)
+    return FetdResult(out.steps, out.times, out.dts, np.array(out.rows), out.chan_val, errs, acc, e_last,
+                      out.mesh_fields)
 
 
 def read_field(path: str) -> np.ndarray:

@@ -9,12 +9,14 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <iterator>
 #include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "../../include/temf_b200.h"
+#include "element.cuh"
 
 namespace {
 
@@ -45,6 +47,7 @@ struct Case {
   bool output[9] = {false, false, false, false, false, false, false, false, false};
   std::vector<double> time_points;
   bool have_time_points = false;
+  std::vector<double> vtk_times;  // whole-mesh field dumps (vtkout)
   // set by load
   std::vector<int> edg_vex;  // (edges, 2) column-major, 1-based
   int n_edges = 0;
@@ -247,6 +250,7 @@ void read_cntl(const std::string& path, Case& c) {
       i += n;
     } else if (k == "vtkout") {
       c.vtkout = inum(first(v));
+      for (int q = 0; q < c.vtkout; ++q) c.vtk_times.push_back(num(line(i + q).at(0)));
       i += std::max(c.vtkout, 0);
     }
   }
@@ -451,6 +455,59 @@ void write_outputs(const Case& c, temf_ctx* ctx, const std::string& root) {
   write_rows(root + ".field2", (int)idx.size(), R, idx.data(), t2.data(), f2.data(), mask);
 }
 
+// msh_output (src/FETD_FWD.f90:1713-1864): the tetrahedron (type 4) element
+// tags of a Gmsh 4.1 file in file order ...
+std::vector<long long> msh_tet_tags(const std::string& path) {
+  const std::vector<std::string> L = read_lines(path);
+  size_t i = 0;
+  while (i < L.size() && L[i].compare(0, 9, "$Elements") != 0) ++i;
+  if (i == L.size()) fail(path + ": no $Elements section");
+  ++i;
+  auto fields = [&](size_t k) -> std::vector<std::string> {
+    if (k >= L.size()) fail(path + ": $Elements is truncated");
+    return split(L[k]);
+  };
+  const int nblk = inum(fields(i).at(0));
+  ++i;
+  std::vector<long long> tags;
+  for (int b = 0; b < nblk; ++b) {
+    const std::vector<std::string> h = fields(i);
+    if (h.size() < 4) fail(path + ": short element block header");
+    const int type = inum(h[2]), cnt = inum(h[3]);
+    ++i;
+    if (type == 4)
+      for (int q = 0; q < cnt; ++q) tags.push_back(std::atoll(fields(i + q).at(0).c_str()));
+    i += cnt;
+  }
+  return tags;
+}
+
+// ... then a copy of the file with one $ElementData block per selected column
+// of fields (tets x 9: E, D, B), absolute values, format (i10, e16.8)
+void write_msh(const Case& c, const std::string& src, const std::string& dst, const double* fields) {
+  static const char* names[9] = {"Ex", "Ey", "Ez", "Dx", "Dy", "Dz", "Bx", "By", "Bz"};
+  const std::vector<long long> tags = msh_tet_tags(src);
+  if (tags.size() != c.tet_phy.size())
+    fail(src + ": " + std::to_string(tags.size()) + " tetrahedra, the mesh has " + std::to_string(c.tet_phy.size()));
+  std::ifstream in(src, std::ios::binary);
+  std::string text((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+  if (!text.empty() && text.back() != '\n') text += '\n';
+  FILE* f = std::fopen(dst.c_str(), "w");
+  if (!f) fail("cannot write " + dst);
+  std::fputs(text.c_str(), f);
+  char buf[64];
+  for (int k = 0; k < 9; ++k) {
+    if (!c.output[k]) continue;
+    std::fprintf(f, "$ElementData\n1\n\"%s data\"\n1\n0.0\n3\n0\n1\n%12d\n", names[k], (int)tags.size());
+    for (size_t t = 0; t < tags.size(); ++t) {
+      std::snprintf(buf, sizeof buf, "%10lld", tags[t]);
+      std::fputs((std::string(buf) + fortran_e(std::fabs(fields[9 * t + k]), 16, 8) + "\n").c_str(), f);
+    }
+    std::fputs("$EndElementData\n", f);
+  }
+  if (std::fclose(f) != 0) fail("writing " + dst + " failed");
+}
+
 void copy_msg(const std::string& s, char* msg, int len) {
   if (msg && len > 0) {
     std::strncpy(msg, s.c_str(), len - 1);
@@ -560,6 +617,49 @@ int temf_case_write_rows(const char* path, int rows, int nrec, const int* steps,
   } catch (const std::exception&) {
     return TEMF_EINTERNAL;
   }
+}
+
+int temf_case_vtk_times(const temf_case* c, int* n, double* times) {
+  if (!c || !n) return TEMF_EARG;
+  *n = (int)c->vtk_times.size();
+  if (times) std::copy(c->vtk_times.begin(), c->vtk_times.end(), times);
+  return TEMF_OK;
+}
+
+int temf_case_write_msh(const temf_case* c, const char* src_msh, const char* dst_msh, const double* fields, char* msg,
+                        int msg_len) {
+  if (!c || !src_msh || !dst_msh || !fields) return TEMF_EARG;
+  try {
+    write_msh(*c, src_msh, dst_msh, fields);
+    copy_msg("", msg, msg_len);
+    return TEMF_OK;
+  } catch (const std::exception& e) {
+    copy_msg(e.what(), msg, msg_len);
+    return TEMF_EARG;
+  }
+}
+
+int temf_mesh_fields_host(int n_nodes, const double* nod_cor, int n_tets, const int* tet_vex, const int* tet_edg,
+                          const int* tet_drc, int n_edges, const double* e, double* fields) {
+  if (n_nodes <= 0 || n_tets <= 0 || n_edges <= 0 || !nod_cor || !tet_vex || !tet_edg || !tet_drc || !e || !fields)
+    return TEMF_EARG;
+  for (int64_t q = 0; q < 4LL * n_tets; ++q)
+    if (tet_vex[q] < 1 || tet_vex[q] > n_nodes) return TEMF_EARG;
+  for (int64_t q = 0; q < 6LL * n_tets; ++q)
+    if (tet_edg[q] < 1 || tet_edg[q] > n_edges) return TEMF_EARG;
+  for (int t = 0; t < n_tets; ++t) {
+    double X[4][3], ev[6], E[3], D[3];
+    for (int k = 0; k < 4; ++k)
+      for (int a = 0; a < 3; ++a) X[k][a] = nod_cor[(int64_t)a * n_nodes + tet_vex[(int64_t)k * n_tets + t] - 1];
+    for (int j = 0; j < 6; ++j)
+      ev[j] = tet_drc[(int64_t)j * n_tets + t] * e[tet_edg[(int64_t)j * n_tets + t] - 1];
+    temf::centroid_fields(X, ev, E, D);
+    for (int a = 0; a < 3; ++a) {
+      fields[6LL * t + a] = E[a];
+      fields[6LL * t + 3 + a] = D[a];
+    }
+  }
+  return TEMF_OK;
 }
 
 int temf_case_load(temf_case* c, temf_ctx* ctx, char* msg, int msg_len) {

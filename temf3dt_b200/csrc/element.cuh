@@ -17,7 +17,7 @@ __host__ __device__ inline int packed_upper(int i, int j) {  // i <= j < 6
 
 // local edge j joins local vertices ind_tet(j,0) -> ind_tet(j,1):
 // (0,1) (0,2) (0,3) (1,2) (3,1) (2,3)
-__device__ __forceinline__ int ind_tet(int j, int k) {
+__host__ __device__ __forceinline__ int ind_tet(int j, int k) {
   return (k == 0) ? (j == 4 ? 3 : (j < 3 ? 0 : (j == 3 ? 1 : 2)))
                   : (j == 0 ? 1 : (j == 1 ? 2 : (j == 2 ? 3 : (j == 3 ? 2 : (j == 4 ? 1 : 3)))));
 }
@@ -25,7 +25,7 @@ __device__ __forceinline__ int ind_tet(int j, int k) {
 // Gradients g_k = (b_k, c_k, d_k) and V, written as differences from the first
 // vertex (the cofactor expansion of the reference's 3x3 determinants after
 // subtracting one row from the others; same values up to rounding).
-__device__ inline void tet_gradients(const double X[4][3], double g[4][3], double& vol) {
+__host__ __device__ inline void tet_gradients(const double X[4][3], double g[4][3], double& vol) {
   // D(u,w; p,q,r) = det [[1,u_p,w_p],[1,u_q,w_q],[1,u_r,w_r]]
   auto D = [&](int u, int w, int p, int q, int r) {
     return (X[q][u] - X[p][u]) * (X[r][w] - X[p][w]) - (X[r][u] - X[p][u]) * (X[q][w] - X[p][w]);
@@ -43,6 +43,28 @@ __device__ inline void tet_gradients(const double X[4][3], double g[4][3], doubl
   const double bx = X[2][0] - X[0][0], by = X[2][1] - X[0][1], bz = X[2][2] - X[0][2];
   const double cx = X[3][0] - X[0][0], cy = X[3][1] - X[0][1], cz = X[3][2] - X[0][2];
   vol = (ax * (by * cz - bz * cy) - ay * (bx * cz - bz * cx) + az * (bx * cy - by * cx)) / 6.0;
+}
+
+// vtk_field_save (src/FETD_FWD.f90:1670-1711) for one tet: E and D of the
+// edge values ev[j] (orientation signs applied) at the centroid, where every
+// barycentric coordinate is 1/4:
+//   E = sum_j ev_j l_j (lam_p g_q - lam_q g_p) / (6V)^2 with lam = 6V / 4,
+//   D = sum_j ev_j 2 l_j (g_p x g_q) / (6V)^2.
+__host__ __device__ inline void centroid_fields(const double X[4][3], const double ev[6], double E[3], double D[3]) {
+  double g[4][3], vol;
+  tet_gradients(X, g, vol);
+  const double v6 = 6.0 * vol;
+  const double inv2 = 1.0 / (v6 * v6), lam = 0.25 * v6;
+  for (int k = 0; k < 3; ++k) E[k] = D[k] = 0.0;
+  for (int j = 0; j < 6; ++j) {
+    const int p = ind_tet(j, 0), q = ind_tet(j, 1);
+    const double dx = X[p][0] - X[q][0], dy = X[p][1] - X[q][1], dz = X[p][2] - X[q][2];
+    const double s = sqrt(dx * dx + dy * dy + dz * dz) * inv2 * ev[j];
+    for (int k = 0; k < 3; ++k) E[k] += s * (lam * g[q][k] - lam * g[p][k]);
+    D[0] += 2.0 * s * (g[p][1] * g[q][2] - g[q][1] * g[p][2]);
+    D[1] += 2.0 * s * (g[q][0] * g[p][2] - g[p][0] * g[q][2]);
+    D[2] += 2.0 * s * (g[p][0] * g[q][1] - g[q][0] * g[p][1]);
+  }
 }
 
 // Unit-material mass (M21) and curl-curl (K21) element matrices; either

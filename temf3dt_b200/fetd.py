@@ -498,6 +498,11 @@ class CaseFile:
         self.rec_cor = rc_[:3 * R].reshape(3, R).T.copy()
         self.time_points = tpts[:ntp].copy() if ntp >= 0 else None
         self.n_iso, self.n_aniso = int(sz[4]), int(sz[5])
+        nv = C.c_int(0)
+        L.temf_case_vtk_times(h, C.byref(nv), None)
+        vt = np.zeros(max(nv.value, 1))
+        L.temf_case_vtk_times(h, C.byref(nv), dptr(vt))
+        self.vtk_times = vt[:nv.value].copy()
 
     def close(self) -> None:
         if self._h:
@@ -535,10 +540,34 @@ class CaseFile:
         gpu._ck(self._L.temf_analysis_stats(gpu._h, dptr(s)), "temf_analysis_stats")
         return int(s[0])
 
+    def write_msh(self, src_msh: str, dst_msh: str, fields: np.ndarray) -> None:
+        """msh_output: a copy of src_msh with $ElementData blocks of the
+        selected output columns of fields (n_tets, 9) = E, D, B."""
+        f = as_f64(np.asarray(fields, dtype=np.float64).reshape(-1, 9))
+        msg = C.create_string_buffer(512)
+        if self._L.temf_case_write_msh(self._h, src_msh.encode(), dst_msh.encode(), dptr(f), msg, 512) != 0:
+            raise ValueError(msg.value.decode())
+
     def write(self, gpu: "FetdGPU", root: str) -> None:
         msg = C.create_string_buffer(512)
         if self._L.temf_case_write(self._h, gpu._h, root.encode(), msg, 512) != 0:
             raise RuntimeError(msg.value.decode())
+
+
+def mesh_fields_host(nod_cor, tet_vex, tet_edg, tet_drc, e) -> np.ndarray:
+    """vtk_field_save's E and D of the edge vector e at every tet centroid,
+    (n_tets, 6) = Ex Ey Ez Dx Dy Dz (the library's host evaluation of the
+    per-tet formula its GPU kernels share)."""
+    nod = fortran_f64(nod_cor)
+    tv, te, td = fortran_i32(tet_vex), fortran_i32(tet_edg), fortran_i32(tet_drc)
+    ev = as_f64(e)
+    T = int(np.asarray(tet_vex).shape[0])
+    out = np.zeros(6 * T)
+    rc = lib().temf_mesh_fields_host(int(np.asarray(nod_cor).shape[0]), dptr(nod), T, iptr(tv), iptr(te), iptr(td),
+                                     len(ev), dptr(ev), dptr(out))
+    if rc != 0:
+        raise TemfError(rc, "temf_mesh_fields_host")
+    return out.reshape(T, 6)
 
 
 def run_case_native(root: str, device: int = 0, legacy_linux: bool = False) -> None:

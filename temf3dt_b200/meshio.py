@@ -95,6 +95,7 @@ class Control:
     output: np.ndarray = field(default_factory=lambda: np.zeros(9, dtype=bool))
     time_points: Optional[np.ndarray] = None
     vtkout: int = 0
+    vtk_times: Optional[np.ndarray] = None
     # anisotropic media (src/FETD_FWD.f90:368-410): per domain
     # (phys, (s1, s2, s3), (a1, a2, a3) degrees) for sigma, eps_r and mu_r
     aniso_domains: List[tuple] = field(default_factory=list)
@@ -166,7 +167,10 @@ def read_cntl(path: str) -> Control:
         elif k == "time_points":
             n = int(v.split()[0]); c.time_points = np.array([_num(L[i + q].split()[0]) for q in range(n)]); i += n
         elif k == "vtkout":
-            c.vtkout = int(v.split()[0]); i += max(c.vtkout, 0)
+            c.vtkout = int(v.split()[0])
+            if c.vtkout > 0:
+                c.vtk_times = np.array([_num(L[i + q].split()[0]) for q in range(c.vtkout)])
+            i += max(c.vtkout, 0)
     if c.rec_cor is None or not len(c.rec_cor) or not (c.domains or c.aniso_domains) or not c.src_num \
             or not c.sp_mthd \
             or not c.sp_division or abs(c.time_maximum) < 1e-20 or not c.sp_double or not c.output.any():
@@ -200,7 +204,12 @@ def write_cntl(path: str, c: Control) -> None:
             fh.write("\ntime_points: %d\n" % len(c.time_points))
             for t in c.time_points:
                 fh.write("%.10g\n" % t)
-        fh.write("\nvtkout: 0\n")
+        if c.vtk_times is not None and len(c.vtk_times):
+            fh.write("\nvtkout: %d\n" % len(c.vtk_times))
+            for t in c.vtk_times:
+                fh.write("%.10g\n" % t)
+        else:
+            fh.write("\nvtkout: 0\n")
 
 
 def rotation(ang_deg) -> np.ndarray:
