@@ -173,6 +173,15 @@ int temf_locate_points(temf_ctx* ctx, int npts, const double* pts, double rec_ch
  * limit.  Results are kept in the context; see temf_result_*. */
 int temf_run(temf_ctx* ctx, int sp_division, int sp_double, int sp_dblesize, double time_maximum, int flags,
              const int* forced, int n_forced, int max_steps);
+/* Whole-mesh field dumps (vtkout, src/FETD_FWD.f90:1642-1864): the following
+ * temf_run evaluates E and D at every tet's centroid at every output row,
+ * accumulates B = sum D dt, and keeps E, D, B of the first row at or after
+ * each of the n_times times (at most 30; 0 turns the dumps off).  One RHS
+ * column; not in batches.  temf_result_mesh_fields: snapshot `index` of the
+ * last run as fields(tets, 9) row-major = Ex Ey Ez Dx Dy Dz Bx By Bz, and
+ * whether the run reached it (*done). */
+int temf_set_mesh_fields(temf_ctx* ctx, int n_times, const double* times);
+int temf_result_mesh_fields(temf_ctx* ctx, int index, double* fields, int* done);
 /* Number of output rows of the last run (the rows of the .field file). */
 int temf_result_rows(temf_ctx* ctx, int* rows);
 /* Output rows: step(rows), time(rows), dt(rows) and fields(9, nrec, rows)
@@ -373,7 +382,8 @@ int temf_case_load(temf_case* cs, temf_ctx* ctx, char* msg, int msg_len);
  * rows the run reached, numbered from 1) when the cntl has time_points. */
 int temf_case_write(const temf_case* cs, temf_ctx* ctx, const char* root, char* msg, int msg_len);
 /* `./FETD -f ROOT` on GPU `device`: read, load, temf_run (flags as there),
- * write ROOT.field(2). */
+ * write ROOT.field(2); with vtkout times in the cntl and ROOT.msh present,
+ * also ROOT_i.msh for each time the run reached (msh_output). */
 int temf_case_run(const char* root, int device, int flags, char* msg, int msg_len);
 
 #ifdef __cplusplus

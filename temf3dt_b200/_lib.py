@@ -76,6 +76,8 @@ SIGNATURES = {
     "temf_case_media": (_i, [_p, _dp, _dp, _ip]),
     "temf_case_write_rows": (_i, [C.c_char_p, _i, _i, _ip, _dp, _dp, _ip]),
     "temf_case_vtk_times": (_i, [_p, _ip, _dp]),
+    "temf_set_mesh_fields": (_i, [_p, _i, _dp]),
+    "temf_result_mesh_fields": (_i, [_p, _i, _dp, _ip]),
     "temf_mesh_fields_host": (_i, [_i, _dp, _i, _ip, _ip, _ip, _i, _dp, _dp]),
     "temf_case_write_msh": (_i, [_p, C.c_char_p, C.c_char_p, _dp, C.c_char_p, _i]),
     "temf_case_load": (_i, [_p, _p, C.c_char_p, _i]),

@@ -539,6 +539,12 @@ int temf_analyse(temf_ctx* c) {
       for (int a = 0; a < 3; ++a)
         mid[3LL * e + a] = 0.5 * (c->xyz[3LL * c->edg_vex[2LL * e] + a] + c->xyz[3LL * c->edg_vex[2LL * e + 1] + a]);
     c->sym_opt.max_sn_cols = kSnCols;
+    // a new ordering invalidates the mesh-field plan's permuted edges
+    c->mf.times.clear();
+    c->mf.done.clear();
+    c->mf.edges.reset();
+    c->mf.b.reset();
+    c->mf.snap.reset();
     analyse(c->n_edges, x2.data(), a2.data(), mid.data(), c->sym_opt, c->sym);
     build_pattern(*c, c->sym.perm, c->sym.iperm, c->pat);
     upload_pattern(*c);
@@ -802,6 +808,44 @@ int temf_locate_points(temf_ctx* c, int npts, const double* pts, double rec_char
   });
 }
 
+int temf_set_mesh_fields(temf_ctx* c, int n_times, const double* times) {
+  return guarded(c, [&] {
+    need(c->analysed, "temf_set_mesh_fields: call temf_analyse first");
+    if (n_times < 0 || n_times > 30 || (n_times > 0 && !times)) throw ArgError("0 to 30 vtkout times expected");
+    temf::MeshFieldPlan& M = c->mf;
+    M.times.assign(times, times + n_times);
+    M.done.assign(n_times, 0);
+    if (n_times == 0) {
+      M.edges.reset();
+      M.b.reset();
+      M.snap.reset();
+      return TEMF_OK;
+    }
+    const int T = c->n_tets;
+    std::vector<int> e(6LL * T);
+    for (int64_t q = 0; q < 6LL * T; ++q) e[q] = c->sym.iperm[c->tet_edg[q]];
+    M.edges.upload(e.data(), e.size(), c->stream);
+    M.b.alloc(3LL * T);
+    M.snap.alloc(9LL * T * n_times);
+    TEMF_CUDA(cudaMemsetAsync(M.snap.p, 0, M.snap.bytes(), c->stream));
+    TEMF_CUDA(cudaStreamSynchronize(c->stream));
+    return TEMF_OK;
+  });
+}
+
+int temf_result_mesh_fields(temf_ctx* c, int index, double* fields, int* done) {
+  return guarded(c, [&] {
+    const temf::MeshFieldPlan& M = c->mf;
+    if (index < 0 || index >= M.n()) throw ArgError("no such vtkout time");
+    if (done) *done = M.done.size() > (size_t)index ? M.done[index] : 0;
+    if (fields) {
+      const size_t cnt = 9ULL * c->n_tets;
+      TEMF_CUDA(cudaMemcpy(fields, M.snap.p + cnt * index, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    return TEMF_OK;
+  });
+}
+
 int temf_run(temf_ctx* c, int sp_division, int sp_double, int sp_dblesize, double time_maximum, int flags,
              const int* forced, int n_forced, int max_steps) {
   return guarded(c, [&] {
@@ -980,6 +1024,7 @@ int temf_batch_run(temf_batch* B, int sp_division, int sp_double, int sp_dblesiz
       need(c->src.nrhs >= 1, "temf_batch_run: set every model's source first");
       for (int r = 0; r < c->rec.nrec; ++r)
         if (c->rec.rec_rhs[r] >= c->src.nrhs) throw ArgError("a receiver samples a RHS column that does not exist");
+      if (c->mf.n() > 0) throw ArgError("whole-mesh field dumps are written by temf_run, not by a batch");
       extra(c).run.valid = false;
       c->adj.valid = false;
     }

@@ -695,9 +695,22 @@ int temf_case_run(const char* root, int device, int flags, char* msg, int msg_le
   try {
     check(temf_create(device, &ctx), nullptr, "temf_create");
     load(*c, ctx);
+    // whole-mesh dumps need the model's Gmsh file next to it (msh_output copies ROOT.msh)
+    const std::string msh = std::string(root) + ".msh";
+    const bool dumps = !c->vtk_times.empty() && std::ifstream(msh).good();
+    if (dumps)
+      check(temf_set_mesh_fields(ctx, (int)c->vtk_times.size(), c->vtk_times.data()), ctx, "temf_set_mesh_fields");
     check(temf_run(ctx, c->sp_division, c->sp_double, c->sp_dblesize, c->time_maximum, flags, nullptr, 0, 0), ctx,
           "temf_run");
     write_outputs(*c, ctx, root);
+    if (dumps) {
+      std::vector<double> f(9 * c->tet_phy.size());
+      for (int i = 0; i < (int)c->vtk_times.size(); ++i) {
+        int done = 0;
+        check(temf_result_mesh_fields(ctx, i, f.data(), &done), ctx, "temf_result_mesh_fields");
+        if (done) write_msh(*c, msh, std::string(root) + "_" + std::to_string(i + 1) + ".msh", f.data());
+      }
+    }
     copy_msg("", msg, msg_len);
     rc = TEMF_OK;
   } catch (const std::exception& e) {

@@ -148,6 +148,20 @@ struct AdjointRecord {
   std::vector<std::unique_ptr<DBuf<double>>> ck;  // W states: nodes ck_first-W .. ck_first-1
 };
 
+// Whole-mesh field dumps of the next temf_run (vtkout, src/FETD_FWD.f90:1642-1864):
+// at every output row E and D at the tet centroids, B accumulated as D * dt,
+// and a snapshot of E, D, B at the first row at or after each time.
+struct MeshFieldPlan {
+  std::vector<double> times;  // vtkout times (at most 30)
+  std::vector<int> done;      // per time: its snapshot was taken in the last run
+  DBuf<int> edges;            // per tet its 6 edges in the permuted order
+  DBuf<double> b;             // tets x 3
+  DBuf<double> snap;          // times x tets x 9 (E, D, B)
+  DBuf<int> trig;             // per trace row: bit i = the row takes snapshot i
+  DBuf<double> dt;            // [0]: the rows' dt
+  int n() const { return (int)times.size(); }
+};
+
 }  // namespace temf
 
 struct temf_ctx {
@@ -191,5 +205,6 @@ struct temf_ctx {
   // scratch vectors
   temf::DBuf<double> d_part;     // backward partial sums (part_len), or block accumulators (macc_len * 64)
   temf::AdjointRecord adj;
+  temf::MeshFieldPlan mf;
   int u_nrhs = 0;
 };

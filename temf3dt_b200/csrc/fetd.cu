@@ -14,6 +14,7 @@
 #include <cmath>
 #include <map>
 
+#include "element.cuh"
 #include "factor.h"
 #include "fetd.h"
 #include "solve.h"
@@ -60,6 +61,43 @@ void launch_receivers_row(temf_ctx& c, const double* x, int nrhs, const int* row
   TEMF_CHECK_LAUNCH();
 }
 
+// vtk_field_save (src/FETD_FWD.f90:1659-1711) for one output row: E and D of
+// x (permuted order, one column) at every tet centroid and B += D dt; a row
+// whose trigger bits are set (trig[row_base + k]) copies E, D, B into those
+// snapshots (msh_output's data, :1790-1860).
+__global__ void k_mesh_fields(int T, const double* __restrict__ xyz, const int* __restrict__ tet_vex,
+                              const int* __restrict__ edges, const int* __restrict__ drc,
+                              const double* __restrict__ x, const double* __restrict__ dt,
+                              const int* __restrict__ trig, const int* __restrict__ row_base, int k,
+                              double* __restrict__ b, double* __restrict__ snap, int nsnap) {
+  const int mask = trig[row_base[0] + k];
+  const double h = dt[0];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+    double X[4][3], ev[6], E[3], D[3];
+    for (int v = 0; v < 4; ++v) {
+      const int node = tet_vex[4 * (int64_t)t + v];
+      for (int a = 0; a < 3; ++a) X[v][a] = xyz[3 * (int64_t)node + a];
+    }
+    for (int j = 0; j < 6; ++j) ev[j] = drc[6 * (int64_t)t + j] * x[edges[6 * (int64_t)t + j]];
+    centroid_fields(X, ev, E, D);
+    double B[3];
+    for (int a = 0; a < 3; ++a) {
+      B[a] = b[3 * (int64_t)t + a] + D[a] * h;
+      b[3 * (int64_t)t + a] = B[a];
+    }
+    if (mask)
+      for (int i = 0; i < nsnap; ++i)
+        if ((mask >> i) & 1) {
+          double* o = snap + ((int64_t)i * T + t) * 9;
+          for (int a = 0; a < 3; ++a) {
+            o[a] = E[a];
+            o[3 + a] = D[a];
+            o[6 + a] = B[a];
+          }
+        }
+  }
+}
+
 namespace {
 
 struct Engine {
@@ -88,6 +126,10 @@ struct Engine {
   std::vector<int> slot_node, tnode;
   DBuf<double> recent;  // W most recent node states, node id % W
   int last_node = 0;
+  // whole-mesh fields: active in the output pass until every snapshot is taken
+  bool mf_act = false;
+  int* mf_h = nullptr;        // pinned: trigger bits of the rows about to be sampled
+  double* mf_dt_h = nullptr;  // pinned: their dt
 
   Engine(temf_ctx& c_, const RunOptions& o, RunResult& r) : c(c_), opt(o), res(r) {
     st = c.stream;
@@ -117,6 +159,13 @@ struct Engine {
     k_set_ptr<<<1, 1, 0, st>>>(lptr.p + 0, c.slots[0].L.p);
     k_set_ptr<<<1, 1, 0, st>>>(lptr.p + 1, c.slots[1].L.p);
     TEMF_CHECK_LAUNCH();
+    if (c.mf.n() > 0) {
+      if (nrhs != 1) throw ArgError("whole-mesh field dumps need one right-hand side");
+      c.mf.trig.alloc(dbl + 8);
+      c.mf.dt.alloc(1);
+      TEMF_CUDA(cudaMallocHost((void**)&mf_h, (dbl + 8) * sizeof(int)));
+      TEMF_CUDA(cudaMallocHost((void**)&mf_dt_h, sizeof(double)));
+    }
     rec = opt.record_every > 0;
     if (rec) {
       if (nrhs != 1) throw ArgError("adjoint recording supports one right-hand side");
@@ -166,6 +215,8 @@ struct Engine {
   void set_sn(int k, int node) { slot_node[((k % RS) + RS) % RS] = node; }
   ~Engine() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    if (mf_h) cudaFreeHost(mf_h);
+    if (mf_dt_h) cudaFreeHost(mf_dt_h);
     if (coef_h) cudaFreeHost(coef_h);
     if (err_h) cudaFreeHost(err_h);
     cudaEventDestroy(ev0);
@@ -209,11 +260,46 @@ struct Engine {
     res.n_solve += 1;
   }
   void sample(const double* x, int k) {
+    if (mf_act) {
+      const int T = c.n_tets;
+      k_mesh_fields<<<std::min(ceil_div(T, 256), 148 * 16), 256, 0, st>>>(
+          T, c.d_xyz.p, c.d_tet_vex.p, c.mf.edges.p, c.d_tet_drc.p, x, c.mf.dt.p, c.mf.trig.p, row_base.p, k,
+          c.mf.b.p, c.mf.snap.p, c.mf.n());
+      TEMF_CHECK_LAUNCH();
+      res.launches += 1;
+    }
     if (!nrec) return;
     k_receivers_row<<<ceil_div(nrec * 6, 128), 128, 0, st>>>(nrec, c.rec.d_edges.p, c.rec.d_rhs.p, c.rec.d_w.p, x,
                                                              nrhs, row_base.p, k, trace.p);
     TEMF_CHECK_LAUNCH();
     res.launches += 1;
+  }
+  // trigger bits of the output rows first_row .. first_row + n - 1 (times t)
+  // and their dt, uploaded before those rows are sampled; the first row at or
+  // after each vtkout time takes its snapshot (src/FETD_FWD.f90:1646-1655)
+  void mf_rows(int first_row, const double* t, int nrows, double dt) {
+    if (!mf_act) return;
+    std::vector<int>& done = c.mf.done;
+    for (int r = 0; r < nrows; ++r) {
+      int mask = 0;
+      for (int i = 0; i < c.mf.n(); ++i)
+        if (!done[i] && t[r] >= c.mf.times[i]) {
+          mask |= 1 << i;
+          done[i] = 1;
+        }
+      mf_h[r] = mask;
+    }
+    mf_dt_h[0] = dt;
+    TEMF_CUDA(cudaMemcpyAsync(c.mf.trig.p + first_row, mf_h, nrows * sizeof(int), cudaMemcpyHostToDevice, st));
+    TEMF_CUDA(cudaMemcpyAsync(c.mf.dt.p, mf_dt_h, sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  // after the rows are sampled: stop once every snapshot is taken
+  void mf_after() {
+    if (!mf_act) return;
+    TEMF_CUDA(cudaStreamSynchronize(st));  // mf_h is rewritten by the next rows
+    bool all = true;
+    for (int d : c.mf.done) all = all && d;
+    if (all) mf_act = false;
   }
   double source_scalar(int step_no, double t, double dt) {
     if (step_no >= opt.step_dvsi) return 0.0;  // sys_right, src/FETD_FWD.f90:1484
@@ -250,9 +336,16 @@ struct Engine {
     for (auto& p : pending) any_src |= (p.coef != 0.0);
     k_set_int<<<1, 1, 0, st>>>(row_base.p, trace_rows);
     TEMF_CHECK_LAUNCH();
+    if (mf_act) {
+      std::vector<double> tr(N);
+      for (int k = 0; k < N; ++k) tr[k] = pending[k].t;
+      mf_rows(trace_rows, tr.data(), N, pending[0].dt);
+    }
+    const bool mf_now = mf_act;
+    const int key = 2 * N + (mf_now ? 1 : 0);  // graphs with and without the mesh-field launches
     TEMF_CUDA(cudaEventRecord(ev0, st));
     if (opt.use_graphs && !any_src && !rec) {
-      auto it = graphs.find(N);
+      auto it = graphs.find(key);
       if (it == graphs.end()) {
         const int64_t l0 = res.launches;
         const int s0 = res.n_solve;
@@ -266,13 +359,13 @@ struct Engine {
         cudaGraphExec_t ge;
         TEMF_CUDA(cudaGraphInstantiate(&ge, g, 0));
         TEMF_CUDA(cudaGraphDestroy(g));
-        graph_kernels[N] = res.launches - l0;
+        graph_kernels[key] = res.launches - l0;
         res.launches = l0;
         res.n_solve = s0;
-        it = graphs.emplace(N, ge).first;
+        it = graphs.emplace(key, ge).first;
       }
       TEMF_CUDA(cudaGraphLaunch(it->second, st));
-      res.launches += graph_kernels[N];
+      res.launches += graph_kernels[key];
       res.n_solve += N;
     } else {
       for (int k = 0; k < N; ++k) coef_h[k] = pending[k].coef;
@@ -297,6 +390,7 @@ struct Engine {
     for (auto& p : pending) out_row(p.step, p.t, p.dt);
     trace_rows += N;
     pending.clear();
+    mf_after();
     return N;
   }
 
@@ -326,7 +420,15 @@ struct Engine {
         }
         k_set_int<<<1, 1, 0, st>>>(row_base.p, 0);
         trace_rows = 0;
+        if (c.mf.n() > 0 && pass_output) {  // a new output pass: B from zero, no snapshot taken
+          mf_act = true;
+          c.mf.done.assign(c.mf.n(), 0);
+          TEMF_CUDA(cudaMemsetAsync(c.mf.b.p, 0, c.mf.b.bytes(), st));
+          const double t0 = time_cur - step_cur;
+          mf_rows(0, &t0, 1, step_cur);
+        }
         sample(E(1), 0);
+        mf_after();
         out_row(0, time_cur - step_cur, step_cur);
         if (rec) {
           set_sn(1, 0); set_sn(0, 0);
@@ -405,7 +507,9 @@ struct Engine {
         }
         k_set_int<<<1, 1, 0, st>>>(row_base.p, trace_rows);
         if (reject) {
+          mf_rows(trace_rows, &time_cur, 1, step_cur);
           sample(T(0), 0);
+          mf_after();
           out_row(step, time_cur, step_cur);
           if (rec) {
             c.adj.row_node.push_back(tnode[0]);
@@ -418,7 +522,12 @@ struct Engine {
           e1 = E(1);
           not_changed += 1;
         } else {
+          {
+            const double t_row = tmp_time_cur + (opt.legacy_linux ? step_cur : 0.0);
+            mf_rows(trace_rows, &t_row, 1, tmp_step_cur);
+          }
           sample(T(dsz - 1), 0);
+          mf_after();
           // e3 = all_e(idx) (src/FETD_FWD.f90:1405); the build that wrote the
           // shipped LINUX/*.field files restarted from all_e(idx - sp_dblesize)
           if (rec) {

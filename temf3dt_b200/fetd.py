@@ -252,6 +252,19 @@ class FetdGPU:
                                   int(max_steps)), "temf_run")
         return self.result()
 
+    def set_mesh_fields(self, times) -> None:
+        """Whole-mesh field snapshots (vtkout) for the next run; [] turns them off."""
+        t = as_f64(times if len(times) else [0.0])
+        self._ck(self._L.temf_set_mesh_fields(self._h, len(times), dptr(t)), "temf_set_mesh_fields")
+
+    def mesh_fields(self, index: int):
+        """(fields (n_tets, 9) = E, D, B at the snapshot, reached?) of the last run."""
+        out = np.zeros(9 * self.n_tets)
+        done = C.c_int(0)
+        self._ck(self._L.temf_result_mesh_fields(self._h, int(index), dptr(out), C.byref(done)),
+                 "temf_result_mesh_fields")
+        return out.reshape(self.n_tets, 9), bool(done.value)
+
     def result(self) -> RunOutput:
         """Output of the last run of this context (temf_run or a batch run)."""
         rows = C.c_int(0)

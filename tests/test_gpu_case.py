@@ -61,3 +61,71 @@ def test_native_driver_reproduces_the_shipped_linux_field(tmp_path):
     big = np.abs(gd) >= 1e-3 * np.abs(gd).max()
     rel = np.abs(v[big] - gd[big]) / np.abs(gd[big])
     assert rel.max() < 6e-4, rel.max()
+
+
+def test_mesh_field_snapshots_match_the_oracle():
+    """vtkout snapshots (E, D, B at every tet centroid) of the GPU run against
+    the oracle's vtk_field_save restatement, same trial decisions."""
+    from oracle import fetd_oracle as O
+    from tests.golden_cases import synth_oracle_model
+    m = tiny_synth()
+    times = [1e-6, 5e-6]
+    om = synth_oracle_model(m)
+    om.ctl.vtk_times = np.array(times)
+    ref = O.run_fetd(om)
+    with fetd.FetdGPU(0) as g:
+        fetd.load_case(g, m.mesh, m.ctl)
+        g.set_mesh_fields(times)
+        out = g.run(m.ctl.sp_division, m.ctl.sp_double, m.ctl.sp_dblesize, m.ctl.time_maximum,
+                    forced=np.array(ref.trial_accepted, dtype=np.int32))
+        assert np.array_equal(out.steps, np.array(ref.steps))
+        for i in range(len(times)):
+            f, done = g.mesh_fields(i)
+            assert done
+            r = ref.mesh_fields[i]
+            for lo in (0, 3, 6):
+                scale = np.abs(r[:, lo:lo + 3]).max()
+                assert np.abs(f[:, lo:lo + 3] - r[:, lo:lo + 3]).max() <= 1e-8 * scale, (i, lo)
+
+
+def test_native_driver_writes_the_msh_dumps(tmp_path):
+    """temf_fetd with vtkout times and ROOT.msh present writes ROOT_i.msh;
+    its element data match the oracle's msh_output to the 8 printed digits."""
+    from oracle import fetd_oracle as O
+    from tests.golden_cases import synth_oracle_model
+    from tests.test_mesh_fields import _write_msh41
+    m = tiny_synth()
+    m.ctl.vtk_times = np.array([1e-6, 5e-6])
+    m.ctl.output = np.array([1, 1, 1, 0, 0, 1, 0, 0, 1], dtype=bool)
+    root = str(tmp_path / "v")
+    meshio.write_mesh(root + ".mesh", m.mesh)
+    meshio.write_cntl(root + ".cntl", m.ctl)
+    _write_msh41(root + ".msh", m.mesh)
+    cli = os.path.join(ROOT, "temf3dt_b200", "temf_fetd")
+    r = subprocess.run([cli, "-f", root], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    om = synth_oracle_model(m)
+    om.ctl.vtk_times = m.ctl.vtk_times
+    om.ctl.o_f = m.ctl.output
+    ref = O.run_fetd(om)
+    for i in (1, 2):
+        O.write_msh_fields(root + ".msh", str(tmp_path / ("o_%d.msh" % i)), ref.mesh_fields[i - 1], m.ctl.output)
+
+        def values(path):
+            vals, on = [], False
+            for ln in open(path):
+                if ln.startswith("$ElementData"):
+                    on, skip = True, 8
+                    continue
+                if ln.startswith("$EndElementData"):
+                    on = False
+                    continue
+                if on:
+                    if skip:
+                        skip -= 1
+                        continue
+                    vals.append(float(ln.split()[1]))
+            return np.array(vals)
+        a, b = values(root + "_%d.msh" % i), values(str(tmp_path / ("o_%d.msh" % i)))
+        assert a.shape == b.shape and len(a) == 5 * len(m.mesh.tet_vex)
+        assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
