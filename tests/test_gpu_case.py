@@ -65,14 +65,29 @@ def test_native_driver_reproduces_the_shipped_linux_field(tmp_path):
 
 def test_mesh_field_snapshots_match_the_oracle():
     """vtkout snapshots (E, D, B at every tet centroid) of the GPU run against
-    the oracle's vtk_field_save restatement, same trial decisions."""
+    the oracle's vtk_field_save restatement, same trial decisions.
+
+    E inside the air (1e-12 S/m) is not determined to 1e-8 by any of the
+    solvers: its gradient part only meets the tiny air mass 3 M_air, so it
+    carries the solve's rounding amplified by the air/earth contrast.  The
+    oracle on SuperLU and the oracle on the CPU supernodal Cholesky (same
+    FP64 loop, another elimination order) already differ there by 2.7e-8
+    and 4e-7 of the group maximum at the two snapshots, while they agree to
+    1e-14 on earth E, D and B.  So air E is held to ten times that measured
+    solver-to-solver floor; everything else to 1e-9."""
     from oracle import fetd_oracle as O
+    from oracle import supernodal_cpu as SN
     from tests.golden_cases import synth_oracle_model
     m = tiny_synth()
     times = [1e-6, 5e-6]
     om = synth_oracle_model(m)
     om.ctl.vtk_times = np.array(times)
     ref = O.run_fetd(om)
+    SN.build()
+    alt = O.run_fetd(om, slots=SN.SupernodalSlots(om, threads=2))
+    assert alt.steps == ref.steps
+    air = om.sig < 1e-6
+    assert air.any() and (~air).any()
     with fetd.FetdGPU(0) as g:
         fetd.load_case(g, m.mesh, m.ctl)
         g.set_mesh_fields(times)
@@ -82,10 +97,17 @@ def test_mesh_field_snapshots_match_the_oracle():
         for i in range(len(times)):
             f, done = g.mesh_fields(i)
             assert done
-            r = ref.mesh_fields[i]
+            r, a = ref.mesh_fields[i], alt.mesh_fields[i]
             for lo in (0, 3, 6):
                 scale = np.abs(r[:, lo:lo + 3]).max()
-                assert np.abs(f[:, lo:lo + 3] - r[:, lo:lo + 3]).max() <= 1e-8 * scale, (i, lo)
+                err = np.abs(f[:, lo:lo + 3] - r[:, lo:lo + 3]).max(axis=1)
+                if lo == 0:
+                    floor = np.abs(a[air, 0:3] - r[air, 0:3]).max()
+                    assert err[air].max() <= max(1e-8 * scale, 10.0 * floor), (i, err[air].max() / scale,
+                                                                                floor / scale)
+                    assert err[~air].max() <= 1e-9 * scale, (i, lo, err[~air].max() / scale)
+                else:
+                    assert err.max() <= 1e-9 * scale, (i, lo, err.max() / scale)
 
 
 def test_native_driver_writes_the_msh_dumps(tmp_path):
