@@ -38,8 +38,13 @@ def test_noalloc_solve_matches_regular_solve_twice():
             b_dev = torch.tensor(b, dtype=torch.float64, device="cuda")
             x_dev = torch.full_like(b_dev, float("nan"))
             torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
             rc = g._L.temf_solve_noalloc(g._h, 1, C.c_void_p(b_dev.data_ptr()), C.c_void_p(x_dev.data_ptr()))
             assert rc == 0, g.last_error()
+            if call == 1:
+                # the second call finds everything in place: the device's free
+                # memory is what it was (cudaMemGetInfo, whole device)
+                assert torch.cuda.mem_get_info()[0] == free_before
             x = x_dev.cpu().numpy()
             nb = np.linalg.norm(b)
             assert np.linalg.norm(A @ x - b) <= BACKWARD_TOL * nb
