@@ -5,17 +5,22 @@ adaptive BDF2 time loop from t = 0 to time_maximum with every refactorisation
 at the dt-doubling trials (adap_euler, src/FETD_FWD.f90:1229-1464), i.e. the
 whole job, with the mesh analysed and the matrices assembled beforehand.
   value = (time steps of the run x RHS columns x ranks) / device time of the run.
-The default workload is the 3-D block model (0.01 S/m host, 0.1 S/m block,
-air 1e-12 S/m, 1000 m square loop, 64 receivers on a 20 m line, ~1.2M edges),
-synthetic and seeded.  Its factors (GBs) exceed the 126 MB L2 many times over,
-so no L2 flush is needed between steps.
+The default workload (config 1) is the 3-D block model: 0.01 S/m host,
+0.1 S/m block of 200 x 200 x 100 m with its top at 100 m, air 1e-12 S/m,
+1000 m square loop, 64 receivers on a 20 m line; 1 238 964 tets and
+1 477 597 edges, synthetic and seeded.  Its factors (GBs) exceed the 126 MB
+L2 many times over, so no L2 flush is needed between steps.
 
-batched: 64 sources on the config-2 mesh as one 64-column block per step
-against the plain single-RHS path on that mesh, over the first 300 steps.
-
-adjoint: one gradient of a dB/dt misfit with respect to log sigma on a
-32 x 32 x 16 inversion grid (recorded forward run + reverse sweep), reported
-beside the metric with its ratio to one forward run.
+Beside the headline, on one GPU, the default line carries the other configs
+of the metric:
+  batched: config 2, the 64 small loops (50 x 50 m, 8 x 8 at 40 m) on the same
+           mesh as one 64-column block per step, the full run, against the
+           headline (plain single-RHS on the same mesh), with the dB/dt error
+           of four columns against plain runs replaying the same decisions;
+  models:  16 layered models of uneven size in one batch against one after another;
+  adjoint: config 3, the gradient of a dB/dt misfit (64 receivers x 40 gates)
+           with respect to log sigma of 32 x 32 x 16 log-normal cells on the
+           same mesh, against one forward run of that model.
 
 e2e: the same metric through the public API with host buffers: per step the
 conductivity/permeability per tet and the source/receiver arrays are copied
@@ -26,9 +31,9 @@ traces copied back.
 which cannot be built or run here; its CPU restatement is timed instead: the
 oracle's adaptive BDF2 loop on a multithreaded supernodal Cholesky
 (oracle/supernodal_cpu.cpp, the same ordering as the GPU path, OpenMP +
-OpenBLAS on all host cores), on the full-resolution model, each bench step
-one run from rest up to the first doubling trial (sp_double - 1 time
-steps) including its factorisation.
+OpenBLAS on all host cores), on the full-resolution model; each bench step
+runs the first 10 time steps from rest, with the factorisation timed once
+and amortised over a doubling period.
 """
 from __future__ import annotations
 
@@ -45,11 +50,24 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# The block models share one grid (the lines of the 1000 m loop and of the 8 x 8
+# small loops; 44 m cells in the core, 22 m vertically near the surface):
+# 1 238 964 tets, 1 477 597 edges.  Config 2 is the config-1 mesh with other
+# sources and receivers; config 3 the config-1 mesh with per-cell conductivity.
+BLOCK_GRID = dict(shared_grid=True, h_core=44.0, h_z=22.0)
 CONFIGS = {
     0: dict(kind="halfspace", kw=dict(h_core=125, ratio=2.0, h_z=25), label="halfspace-0.001Spm-loop500m-150k-edges"),
-    1: dict(kind="block", kw=dict(), label="block3d-0.01/0.1Spm-square1000m-64rec-1.2M-edges"),
-    2: dict(kind="multiloop", kw=dict(), label="block3d-64-loops-64rhs"),
+    1: dict(kind="block", kw=dict(BLOCK_GRID), label="block3d-0.01/0.1Spm-square1000m-64rec-1.24M-tets-1.48M-edges"),
+    2: dict(kind="multiloop", kw=dict(BLOCK_GRID), label="block3d-1.48M-edges-64-loops-64rhs"),
+    3: dict(kind="block", kw=dict(BLOCK_GRID),
+            label="block3d-1.48M-edges-lognormal-32x32x16-cells-64rec-40gates-adjoint"),
 }
+# config 3: the inversion grid (32 x 32 x 16 cells of 25 x 25 x 12.5 m under the
+# loop), log-normal cell conductivities around 0.01 S/m with 0.5 decades, and
+# the observations of a seeded perturbation of that model (0.1 decades)
+INV_SHAPE = (32, 32, 16)
+INV_BOX = ((-400.0, 400.0), (-400.0, 400.0), (0.0, 200.0))
+GATES = np.logspace(-6, -2, 40)
 COMMON = dict(t0=1e-6, sp_division=10, sp_double=100, time_maximum=1e-2)
 
 
@@ -132,18 +150,17 @@ def host_cores() -> int:
     return host_threads()
 
 
-def cpu_arm(cfg: int, steps: int, warmup: int, sample_steps: int = 0, scaled: bool = False):
+def cpu_arm(cfg: int, steps: int, warmup: int, sample_steps: int = 0):
     """The reference's CPU path restated (oracle/): the adaptive BDF2 loop of
     fetd_oracle on the CPU supernodal Cholesky (oracle/supernodal_cpu.cpp,
     OpenMP + OpenBLAS, all host cores), on the full-resolution model of the
-    config.  One bench step = one run of the loop from rest over its first
-    `sample_steps` time steps (default: sp_double - 1, up to the first
-    doubling trial), including its factorisation.  Warm-up: one factorisation at the
-    first time step's dt, then one solve per warm-up step.
-    `scaled`: a shorter sample whose factorisation time is amortised over a
-    doubling period (one factorisation per sp_double steps, as in the full
-    run): steps/s = 1 / (seconds per time step + factorisation / sp_double).
-    Falls back to the reduced-resolution model when two factor slots do not
+    config.  One bench step = the loop's first `sample_steps` time steps from
+    rest (default 10: BDF2 right-hand side, source, solve, receivers), on the
+    factor of the first dt.  That factorisation is timed once, at warm-up,
+    and amortised over one doubling period, as the full run has about one
+    factorisation per sp_double steps (10 in 995 on the block model):
+        steps/s = 1 / (seconds per time step + factorisation s / sp_double).
+    Falls back to the reduced-resolution model when a factor slot does not
     fit in free host memory."""
     from oracle import fetd_oracle as O
     from oracle import supernodal_cpu as SN
@@ -155,7 +172,7 @@ def cpu_arm(cfg: int, steps: int, warmup: int, sample_steps: int = 0, scaled: bo
     slots = SN.SupernodalSlots(om, threads=threads)
     try:
         import psutil
-        if 2 * 8 * slots.stats[2] + 4e9 > psutil.virtual_memory().available:
+        if 8 * slots.stats[2] + 4e9 > psutil.virtual_memory().available:
             del slots
             reduced = True
             om = synth_oracle_model(model_for(cfg, reduced=True))
@@ -163,113 +180,169 @@ def cpu_arm(cfg: int, steps: int, warmup: int, sample_steps: int = 0, scaled: bo
     except ImportError:
         pass
     period = int(om.ctl.step_dble)
-    # the default sample stops before the first doubling trial (step sp_double), whose extra
-    # factorisation would give it two factorisations per period instead of the run's one
-    S = sample_steps or period - 1
-    fac_s = [0.0]
-    factor = slots.factor
+    S = sample_steps or 10
+    dt0 = om.ctl.src_pulsewidth / om.ctl.step_dvsi
+    # the factor of the first dt is computed once and reused by every sample
+    t0 = time.perf_counter()
+    slots.factor(1, dt0)
+    fac_s = time.perf_counter() - t0
+    factor, release = slots.factor, slots.release
+    held = {1: dt0}
 
-    def timed_factor(slot, dt):
-        t0 = time.perf_counter()
-        factor(slot, dt)
-        fac_s[0] += time.perf_counter() - t0
+    def cached_factor(slot, dt):
+        if held.get(slot) != dt:
+            factor(slot, dt)
+            held[slot] = dt
 
-    slots.factor = timed_factor
-    if warmup > 0:  # one factorisation, then one solve per warm-up step
-        factor(1, om.ctl.src_pulsewidth / om.ctl.step_dvsi)
-        rhs = np.ones(om.n)
-        for _ in range(warmup):
-            slots.solve(1, rhs)
-        slots.release(1)
+    def keep_release(slot):
+        if slot != 1:
+            release(slot)
+            held.pop(slot, None)
+
+    slots.factor, slots.release = cached_factor, keep_release
+    rhs = np.ones(om.n)
+    for _ in range(warmup):   # one solve per warm-up step
+        slots.solve(1, rhs)
     vals, secs = [], []
     for _ in range(steps):
-        fac_s[0] = 0.0
-        nf = slots.n_factor
         t = time.perf_counter()
         res = O.run_fetd(om, max_steps=S, slots=slots)
         dt = time.perf_counter() - t
         n = len(res.steps) - 1
-        if scaled:
-            per_factor = fac_s[0] / max(1, slots.n_factor - nf)
-            vals.append(1.0 / ((dt - fac_s[0]) / n + per_factor / period))
-        else:
-            vals.append(n / dt)
+        vals.append(1.0 / (dt / n + fac_s / period))
         secs.append(dt)
     info = dict(n_edges=om.n, steps=S, seconds=float(np.mean(secs)), threads=threads, reduced=reduced,
-                factorisations=slots.n_factor, stored=float(slots.stats[2]))
-    how = ("%d time steps from rest incl. the factorisation, %.1f s per sample" % (S, info["seconds"]) if not scaled
-           else "%d time steps from rest (%.1f s), the factorisation time amortised over one doubling period "
-                "(%d steps)" % (S, info["seconds"], period))
+                factor_s=fac_s, stored=float(slots.stats[2]))
+    how = ("%d time steps from rest per sample (%.1f s), on the factor of the first dt; its factorisation "
+           "(%.1f s, timed once) amortised over one doubling period (%d steps)" % (S, info["seconds"], fac_s, period))
     text = ("CPU restatement (oracle/: fetd_oracle's adaptive BDF2 loop on a supernodal Cholesky with the same "
             "ordering, OpenMP + OpenBLAS on %d threads) on the %s %d-edge model: %s; not MKL PARDISO, which "
             "cannot be built here" % (threads, "reduced-resolution" if reduced else "full-resolution", om.n, how))
     return float(np.mean(vals)), info, text
 
 
-def inversion_cells(m, shape=(32, 32, 16), box=((-640.0, 640.0), (-640.0, 640.0), (0.0, 400.0))):
-    """Tet -> cell map of a regular inversion grid under the loop (0-based, -1
-    outside): 32 x 32 x 16 cells of 40 x 40 x 25 m by default."""
-    X = m.mesh.nod_cor[m.mesh.tet_vex - 1].mean(axis=1)
-    idx = []
-    inside = np.ones(len(X), dtype=bool)
-    for a in range(3):
-        lo, hi = box[a]
-        k = np.floor((X[:, a] - lo) / (hi - lo) * shape[a]).astype(np.int64)
-        inside &= (k >= 0) & (k < shape[a])
-        idx.append(np.clip(k, 0, shape[a] - 1))
-    cell = (idx[0] * shape[1] + idx[1]) * shape[2] + idx[2]
-    return np.where(inside, cell, -1), int(np.prod(shape))
+def config3_media(m, seed: int = 3):
+    """Config 3 on the config-1 mesh: the tet -> cell map of the 32 x 32 x 16
+    inversion grid, the log-normal model (median 0.01 S/m, 0.5 decades) and
+    the seeded perturbation (x 10^(0.1 N(0,1)) per cell) that makes the
+    observations; conductivity per tet for both, permeability per tet."""
+    from temf3dt_b200 import inversion, meshio
+    grid = inversion.InversionGrid(INV_SHAPE, INV_BOX)
+    cell = grid.tet_cells(m.mesh.nod_cor, m.mesh.tet_vex)
+    sig0, mu = meshio.media_per_tet(m.mesh.tet_phy, m.ctl)
+    earth = sig0 > 1e-6
+    cell = np.where(earth, cell, -1)            # the grid lies below the surface; air tets keep 1e-12
+    sc = inversion.lognormal_cells(grid.ncell, 0.01, 0.5, seed)
+    sc_true = sc * 10.0 ** (0.1 * np.random.default_rng(seed + 30).standard_normal(grid.ncell))
+    return dict(cell=cell, ncell=grid.ncell, mu=mu, sig=inversion.sigma_with_cells(sig0, cell, sc),
+                sig_true=inversion.sigma_with_cells(sig0, cell, sc_true), cell_sigma=sc)
 
 
-def adjoint_measure(g, m, one_run, forward_ms):
-    """Gradient of J = 1/2 sum (d - d_obs)^2 over the receivers' dB/dt with
-    respect to log sigma of a 32 x 32 x 16 grid: a recorded forward run
-    (eager launches, checkpoints every 50 solves) and the reverse sweep, both
-    timed with CUDA events inside the library."""
-    cell, ncell = inversion_cells(m)
-    g.adjoint_record(50)
-    o = one_run()
-    rng = np.random.default_rng(7)
-    d_obs = o.fields * (1 + 0.05 * rng.standard_normal(o.fields.shape))
-    mask = np.zeros_like(d_obs)
-    mask[:, :, 3:6] = 1.0
-    dJ = mask * (o.fields - d_obs)
-    grad, _, tm = g.adjoint(dJ, cell, ncell)
-    g.adjoint_record(0)
-    return {"ms": tm["ms_total"], "recorded_forward_ms": o.ms_total, "forward_ms": forward_ms,
-            "ratio_to_forward": tm["ms_total"] / forward_ms, "factor_ms": tm["ms_factor"], "nodes": tm["nodes"],
-            "blocks": tm["blocks"], "factorisations": tm["factors"], "launches": tm["launches"],
-            "checkpoint_every": 50, "cells": ncell, "cells_in_mesh": int(len(np.unique(cell[cell >= 0]))),
-            "grad_finite": bool(np.isfinite(grad).all())}
+def adjoint_measure(local: int, fd_cells: int = 0):
+    """Config 3: gradient of J = 1/2 sum (dBz/dt - d_obs)^2 over 64 receivers x
+    40 gates with respect to log sigma of the 32 x 32 x 16 cells: a recorded
+    forward run (eager launches, checkpoints every 50 solves) and the reverse
+    sweep, both timed with CUDA events inside the library, against one
+    forward run of the same model.  fd_cells > 0: central differences
+    (log sigma +- 1e-3, the run's accept/reject decisions replayed) on that
+    many seeded random cells."""
+    from temf3dt_b200 import fetd, inversion
+    m = model_for(3)
+    c = m.ctl
+    md = config3_media(m)
+    args = (c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum)
+    with fetd.FetdGPU(local) as g:
+        fetd.load_case(g, m.mesh, m.ctl)
+        g.set_media(md["sig_true"], md["mu"])
+        g.assemble()
+        o_true = g.run(*args)
+        d_obs = inversion.gate_matrix(o_true.times, GATES) @ o_true.fields[:, :, 5]
+        g.set_media(md["sig"], md["mu"])
+        g.assemble()
+        o_fwd = g.run(*args)
+        g.adjoint_record(50)
+        o = g.run(*args)
+        J, dJ = inversion.dbdt_misfit(o.fields, o.times, GATES, d_obs)
+        grad, _, tm = g.adjoint(dJ, md["cell"], md["ncell"])
+        g.adjoint_record(0)
+        out = {"ms": tm["ms_total"], "recorded_forward_ms": o.ms_total, "forward_ms": o_fwd.ms_total,
+               "ratio_to_forward": tm["ms_total"] / o_fwd.ms_total, "factor_ms": tm["ms_factor"],
+               "nodes": tm["nodes"], "blocks": tm["blocks"], "factorisations": tm["factors"],
+               "launches": tm["launches"], "checkpoint_every": 50, "cells": md["ncell"],
+               "cells_in_mesh": int(len(np.unique(md["cell"][md["cell"] >= 0]))), "misfit": J,
+               "receivers": int(o.fields.shape[1]), "gates": len(GATES), "grad_finite": bool(np.isfinite(grad).all()),
+               "model": "log-normal cells (median 0.01 S/m, 0.5 decades), observations of a 0.1-decade perturbation"}
+        if fd_cells > 0:
+            forced = o.trial_accepted.astype(np.int32)
+            hit = np.unique(md["cell"][md["cell"] >= 0])
+            pick = np.random.default_rng(32).choice(hit, size=min(fd_cells, len(hit)), replace=False)
+            h = 1e-3
+            rel = []
+            for k in pick:
+                Jpm = []
+                for sgn in (1.0, -1.0):
+                    sig = md["sig"].copy()
+                    sig[md["cell"] == k] *= np.exp(sgn * h)
+                    g.set_media(sig, md["mu"])
+                    g.assemble()
+                    ok = g.run(*args, forced=forced)
+                    Jpm.append(inversion.dbdt_misfit(ok.fields, ok.times, GATES, d_obs)[0])
+                fd = (Jpm[0] - Jpm[1]) / (2 * h)
+                rel.append(abs(fd - grad[k]) / max(abs(fd), 1e-300))
+            scale = float(np.abs(grad).max())
+            out["fd"] = {"cells": [int(k) for k in pick], "max_rel_err": float(max(rel)),
+                         "median_rel_err": float(np.median(rel)), "step": h, "grad_max": scale}
+    return out
 
 
-def batched_measure(local: int, max_steps: int):
-    """64 small loops on the 3-D block mesh as one 64-column block per step
-    against the plain single-RHS path on the same mesh, both over the same
-    leading steps of the run (factorisations included), after one warm-up."""
+def batched_measure(local: int, plain_value: float, check_cols=(0, 27, 36, 63)):
+    """Config 2: the 64 small loops on the config-1 mesh as one 64-column
+    block per step, the full adaptive run (every factorisation included),
+    after one warm-up run over the first 150 steps (autotuning, graph
+    captures).  Against the plain single-RHS path on the same mesh (the
+    headline value).  Accuracy: the columns in check_cols run again as plain
+    single-RHS runs replaying the block run's accept/reject decisions; the
+    largest dB/dt difference relative to each trace's maximum is reported."""
     from temf3dt_b200 import fetd
     m = model_for(2)
     c = m.ctl
+    args = (c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum)
     out = {}
     with fetd.FetdGPU(local) as g:
         info = fetd.load_case(g, m.mesh, m.ctl)
-        out["n_edges"] = int(g.stats()["n"])
-        g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum, max_steps=max_steps)
-        o = g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum, max_steps=max_steps)
-        plain = (len(o.steps) - 1) / (o.ms_total / 1e3)
+        st = g.stats()
+        out["n_edges"] = int(st["n"])
         cols = m.source_columns(info["edg_vex"])
+        rec_tet = g.locate(m.receivers, c.rec_charac)
         g.set_sources(cols, 1, c.pulse_type, c.t0, 1.0)
-        g.set_receivers(g.locate(m.receivers, c.rec_charac), m.receivers, rec_rhs=m.rec_rhs)
-        g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum, max_steps=max_steps)
-        ob = g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum, max_steps=max_steps)
+        g.set_receivers(rec_tet, m.receivers, rec_rhs=m.rec_rhs)
+        g.run(*args, max_steps=150)
+        ob = g.run(*args)
         batched = (len(ob.steps) - 1) * len(cols) / (ob.ms_total / 1e3)
-    out.update({"value": batched, "unit": "steps*RHS/s", "rhs": len(cols), "plain_value": plain,
-                "batched_over_plain": batched / plain, "steps": len(ob.steps) - 1,
-                "ms_per_step_batched": ob.ms_steps / max(ob.n_solve, 1),
-                "ms_per_step_plain": o.ms_steps / max(o.n_solve, 1),
-                "ms_factor_batched": ob.ms_factor, "ms_factor_plain": o.ms_factor,
-                "workload": CONFIGS[2]["label"] + ", first %d steps" % max_steps})
-    return out
+        forced = ob.trial_accepted.astype(np.int32)
+        errs = {}
+        for k in check_cols:
+            g.set_sources([cols[k]], 1, c.pulse_type, c.t0, 1.0)
+            r = [i for i in range(len(m.receivers)) if m.rec_rhs[i] == k]
+            g.set_receivers(rec_tet[r], m.receivers[r], rec_rhs=np.zeros(len(r), dtype=np.int32))
+            o = g.run(*args, forced=forced)
+            if not np.array_equal(o.steps, ob.steps):
+                errs[int(k)] = float("inf")
+                continue
+            a, b = ob.fields[:, r, 3:6], o.fields[:, :, 3:6]
+            errs[int(k)] = float(np.abs(a - b).max() / np.abs(b).max())
+    ms_step = ob.ms_steps / max(ob.n_solve, 1)
+    flops = (4 * st["nnz_L"] + 2 * st["nnz_A"]) * len(cols)
+    return {**out, "value": batched, "unit": "steps*RHS/s", "rhs": len(cols), "plain_value": plain_value,
+            "batched_over_plain": batched / plain_value, "steps": len(ob.steps) - 1,
+            "factorisations": ob.n_factor, "ms_run": ob.ms_total, "ms_per_step_batched": ms_step,
+            "ms_factor_batched": ob.ms_factor,
+            "dbdt_rel_err_vs_plain": {"columns": errs, "max": max(errs.values()),
+                                      "definition": "max |batched - plain| / max |plain| over the run, dB/dt"},
+            "roofline": {"bound": "tensor", "unit": "TFLOP/s", "algorithmic_flops_per_step": flops,
+                         "achieved": flops / (ms_step / 1e3) / 1e12,
+                         "kernel": "one 64-column block step: BDF2 SpMM + persistent DMMA block sweeps + receivers"},
+            "workload": CONFIGS[2]["label"] + ", full run"}
 
 
 def layered_models(n_models: int = 16, seed: int = 5):
@@ -342,7 +415,7 @@ def cpu_baseline(cfg: int, sample_steps: int) -> dict:
     scaled sample, run in a fresh process (no CUDA context, no torch threads)."""
     env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
     cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--config", str(cfg), "--steps", "1",
-           "--warmup", "0", "--sample-steps", str(sample_steps), "--cpu-scaled", "1"]
+           "--warmup", "0", "--sample-steps", str(sample_steps)]
     try:
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800, env=env)
     except subprocess.TimeoutExpired:
@@ -360,7 +433,7 @@ def reference_arm(args):
         return 0
     cfg = args.config
     try:
-        value, info, text = cpu_arm(cfg, args.steps, args.warmup, args.sample_steps, scaled=bool(args.cpu_scaled))
+        value, info, text = cpu_arm(cfg, args.steps, args.warmup, args.sample_steps)
     except Exception as e:  # noqa: BLE001 - the arm reports why it could not run
         print(json.dumps({"impl": "reference", "unavailable": "CPU restatement failed: %s" % repr(e)[:300]}))
         return 0
@@ -370,7 +443,7 @@ def reference_arm(args):
         "ms_per_step": 1e3 * info["seconds"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": CONFIGS[cfg]["label"], "n_edges": info["n_edges"],
-                   "sample": "first %d time steps from rest per step" % info["steps"],
+                   "sample": "first %d time steps from rest per step, factorisation amortised" % info["steps"],
                    "reduced_model": info["reduced"]},
         "cpu_baseline": {"value": value, "unit": "steps*RHS/s", "cores": info["threads"], "kind": "port",
                          "sample": text},
@@ -462,16 +535,20 @@ def ours(args):
         e2e_times.append(time.perf_counter() - t0)
     e2e_steps = len(o.steps) - 1
     e2e_val = e2e_steps * ncols * world / float(np.mean(e2e_times))
-    # --- adjoint gradient (single-RHS workloads): one recorded run + one reverse sweep ---
-    adj = None
-    if cfg != 2 and args.adjoint:
-        adj = adjoint_measure(g, m, one_run, outs[-1].ms_total)
-    models = None
-    if cfg == 2 and args.models > 0 and world == 1:
-        models = models_measure(local, args.models)
-    batched = None
-    if cfg == 1 and args.batched_steps > 0 and world == 1:
-        batched = batched_measure(local, args.batched_steps)
+    # --- the other configs of the metric, beside the headline (one GPU) ---
+    #   batched: config 2 (64 loops on this mesh as one block, full run) against this line's value
+    #   models:  16 layered models of uneven size, one after another and as one batch
+    #   adjoint: config 3 (log-normal cells on this mesh), one gradient against one forward run
+    adj = models = batched = None
+    if cfg == 1 and world == 1:
+        g.close()
+        g = None
+        if args.batched:
+            batched = batched_measure(local, value)
+        if args.models > 0:
+            models = models_measure(local, args.models)
+        if args.adjoint:
+            adj = adjoint_measure(local)
     # --- roofline of the dominant phase ---
     o = outs[-1]
     ms_fac = o.ms_factor / max(o.n_factor, 1)
@@ -538,9 +615,64 @@ def ours(args):
     }
     if rank == 0:
         print(json.dumps(line))
-    g.close()
+    if g is not None:
+        g.close()
     if world > 1:
         dist.destroy_process_group()
+    return 0
+
+
+def profile_run(args):
+    """--profile-steps N: the first N time steps of the config's model (its
+    factorisations included), for profiler captures; prints the phase
+    timings.  Not a bench line (no warm-up, part of a run).  With --timeline,
+    one single-column solve with per-task GPU timestamps instead, summarised
+    per phase of the tree (for the sweep kernels)."""
+    from temf3dt_b200 import fetd, synth
+    if args.h_core > 0:
+        kw = dict(CONFIGS[args.config]["kw"], **COMMON)
+        kw["h_core"] = args.h_core
+        m = synth.build_model(CONFIGS[args.config]["kind"], seed=args.config, **kw)
+    else:
+        m = model_for(args.config)
+    c = m.ctl
+    with fetd.FetdGPU(0) as g:
+        info = fetd.load_case(g, m.mesh, m.ctl)
+        if args.replicate > 1:
+            # the single loop as this many identical RHS columns
+            cols = [(info["src_edg"], info["src_drc"])] * args.replicate
+            g.set_sources(cols, c.source_type, c.pulse_type, c.t0, c.current)
+            g.set_receivers(np.repeat(info["rec_tet"], args.replicate), np.repeat(c.rec_cor, args.replicate, axis=0),
+                            rec_rhs=np.arange(args.replicate))
+        elif args.config == 2:
+            cols = m.source_columns(info["edg_vex"])
+            k = len(cols) if args.rhs <= 0 else min(args.rhs, len(cols))
+            g.set_sources(cols[:k], 1, c.pulse_type, c.t0, 1.0)
+            sel = [i for i in range(len(m.receivers)) if m.rec_rhs[i] < k]
+            g.set_receivers(g.locate(m.receivers[sel], c.rec_charac), m.receivers[sel], rec_rhs=m.rec_rhs[sel])
+        st = g.stats()
+        if args.timeline:
+            g.factor(1, c.t0 / c.sp_division)
+            split, cand = g.tune_solve(1, 1)
+            f, b = g.solve_timeline(1)
+            out = {"config": args.config, "stats": st, "split": split, "candidates_ms": cand}
+            for name, T in (("forward", f), ("backward", b)):
+                t0 = T[:, 0].min()
+                lev = T[:, 7]
+                ends = np.array([T[lev == l, 2].max() - t0 for l in range(lev.max() + 1)]) / 1e3
+                span = (T[:, 2].max() - t0) / 1e3
+                done = np.maximum.accumulate(ends if name == "forward" else ends[::-1])
+                q = {p: float(done[int(p / 100 * (len(done) - 1))]) for p in (10, 25, 50, 75, 100)}
+                out[name] = {"tasks": int(len(T)), "span_us": float(span), "levels": int(len(ends)),
+                             "done_us_at_level_pct": q,
+                             "work_us_mean": float(np.mean(T[:, 2] - T[:, 1]) / 1e3),
+                             "to_ready_us_mean": float(np.mean(T[:, 1] - T[:, 0]) / 1e3)}
+            print(json.dumps(out))
+            return 0
+        o = g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum, max_steps=args.profile_steps)
+        print(json.dumps({"config": args.config, "stats": st, "rows": len(o.steps), "ms_factor": o.ms_factor,
+                          "n_factor": o.n_factor, "ms_steps": o.ms_steps, "n_solve": o.n_solve,
+                          "ms_per_solve": o.ms_steps / max(o.n_solve, 1), "ms_total": o.ms_total}))
     return 0
 
 
@@ -550,20 +682,35 @@ def main():
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2])
-    ap.add_argument("--sample-steps", type=int, default=0,
-                    help="CPU arm: time steps per sample (0: sp_double - 1, up to the first doubling trial)")
-    ap.add_argument("--cpu-scaled", type=int, default=0,
-                    help="CPU arm: amortise the sample's factorisation over a doubling period")
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3],
+                    help="3: the adjoint measurement of config 3 alone (one JSON object, not a bench line)")
+    ap.add_argument("--sample-steps", type=int, default=0, help="CPU arm: time steps per sample (0: 10)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--adjoint", type=int, default=1, help="1: also time one adjoint gradient (single-RHS configs)")
+    ap.add_argument("--adjoint", type=int, default=1, help="config 1: also time one config-3 adjoint gradient")
     ap.add_argument("--models", type=int, default=16,
-                    help="config 2: also run this many layered models one by one and as one batch")
-    ap.add_argument("--batched-steps", type=int, default=300,
-                    help="config 1: also compare a 64-RHS block with one RHS on the config-2 mesh over these steps")
+                    help="config 1: also run this many layered models one by one and as one batch")
+    ap.add_argument("--batched", type=int, default=1,
+                    help="config 1: also run config 2 (64 loops as one 64-column block) on the same mesh")
+    ap.add_argument("--fd-cells", type=int, default=0,
+                    help="config 3: central differences on this many random cells beside the gradient")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="profiling: run only the first N time steps of the config's model and print phase timings")
+    ap.add_argument("--timeline", action="store_true", help="profiling: one solve with per-task GPU timestamps")
+    ap.add_argument("--rhs", type=int, default=0, help="profiling, config 2: the first RHS loops only (0 = all)")
+    ap.add_argument("--h-core", type=float, default=0.0, help="profiling: core cell size override (m)")
+    ap.add_argument("--replicate", type=int, default=1,
+                    help="profiling: solve the config's loop as this many identical RHS columns")
     args = ap.parse_args()
+    if args.profile_steps > 0 or args.timeline:
+        return profile_run(args)
     if args.impl == "reference":
         return reference_arm(args)
+    if args.config == 3:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({"config": CONFIGS[3]["label"],
+                          "adjoint": adjoint_measure(int(os.environ.get("LOCAL_RANK", "0")), args.fd_cells)}))
+        return 0
     return ours(args)
 
 

@@ -130,8 +130,9 @@ int temf_solve(temf_ctx* ctx, int slot, int nrhs, const double* b, double* x, in
  * - Every call shares the array, so calls whose GPU work overlaps (two
  *   contexts, two threads, two devices' calls are separate arrays) race.
  *   Serialise them.
- * - The call runs on the context's stream and returns after the solve
- *   finished. */
+ * - The call runs on the context's stream and blocks: it synchronises that
+ *   stream and returns after the solve finished, with the status of its
+ *   waits. */
 int temf_solve_noalloc(temf_ctx* ctx, int slot, const double* b_dev, double* x_dev);
 /* Forget the factor in `slot` (pardiso_direct_3, src/FETD_UTILITY.f90:959-975).
  * Device memory is kept for reuse until temf_destroy. */
@@ -212,14 +213,27 @@ int temf_result_timing(temf_ctx* ctx, double* ms_factor, double* ms_steps, doubl
  * receive the candidates.  temf_solve_schedule reports the level in use. */
 int temf_tune_solve(temf_ctx* ctx, int slot, int nrhs, int* split, int* n_cand, int* cand_split, double* cand_ms);
 int temf_solve_schedule(temf_ctx* ctx, int nrhs, int* split, int* tuned);
+/* The single-column sweeps (temf_solve, temf_run) first sweep the bottom of
+ * the supernodal tree as whole subtrees, one warp each: the supernodes below
+ * a subtree level, with no waits; the persistent task sweeps cover the rest.
+ * For nrhs = 1, temf_tune_solve also picks the subtree level (0 = none, or
+ * levels that leave at least one subtree per SM) before the queue split, and
+ * reports the split candidates at the chosen level.  temf_set_solve_plan sets
+ * both explicitly (checked on the host, marked tuned); temf_solve_plan
+ * reports the plan in use and its number of subtrees.  No reference
+ * counterpart. */
+int temf_set_solve_plan(temf_ctx* ctx, int tree_level, int split);
+int temf_solve_plan(temf_ctx* ctx, int* tree_level, int* split, int* n_trees, int* tuned);
 
 /* ---- profiling aid -------------------------------------------------------------
  * No reference counterpart.  One single-column solve (right-hand side all
  * ones) with the factor in slot 1 or 2, recording per task of the persistent
  * sweeps: start, dependency satisfied, end (GPU global timer, ns), SM id,
- * supernode, kind (0 diagonal, 1 row chunk), first row, supernode level --
- * 8 words per task, the n_fwd forward tasks first, then the n_bwd backward
- * ones.  With out = NULL only the counts are returned. */
+ * supernode, kind (0 diagonal, 1 row chunk, 2 a whole subtree swept by one
+ * warp: supernode = its root, first row = its first supernode), first row,
+ * supernode level -- 8 words per task, the n_fwd forward tasks first (forward
+ * subtrees, then tasks), then the n_bwd backward ones (tasks, then
+ * subtrees).  With out = NULL only the counts are returned. */
 int temf_solve_timeline(temf_ctx* ctx, int slot, long long cap, unsigned long long* out, int* n_fwd, int* n_bwd);
 
 /* ---- adjoint gradient --------------------------------------------------------

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 
@@ -42,19 +43,29 @@ struct CtxExtra {
   DBuf<int> shim_map_d;
   DBuf<double> vec;           // scratch vectors for host-facing solves
   DBuf<double*> lb;           // device word holding the factor base for host solves
+  DBuf<int> perm;             // fill-reducing permutation on the device (perm[new] = old)
 };
 
+// Contexts may live on different host threads: the registry is locked.  An
+// entry is created on first use and freed by temf_destroy (drop_extra), so a
+// new context at a reused address starts from a fresh entry.
+std::mutex& registry_lock() {
+  static std::mutex m;
+  return m;
+}
 std::vector<std::pair<temf_ctx*, CtxExtra*>>& registry() {
   static std::vector<std::pair<temf_ctx*, CtxExtra*>> r;
   return r;
 }
 CtxExtra& extra(temf_ctx* c) {
+  std::lock_guard<std::mutex> g(registry_lock());
   for (auto& p : registry())
     if (p.first == c) return *p.second;
   registry().push_back({c, new CtxExtra()});
   return *registry().back().second;
 }
 void drop_extra(temf_ctx* c) {
+  std::lock_guard<std::mutex> g(registry_lock());
   auto& r = registry();
   for (size_t i = 0; i < r.size(); ++i)
     if (r[i].first == c) { delete r[i].second; r.erase(r.begin() + i); return; }
@@ -229,13 +240,7 @@ __global__ void k_permute_out(int n, int nrhs, const int* __restrict__ perm, con
   dst[(int64_t)c * ld + perm[i]] = src[gid];
 }
 
-DBuf<int>& perm_dev(temf_ctx* c) {
-  static std::vector<std::pair<temf_ctx*, DBuf<int>*>> m;
-  for (auto& p : m)
-    if (p.first == c) return *p.second;
-  m.push_back({c, new DBuf<int>()});
-  return *m.back().second;
-}
+DBuf<int>& perm_dev(temf_ctx* c) { return extra(c).perm; }
 
 }  // namespace
 
@@ -840,7 +845,9 @@ int temf_result_mesh_fields(temf_ctx* c, int index, double* fields, int* done) {
     if (done) *done = M.done.size() > (size_t)index ? M.done[index] : 0;
     if (fields) {
       const size_t cnt = 9ULL * c->n_tets;
-      TEMF_CUDA(cudaMemcpy(fields, M.snap.p + cnt * index, cnt * sizeof(double), cudaMemcpyDeviceToHost));
+      TEMF_CUDA(cudaMemcpyAsync(fields, M.snap.p + cnt * index, cnt * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+      TEMF_CUDA(cudaStreamSynchronize(c->stream));
     }
     return TEMF_OK;
   });
@@ -1086,7 +1093,7 @@ int temf_tune_solve(temf_ctx* c, int slot, int nrhs, int* split, int* n_cand, in
       clear_solve_error_flag(*c);
       throw StateError("a triangular-solve wait timed out while tuning (code " + std::to_string(fl) + ")");
     }
-    const QueuePlan& Q = nrhs > 1 ? c->splan.qm : c->splan.q1;
+    const QueuePlan& Q = nrhs > 1 ? c->splan.qm : c->splan.tree.q;
     if (split) *split = best;
     if (n_cand) *n_cand = (int)Q.tune_ms.size();
     for (size_t i = 0; i < Q.tune_ms.size(); ++i) {
@@ -1100,9 +1107,29 @@ int temf_tune_solve(temf_ctx* c, int slot, int nrhs, int* split, int* n_cand, in
 int temf_solve_schedule(temf_ctx* c, int nrhs, int* split, int* tuned) {
   return guarded(c, [&] {
     need(c->analysed, "temf_solve_schedule: call temf_analyse first");
-    const QueuePlan& Q = nrhs > 1 ? c->splan.qm : c->splan.q1;
+    const QueuePlan& Q = nrhs > 1 ? c->splan.qm : c->splan.tree.q;
     if (split) *split = Q.split;
     if (tuned) *tuned = Q.tuned ? 1 : 0;
+    return TEMF_OK;
+  });
+}
+
+int temf_set_solve_plan(temf_ctx* c, int tree_level, int split) {
+  return guarded(c, [&] {
+    need(c->analysed, "temf_set_solve_plan: call temf_analyse first");
+    set_tree_plan(*c, tree_level, split);
+    return TEMF_OK;
+  });
+}
+
+int temf_solve_plan(temf_ctx* c, int* tree_level, int* split, int* n_trees, int* tuned) {
+  return guarded(c, [&] {
+    need(c->analysed, "temf_solve_plan: call temf_analyse first");
+    const TreePlan& T = c->splan.tree;
+    if (tree_level) *tree_level = T.level;
+    if (split) *split = T.q.split;
+    if (n_trees) *n_trees = T.ntree;
+    if (tuned) *tuned = T.tuned ? 1 : 0;
     return TEMF_OK;
   });
 }

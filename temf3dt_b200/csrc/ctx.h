@@ -79,6 +79,24 @@ struct QueuePlan {
   DBuf<int> qbuf;
 };
 
+// Single-column sweeps with the bottom of the tree cut into whole subtrees:
+// the supernodes below `level` form disjoint subtrees (contiguous index ranges
+// [first, root] of the postordered supernodes), each swept by one warp with
+// no waits (k_fwd_subtrees before, k_bwd_subtrees after the task kernels);
+// the task schedules and their ready-queue data cover the supernodes at or
+// above `level` only.  level 0: no subtrees (the full schedules).
+struct TreePlan {
+  int level = 0;
+  int ntree = 0;
+  DBuf<int2> trees;            // (first, root) per subtree, most stored panel values first
+  DBuf<SolveTask> ftask, btask;
+  int n_ftask = 0, n_btask = 0;
+  DBuf<int> ftgt_ptr, ftgt, fexpect, btgt_ptr, btgt;
+  QueuePlan q;
+  bool tuned = false;
+  std::vector<int> tune_level;  // per candidate (level, split) when tuned; splits and times in q
+};
+
 struct SolvePlan {
   int64_t u_len = 0;           // sum over supernodes of the rows below the diagonal block
   // persistent schedules (tasks in an order where every wait targets an earlier task)
@@ -98,6 +116,7 @@ struct SolvePlan {
   DBuf<int64_t> macc_off;      // per supernode with >= 2 chunks: row offset of its c x 64 accumulator
   int64_t macc_len = 0;
   QueuePlan qm;
+  TreePlan tree;               // the single-column sweeps of temf_solve / temf_run
   DBuf<int> sync;              // ready | ydone | cdone | xdone (nsn each) | counters
   int nsn = 0;
 };

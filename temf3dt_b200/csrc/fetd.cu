@@ -248,7 +248,7 @@ struct Engine {
     return ms;
   }
 
-  int64_t solve_launches() const { return solve_launch_count(nrhs); }  // persistent forward + backward kernels
+  int64_t solve_launches() const { return solve_launch_count(c, nrhs); }  // subtree and persistent task kernels
 
   // one BDF2 step: out = A^{-1} (M (4 e2 - e3) - coef * s)
   void step(const double* e2, const double* e3, double* out, const double* coefp, double* const* Lb) {
@@ -441,7 +441,7 @@ struct Engine {
         factor(0, step_cur);
         set_current(0);
         // first solve on this analysis: pick the sweep schedule (once)
-        if (!(nrhs > 1 ? c.splan.qm.tuned : c.splan.q1.tuned)) tune_solve(c, 0, nrhs);
+        if (!(nrhs > 1 ? c.splan.qm.tuned : c.splan.tree.tuned)) tune_solve(c, 0, nrhs);
         N = 0;
         e1 = E(1);
       }

@@ -568,6 +568,247 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_queued(const SweepView V,
 }
 
 // ---------------------------------------------------------------------------
+// The bottom of the tree, whole subtrees per warp (single right-hand side).
+// The supernodes below the tree level form disjoint subtrees, each a
+// contiguous range [first, root] of supernode indices (the nested-dissection
+// order is a postorder of the tree).  One warp sweeps one subtree at a time,
+// supernode by supernode, with no flags and no waits:
+//  * forward (before the task kernels): every contribution to a supernode of
+//    the subtree comes from its descendants, which the same warp has done;
+//  * backward (after them): every row a supernode reads belongs to an
+//    ancestor, done earlier by the same warp or, above the root, finished
+//    when the task kernels ended.
+// Rows inside the subtree (index < first column after the root) have one
+// writer, so the forward sweep updates them with plain read-modify-writes;
+// rows above it receive FP64 atomics (other subtrees add to them too).  Warps
+// order their own accesses with __syncwarp between supernodes.  Panel values
+// are read with coalesced 32-row loads: lane i holds row i of the diagonal
+// block (forward) or column i (backward), and row i of each 32-row chunk.
+// ---------------------------------------------------------------------------
+constexpr int kTreeThreads = 128;  // four warps per CTA, one subtree each
+constexpr unsigned kFull = 0xffffffffu;
+
+// Optional per-subtree timeline (start, end, SM) of the subtree kernels
+// (profiling aid; null unless temf_solve_timeline is running).
+__device__ unsigned long long* g_timeline_tf = nullptr;
+__device__ unsigned long long* g_timeline_tb = nullptr;
+
+struct TreeView {
+  const int2* trees;
+  int ntree;
+  const int* sn_first;
+  const int64_t* rows_ptr;
+  const int* sn_rows;
+  const int64_t* Lptr;
+  double* const* Lbase;
+  double* x;
+  int* counter;
+};
+
+// Sum over the 32 lanes of each of the 32 per-lane values a[0..31]: lane l
+// ends with the sum of a[l] (31 shuffles: each step halves the live values).
+__device__ __forceinline__ double lane_transpose_sum(double a[32]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int k = 0; k < o; ++k) {
+      const double send = up ? a[k] : a[k + o];
+      const double keep = up ? a[k + o] : a[k];
+      a[k] = keep + __shfl_xor_sync(kFull, send, o);
+    }
+  }
+  return a[0];
+}
+
+// forward L y = b for supernode s by one warp; ys: this warp's 64 doubles of shared memory
+__device__ __forceinline__ void fwd_sn_warp(const TreeView& V, const double* Lb, int s, int inside_end, double* ys) {
+  const int lane = threadIdx.x & 31;
+  const int f = V.sn_first[s];
+  const int c = V.sn_first[s + 1] - f;
+  const int64_t rp = V.rows_ptr[s];
+  const int r = (int)(V.rows_ptr[s + 1] - rp);
+  const int64_t ld = c + r;
+  const double* P = Lb + V.Lptr[s];
+  double* x = V.x;
+  const int c0 = min(c, 32);
+  // columns 0..31: lane i holds row i of the diagonal block
+  double a[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) a[j] = (j < lane && lane < c) ? P[(int64_t)j * ld + lane] : 0.0;
+  const double rinv0 = lane < c ? 1.0 / P[(int64_t)lane * ld + lane] : 0.0;
+  double v0 = lane < c ? __ldcg(x + f + lane) : 0.0;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j < c0) {
+      if (lane == j) v0 *= rinv0;
+      const double yj = __shfl_sync(kFull, v0, j);
+      if (lane > j) v0 -= a[j] * yj;
+    }
+  }
+  double v1 = 0.0;
+  if (c > 32) {  // warp-uniform: rows 32..c-1
+    const bool on = 32 + lane < c;
+    v1 = on ? __ldcg(x + f + 32 + lane) : 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) a[j] = on ? P[(int64_t)j * ld + 32 + lane] : 0.0;
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) acc += a[j] * __shfl_sync(kFull, v0, j);
+    v1 -= acc;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) a[m] = (m < lane && on) ? P[(int64_t)(32 + m) * ld + 32 + lane] : 0.0;
+    const double rinv1 = on ? 1.0 / P[(int64_t)(32 + lane) * ld + 32 + lane] : 0.0;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) {
+      if (32 + m < c) {
+        if (lane == m) v1 *= rinv1;
+        const double ym = __shfl_sync(kFull, v1, m);
+        if (lane > m) v1 -= a[m] * ym;
+      }
+    }
+  }
+  if (lane < c) x[f + lane] = v0;
+  if (32 + lane < c) x[f + 32 + lane] = v1;
+  ys[lane] = lane < c ? v0 : 0.0;
+  ys[32 + lane] = 32 + lane < c ? v1 : 0.0;
+  __syncwarp();
+  // rows below the diagonal block, 32 at a time: push -L21 y
+  const int* rows = V.sn_rows + rp;
+  for (int q0 = 0; q0 < r; q0 += 32) {
+    const int i = q0 + lane;
+    if (i < r) {
+      const double* col = P + c + i;
+      double acc0 = 0.0, acc1 = 0.0;
+      for (int h = 0; h < c; h += 32) {  // 32 columns' loads in flight at a time
+        double w[32];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) w[k] = h + k < c ? __ldg(col + (int64_t)(h + k) * ld) : 0.0;
+#pragma unroll
+        for (int k = 0; k < 32; k += 2) {
+          acc0 += w[k] * ys[h + k];
+          acc1 += w[k + 1] * ys[h + k + 1];
+        }
+      }
+      const double acc = acc0 + acc1;
+      const int row = rows[i];
+      if (row < inside_end) x[row] = __ldcg(x + row) - acc;  // one writer: this warp
+      else atomicAdd(x + row, -acc);
+    }
+  }
+  __syncwarp();
+}
+
+// backward L^T x = y for supernode s by one warp
+__device__ __forceinline__ void bwd_sn_warp(const TreeView& V, const double* Lb, int s) {
+  const int lane = threadIdx.x & 31;
+  const int f = V.sn_first[s];
+  const int c = V.sn_first[s + 1] - f;
+  const int64_t rp = V.rows_ptr[s];
+  const int r = (int)(V.rows_ptr[s + 1] - rp);
+  const int64_t ld = c + r;
+  const double* P = Lb + V.Lptr[s];
+  double* x = V.x;
+  const int* rows = V.sn_rows + rp;
+  double v0 = lane < c ? __ldcg(x + f + lane) : 0.0;
+  double v1 = 32 + lane < c ? __ldcg(x + f + 32 + lane) : 0.0;
+  // z_j = y_j - sum_i L21[i][j] x[rows_i], 32 columns at a time
+  double acc[32];
+  for (int h = 0; h * 32 < c; ++h) {
+#pragma unroll
+    for (int k = 0; k < 32; ++k) acc[k] = 0.0;
+    for (int q0 = 0; q0 < r; q0 += 32) {
+      const int i = q0 + lane;
+      const bool on = i < r;
+      const double xi = on ? __ldcg(x + rows[i]) : 0.0;
+      const double* col = P + c + i;
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        const int j = h * 32 + k;
+        acc[k] += (on && j < c) ? __ldg(col + (int64_t)j * ld) * xi : 0.0;
+      }
+    }
+    const double p = lane_transpose_sum(acc);
+    if (h == 0) v0 -= p;
+    else v1 -= p;
+  }
+  // diagonal block, columns c-1 .. 32 (lane m holds column 32 + m)
+  double b[32];
+  if (c > 32) {
+    const bool on = 32 + lane < c;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) b[m] = (m > lane && 32 + m < c && on) ? P[(int64_t)(32 + lane) * ld + 32 + m] : 0.0;
+    const double rinv1 = on ? 1.0 / P[(int64_t)(32 + lane) * ld + 32 + lane] : 0.0;
+#pragma unroll
+    for (int m = 31; m >= 0; --m) {
+      if (32 + m < c) {
+        if (lane == m) v1 *= rinv1;
+        const double xm = __shfl_sync(kFull, v1, m);
+        if (lane < m) v1 -= b[m] * xm;
+      }
+    }
+    // their contribution to columns 0..31 (lane l holds column l)
+#pragma unroll
+    for (int m = 0; m < 32; ++m) b[m] = (32 + m < c && lane < c) ? P[(int64_t)lane * ld + 32 + m] : 0.0;
+    double acc2 = 0.0;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) acc2 += b[m] * __shfl_sync(kFull, v1, m);
+    v0 -= acc2;
+  }
+  // columns min(c,32)-1 .. 0
+  const int c0 = min(c, 32);
+#pragma unroll
+  for (int m = 0; m < 32; ++m) b[m] = (m > lane && m < c0) ? P[(int64_t)lane * ld + m] : 0.0;
+  const double rinv0 = lane < c ? 1.0 / P[(int64_t)lane * ld + lane] : 0.0;
+#pragma unroll
+  for (int m = 31; m >= 0; --m) {
+    if (m < c0) {
+      if (lane == m) v0 *= rinv0;
+      const double xm = __shfl_sync(kFull, v0, m);
+      if (lane < m) v0 -= b[m] * xm;
+    }
+  }
+  if (lane < c) x[f + lane] = v0;
+  if (32 + lane < c) x[f + 32 + lane] = v1;
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(kTreeThreads, 3) k_fwd_subtrees(const TreeView V) {
+  __shared__ double ysm[kTreeThreads / 32][kSnCols];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double* Lb = *V.Lbase;
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(V.counter, 1);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= V.ntree) break;
+    unsigned long long* rec = g_timeline_tf ? g_timeline_tf + 4 * (size_t)t : nullptr;
+    if (rec && lane == 0) rec[0] = gtime();
+    const int2 tr = V.trees[t];
+    const int inside_end = V.sn_first[tr.y + 1];
+    for (int s = tr.x; s <= tr.y; ++s) fwd_sn_warp(V, Lb, s, inside_end, ysm[warp]);
+    if (rec && lane == 0) { rec[1] = rec[0]; rec[2] = gtime(); rec[3] = smid(); }
+  }
+}
+
+__global__ void __launch_bounds__(kTreeThreads, 3) k_bwd_subtrees(const TreeView V) {
+  const int lane = threadIdx.x & 31;
+  const double* Lb = *V.Lbase;
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(V.counter, 1);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= V.ntree) break;
+    unsigned long long* rec = g_timeline_tb ? g_timeline_tb + 4 * (size_t)t : nullptr;
+    if (rec && lane == 0) rec[0] = gtime();
+    const int2 tr = V.trees[t];
+    for (int s = tr.y; s >= tr.x; --s) bwd_sn_warp(V, Lb, s);
+    if (rec && lane == 0) { rec[1] = rec[0]; rec[2] = gtime(); rec[3] = smid(); }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Many models at once (one right-hand side each): the persistent sweeps over
 // the merged task list of all models.  `order` holds (model, task) pairs,
 // each model's tasks in its own dependency order, so every wait still targets
@@ -1072,7 +1313,9 @@ struct Sched {
   std::vector<int64_t> poff;
 };
 
-void build_sched(const Symbolic& S, int CH, Sched& o) {
+// min_level > 0: supernodes below that level (swept by the subtree kernels)
+// get no tasks and feed no counts.
+void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0) {
   const int nsn = S.nsn;
   // distinct owner supernodes of rows [r0, r1) of s (rows ascending -> owners ascending)
   std::vector<int> tmp;
@@ -1094,7 +1337,7 @@ void build_sched(const Symbolic& S, int CH, Sched& o) {
   }
   // forward: bottom-up levels; per supernode its diagonal task (with the first
   // row chunk), then the other chunks
-  for (int l = 0; l < S.nlevels; ++l)
+  for (int l = std::max(0, min_level); l < S.nlevels; ++l)
     for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
       const int s = S.level_sn[q];
       const int r = (int)(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]);
@@ -1108,7 +1351,7 @@ void build_sched(const Symbolic& S, int CH, Sched& o) {
     }
   // backward: top-down levels; per supernode its other chunks, then the
   // diagonal task with the first chunk
-  for (int l = S.nlevels - 1; l >= 0; --l)
+  for (int l = S.nlevels - 1; l >= std::max(0, min_level); --l)
     for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
       const int s = S.level_sn[q];
       const int r = (int)(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]);
@@ -1217,9 +1460,9 @@ void upload_queue_plan(const Sched& a, const Symbolic& S, int split, QueuePlan& 
 // Forward: queue phase, then the ordered phase; backward: the other way
 // round, the ordered tasks' completions feeding the queue.  Returns an empty
 // string or the first violation.
-std::string check_schedule(const Symbolic& S, int CH, int split) {
+std::string check_schedule(const Symbolic& S, int CH, int split, int min_level = 0) {
   Sched a;
-  build_sched(S, CH, a);
+  build_sched(S, CH, a, min_level);
   int f_hi = 0, b_lo = 0;
   split_ranges(a, S, split, f_hi, b_lo);
   QueueData q;
@@ -1298,6 +1541,114 @@ std::string check_schedule(const Symbolic& S, int CH, int split) {
   }
   return std::string();
 }
+
+// Subtrees of the supernodes below `level`: a root is such a supernode whose
+// parent is at or above the level (or that has none); its subtree is the
+// index range [first descendant, root], which the postorder of the supernodes
+// makes contiguous (checked).  Largest stored panels first, so the warps that
+// take the last subtrees finish together.
+std::vector<int2> build_trees(const Symbolic& S, int level) {
+  std::vector<int2> out;
+  if (level <= 0) return out;
+  const int nsn = S.nsn;
+  std::vector<int> first(nsn), cnt(nsn, 1);
+  for (int s = 0; s < nsn; ++s) first[s] = s;
+  for (int s = 0; s < nsn; ++s) {
+    const int p = S.sn_parent[s];
+    if (p < 0) continue;
+    if (p <= s) throw StateError("supernodes are not in postorder (parent before child)");
+    first[p] = std::min(first[p], first[s]);
+    cnt[p] += cnt[s];
+  }
+  std::vector<std::pair<int64_t, int2>> v;
+  for (int s = 0; s < nsn; ++s) {
+    if (S.sn_level[s] >= level) continue;
+    const int p = S.sn_parent[s];
+    if (p >= 0 && S.sn_level[p] < level) continue;
+    if (cnt[s] != s - first[s] + 1) throw StateError("a subtree is not a contiguous supernode range");
+    v.push_back({S.sn_Lptr[s + 1] - S.sn_Lptr[first[s]], make_int2(first[s], s)});
+  }
+  std::stable_sort(v.begin(), v.end(), [](const std::pair<int64_t, int2>& a, const std::pair<int64_t, int2>& b) {
+    return a.first > b.first;
+  });
+  out.reserve(v.size());
+  for (const auto& e : v) out.push_back(e.second);
+  return out;
+}
+
+// Host check of the subtree protocol at `level`: the subtrees cover every
+// supernode below the level exactly once, each supernode's rows are owned by
+// later supernodes, rows owned inside its subtree belong to supernodes of
+// that subtree, and rows above it to supernodes at or above the level (done
+// by the task kernels, never by another subtree).
+std::string check_trees(const Symbolic& S, int level) {
+  std::vector<int2> trees;
+  try {
+    trees = build_trees(S, level);
+  } catch (const std::exception& e) {
+    return e.what();
+  }
+  std::vector<int> seen(S.nsn, 0);
+  for (const int2& t : trees) {
+    const int inside_end = S.sn_first[t.y + 1];
+    for (int s = t.x; s <= t.y; ++s) {
+      if (seen[s]++) return "a supernode in two subtrees";
+      if (S.sn_level[s] >= level) return "a subtree holds a supernode at or above the level";
+      for (int64_t k = S.sn_rows_ptr[s]; k < S.sn_rows_ptr[s + 1]; ++k) {
+        const int row = S.sn_rows[k];
+        const int o = S.col2sn[row];
+        if (o <= s) return "a row owned by an earlier supernode";
+        if (row < inside_end ? (o > t.y) : (S.sn_level[o] < level)) return "a row owned outside the protocol";
+      }
+    }
+  }
+  for (int s = 0; s < S.nsn; ++s)
+    if (S.sn_level[s] < level && !seen[s]) return "a supernode below the level in no subtree";
+  return std::string();
+}
+
+// The single-column plan at a subtree level and queue split.
+void upload_tree_plan(temf_ctx& c, int level, int split) {
+  const Symbolic& S = c.sym;
+  TreePlan& T = c.splan.tree;
+  cudaStream_t st = c.stream;
+  const std::vector<int2> trees = build_trees(S, level);
+  Sched a;
+  build_sched(S, kChunkRows, a, level);
+  T.level = level;
+  T.ntree = (int)trees.size();
+  if (trees.empty()) T.trees.alloc(1);
+  else T.trees.upload(trees.data(), trees.size(), st);
+  T.n_ftask = (int)a.ft.size();
+  T.n_btask = (int)a.bt.size();
+  auto up_tasks = [&](DBuf<SolveTask>& d, const std::vector<SolveTask>& v) {
+    if (v.empty()) d.alloc(1);
+    else d.upload(v.data(), v.size(), st);
+  };
+  up_tasks(T.ftask, a.ft);
+  up_tasks(T.btask, a.bt);
+  T.ftgt_ptr.upload(a.ftp.data(), a.ftp.size(), st);
+  T.ftgt.upload(a.ftg.data(), std::max<size_t>(a.ftg.size(), 1), st);
+  T.fexpect.upload(a.expect.data(), a.expect.size(), st);
+  T.btgt_ptr.upload(a.btp.data(), a.btp.size(), st);
+  T.btgt.upload(a.btg.data(), std::max<size_t>(a.btg.size(), 1), st);
+  upload_queue_plan(a, S, split, T.q, st);  // synchronises: the host vectors go out of scope
+}
+
+// The highest subtree level (up to 11) below which there are still at least
+// min_roots subtrees.  The plan built with the analysis uses two subtrees per
+// resident warp of the subtree kernels (148 SMs x 12 warps).
+int default_tree_level(const Symbolic& S, int min_roots = 2 * 148 * 12) {
+  int best = 0;
+  for (int l = 1; l < std::min(S.nlevels, 12); ++l) {
+    int roots = 0;
+    for (int s = 0; s < S.nsn; ++s)
+      if (S.sn_level[s] < l && (S.sn_parent[s] < 0 || S.sn_level[S.sn_parent[s]] >= l)) ++roots;
+    if (roots < min_roots) break;
+    best = l;
+  }
+  return best;
+}
 }  // namespace
 
 void build_solve_plan(temf_ctx& c) {
@@ -1340,7 +1691,9 @@ void build_solve_plan(temf_ctx& c) {
   P.macc_len = aoff[nsn];
   P.macc_off.upload(aoff.data(), aoff.size(), st);
   upload_queue_plan(b, S, default_split(S), P.qm, st);
-  P.sync.alloc(4 * (size_t)nsn + 4);
+  P.sync.alloc(4 * (size_t)nsn + 8);  // + 2 claim counters of the task kernels, 2 of the subtree kernels
+  upload_tree_plan(c, default_tree_level(S), default_split(S));
+  P.tree.tuned = false;
   TEMF_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -1384,7 +1737,11 @@ static void launch_solve_multi(temf_ctx& c, double* const* Lbase, double* x, int
   }
 }
 
-int solve_launch_count(int nrhs) { return nrhs == 1 ? 2 : 2 * ceil_div(nrhs, kMultiCols); }
+int solve_launch_count(const temf_ctx& c, int nrhs) {
+  if (nrhs > 1) return 2 * ceil_div(nrhs, kMultiCols);
+  const TreePlan& T = c.splan.tree;
+  return (T.ntree ? 2 : 0) + (T.n_ftask ? 1 : 0) + (T.n_btask ? 1 : 0);
+}
 
 // Views of the sweeps through the ready queue: the single-column schedules
 // (q1) or the 64-row ones of the block sweeps (qm, backward accumulators in
@@ -1423,6 +1780,55 @@ static void reset_queues(temf_ctx& c, bool block, cudaStream_t st) {
   TEMF_CUDA(cudaMemcpyAsync(words + 2, Q.qtails.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st));
 }
 
+// Views of the single-column sweeps of the tree plan: its task schedules
+// (the supernodes at or above the subtree level) with their ready queue.
+static void tree_views(temf_ctx& c, double* const* Lbase, double* x, SweepView& vf, SweepView& vb) {
+  FactorPlan& F = c.fplan;
+  SolvePlan& P = c.splan;
+  TreePlan& T = P.tree;
+  QueuePlan& Q = T.q;
+  const int nf = T.n_ftask, nb = T.n_btask;
+  int* q = Q.qbuf.p;
+  int* words = q + (size_t)nf + 2 * (size_t)nb;  // fhead, bhead, ftail, btail
+  vf = SweepView{T.ftask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x, T.ftgt_ptr.p,
+                 T.ftgt.p, T.fexpect.p, nullptr, nullptr, nullptr, P.sync.p, P.nsn, nf,
+                 q, words + 0, words + 2, Q.fdiag.p, nullptr, nullptr, nullptr, nullptr, 0, Q.f_hi};
+  vb = SweepView{T.btask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x, T.btgt_ptr.p,
+                 T.btgt.p, nullptr, P.nchunk.p, P.part_off.p, c.d_part.p, P.sync.p, P.nsn, nb,
+                 q + nf, words + 1, words + 3, Q.bdiag.p, Q.bdep_ptr.p, Q.bdep.p, Q.bneed.p, q + nf + nb,
+                 Q.b_lo, nb};
+}
+
+static void reset_tree_queues(temf_ctx& c, cudaStream_t st) {
+  SolvePlan& P = c.splan;
+  TreePlan& T = P.tree;
+  QueuePlan& Q = T.q;
+  const int nf = T.n_ftask, nb = T.n_btask;
+  int* q = Q.qbuf.p;
+  int* words = q + (size_t)nf + 2 * (size_t)nb;
+  TEMF_CUDA(cudaMemsetAsync(P.sync.p, 0, P.sync.bytes(), st));
+  TEMF_CUDA(cudaMemsetAsync(q, 0, Q.qbuf.bytes(), st));
+  if (Q.n_finit)
+    TEMF_CUDA(cudaMemcpyAsync(q, Q.finit.p, Q.n_finit * sizeof(int), cudaMemcpyDeviceToDevice, st));
+  if (Q.n_binit)
+    TEMF_CUDA(cudaMemcpyAsync(q + nf, Q.binit.p, Q.n_binit * sizeof(int), cudaMemcpyDeviceToDevice, st));
+  TEMF_CUDA(cudaMemcpyAsync(words + 2, Q.qtails.p, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st));
+}
+
+static int tree_grid() {
+  static int g = 0;
+  if (!g) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fwd_subtrees, kTreeThreads, 0);
+    int perb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perb, k_bwd_subtrees, kTreeThreads, 0);
+    g = std::max(1, sms) * std::max(1, std::min(per, perb));
+  }
+  return g;
+}
+
 void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st) {
   SolvePlan& P = c.splan;
   ensure_update_buffer(c, nrhs);
@@ -1430,15 +1836,36 @@ void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaSt
     launch_solve_multi(c, Lbase, x, nrhs, st);
     return;
   }
+  // single column: subtrees (forward), task kernels above the subtree level
+  // (forward, backward), subtrees (backward)
+  TreePlan& T = P.tree;
   SweepView vf, vb;
-  queued_views(c, false, Lbase, x, vf, vb);
-  reset_queues(c, false, st);
-  const int grid = std::min(persistent_grid(k_fwd_queued, 0), std::max(P.n_ftask, 1));
-  k_fwd_queued<<<grid, kSolveThreads, 0, st>>>(vf, c.d_status.p + 1);
-  TEMF_CHECK_LAUNCH();
-  const int gridb = std::min(persistent_grid(k_bwd_queued, 0), std::max(P.n_btask, 1));
-  k_bwd_queued<<<gridb, kSolveThreads, 0, st>>>(vb, c.d_status.p + 1);
-  TEMF_CHECK_LAUNCH();
+  tree_views(c, Lbase, x, vf, vb);
+  reset_tree_queues(c, st);
+  int* tcount = P.sync.p + 4 * (size_t)P.nsn + 4;
+  const int tgrid = std::min(tree_grid(), std::max(1, ceil_div(T.ntree, kTreeThreads / 32)));
+  if (T.ntree) {
+    k_fwd_subtrees<<<tgrid, kTreeThreads, 0, st>>>(TreeView{T.trees.p, T.ntree, c.fplan.sn_first.p,
+                                                            c.fplan.sn_rows_ptr.p, c.fplan.sn_rows.p,
+                                                            c.fplan.sn_Lptr.p, Lbase, x, tcount});
+    TEMF_CHECK_LAUNCH();
+  }
+  if (T.n_ftask) {
+    const int grid = std::min(persistent_grid(k_fwd_queued, 0), T.n_ftask);
+    k_fwd_queued<<<grid, kSolveThreads, 0, st>>>(vf, c.d_status.p + 1);
+    TEMF_CHECK_LAUNCH();
+  }
+  if (T.n_btask) {
+    const int gridb = std::min(persistent_grid(k_bwd_queued, 0), T.n_btask);
+    k_bwd_queued<<<gridb, kSolveThreads, 0, st>>>(vb, c.d_status.p + 1);
+    TEMF_CHECK_LAUNCH();
+  }
+  if (T.ntree) {
+    k_bwd_subtrees<<<tgrid, kTreeThreads, 0, st>>>(TreeView{T.trees.p, T.ntree, c.fplan.sn_first.p,
+                                                            c.fplan.sn_rows_ptr.p, c.fplan.sn_rows.p,
+                                                            c.fplan.sn_Lptr.p, Lbase, x, tcount + 1});
+    TEMF_CHECK_LAUNCH();
+  }
 }
 
 void launch_solve_scratch(temf_ctx& c, double* const* Lbase, double* x, int* sync, double* part, int* err,
@@ -1566,14 +1993,17 @@ void queue_init_lists(const temf_ctx& c, std::vector<int>& finit, std::vector<in
 void solve_timeline(temf_ctx& c, int slot, const double* b_perm, int64_t cap, unsigned long long* out,
                     int* n_fwd, int* n_bwd) {
   SolvePlan& P = c.splan;
-  const int64_t nt = (int64_t)P.n_ftask + P.n_btask;
-  *n_fwd = P.n_ftask;
-  *n_bwd = P.n_btask;
+  TreePlan& T = P.tree;
+  const int nf = T.ntree + T.n_ftask, nb = T.n_btask + T.ntree;
+  const int64_t nt = (int64_t)nf + nb;
+  *n_fwd = nf;
+  *n_bwd = nb;
   if (!out) return;
   if (cap < 8 * nt) throw ArgError("timeline buffer too small: need 8 words per task");
   cudaStream_t st = c.stream;
+  // stamps: forward subtrees, forward tasks, backward tasks, backward subtrees
   DBuf<unsigned long long> rec;
-  rec.alloc(4 * (size_t)nt);
+  rec.alloc(4 * (size_t)std::max<int64_t>(nt, 1));
   TEMF_CUDA(cudaMemsetAsync(rec.p, 0, rec.bytes(), st));
   DBuf<double> x;
   x.upload(b_perm, c.n_edges, st);
@@ -1581,28 +2011,50 @@ void solve_timeline(temf_ctx& c, int slot, const double* b_perm, int64_t cap, un
   lb.alloc(1);
   double* Lp = c.slots[slot].L.p;
   TEMF_CUDA(cudaMemcpyAsync(lb.p, &Lp, sizeof(double*), cudaMemcpyHostToDevice, st));
-  unsigned long long* pf = rec.p;
-  unsigned long long* pb = rec.p + 4 * (size_t)P.n_ftask;
+  unsigned long long* ptf = rec.p;
+  unsigned long long* pf = rec.p + 4 * (size_t)T.ntree;
+  unsigned long long* pb = rec.p + 4 * (size_t)nf;
+  unsigned long long* ptb = rec.p + 4 * ((size_t)nf + T.n_btask);
   unsigned long long* none = nullptr;
   TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_f, &pf, sizeof(pf), 0, cudaMemcpyHostToDevice, st));
   TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_b, &pb, sizeof(pb), 0, cudaMemcpyHostToDevice, st));
+  TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_tf, &ptf, sizeof(ptf), 0, cudaMemcpyHostToDevice, st));
+  TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_tb, &ptb, sizeof(ptb), 0, cudaMemcpyHostToDevice, st));
   launch_solve(c, lb.p, x.p, 1, st);
   TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_f, &none, sizeof(none), 0, cudaMemcpyHostToDevice, st));
   TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_b, &none, sizeof(none), 0, cudaMemcpyHostToDevice, st));
-  std::vector<unsigned long long> h(4 * (size_t)nt);
-  std::vector<SolveTask> tf(P.n_ftask), tb(P.n_btask);
+  TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_tf, &none, sizeof(none), 0, cudaMemcpyHostToDevice, st));
+  TEMF_CUDA(cudaMemcpyToSymbolAsync(g_timeline_tb, &none, sizeof(none), 0, cudaMemcpyHostToDevice, st));
+  std::vector<unsigned long long> h(4 * (size_t)std::max<int64_t>(nt, 1));
+  std::vector<SolveTask> tf(T.n_ftask), tb(T.n_btask);
+  std::vector<int2> tr(T.ntree);
   TEMF_CUDA(cudaMemcpyAsync(h.data(), rec.p, rec.bytes(), cudaMemcpyDeviceToHost, st));
-  TEMF_CUDA(cudaMemcpyAsync(tf.data(), P.ftask.p, tf.size() * sizeof(SolveTask), cudaMemcpyDeviceToHost, st));
-  TEMF_CUDA(cudaMemcpyAsync(tb.data(), P.btask.p, tb.size() * sizeof(SolveTask), cudaMemcpyDeviceToHost, st));
+  if (T.n_ftask)
+    TEMF_CUDA(cudaMemcpyAsync(tf.data(), T.ftask.p, tf.size() * sizeof(SolveTask), cudaMemcpyDeviceToHost, st));
+  if (T.n_btask)
+    TEMF_CUDA(cudaMemcpyAsync(tb.data(), T.btask.p, tb.size() * sizeof(SolveTask), cudaMemcpyDeviceToHost, st));
+  if (T.ntree) TEMF_CUDA(cudaMemcpyAsync(tr.data(), T.trees.p, tr.size() * sizeof(int2), cudaMemcpyDeviceToHost, st));
   TEMF_CUDA(cudaStreamSynchronize(st));
   for (int64_t i = 0; i < nt; ++i) {
-    const SolveTask& T = i < P.n_ftask ? tf[i] : tb[i - P.n_ftask];
+    // which list row i is in, and its task / subtree
+    SolveTask t{0, 0, 0, 0};
+    if (i < T.ntree) {
+      const int2 q = tr[i];
+      t = SolveTask{q.y, 2, q.x, 0};
+    } else if (i < nf) {
+      t = tf[i - T.ntree];
+    } else if (i < nf + T.n_btask) {
+      t = tb[i - nf];
+    } else {
+      const int2 q = tr[i - nf - T.n_btask];
+      t = SolveTask{q.y, 2, q.x, 0};
+    }
     unsigned long long* o = out + 8 * i;
     for (int q = 0; q < 4; ++q) o[q] = h[4 * i + q];
-    o[4] = (unsigned long long)T.s;
-    o[5] = (unsigned long long)T.kind;
-    o[6] = (unsigned long long)T.r0;
-    o[7] = (unsigned long long)c.sym.sn_level[T.s];
+    o[4] = (unsigned long long)t.s;
+    o[5] = (unsigned long long)t.kind;
+    o[6] = (unsigned long long)t.r0;
+    o[7] = (unsigned long long)c.sym.sn_level[t.s];
   }
 }
 
@@ -1639,6 +2091,8 @@ static std::string check_structure(const Symbolic& S) {
   return std::string();
 }
 
+static std::vector<int> split_candidates(const Symbolic& S, int level);
+
 std::string check_schedules(const Symbolic& S) {
   {
     const std::string w = check_structure(S);
@@ -1651,12 +2105,25 @@ std::string check_schedules(const Symbolic& S) {
     w = check_schedule(S, kChunkRowsMulti, sp);
     if (!w.empty()) return "64-row chunks, split " + std::to_string(sp) + ": " + w;
   }
+  // the single-column plans with subtrees: every level the tuner may pick,
+  // the subtree protocol and the task schedules above it at each queue split
+  for (int l = 1; l <= std::max(default_tree_level(S, 148), std::min(S.nlevels, 3)); ++l) {
+    std::string w = check_trees(S, l);
+    if (!w.empty()) return "subtrees below level " + std::to_string(l) + ": " + w;
+    for (int sp : split_candidates(S, l)) {
+      w = check_schedule(S, kChunkRows, sp, l);
+      if (!w.empty()) return "subtree level " + std::to_string(l) + ", split " + std::to_string(sp) + ": " + w;
+    }
+  }
   return std::string();
 }
 
 // Autotuner of the queue split: times one solve (right-hand side all ones,
 // nrhs columns) for each candidate split level and keeps the fastest.
+static int tune_tree(temf_ctx& c, int slot);
+
 int tune_solve(temf_ctx& c, int slot, int nrhs) {
+  if (nrhs == 1) return tune_tree(c, slot);
   const Symbolic& S = c.sym;
   SolvePlan& P = c.splan;
   const bool block = nrhs > 1;
@@ -1710,6 +2177,103 @@ int tune_solve(temf_ctx& c, int slot, int nrhs) {
   upload_queue_plan(a, S, best, Q, st);
   Q.tuned = true;
   return best;
+}
+
+// Candidate queue splits above a subtree level (the level itself: no queue).
+static std::vector<int> split_candidates(const Symbolic& S, int level) {
+  std::vector<int> cand = {level};
+  for (int w : {4096, 1024, 512, 148, 32}) {
+    const int l = level_below_width(S, w);
+    if (l > level) cand.push_back(l);
+  }
+  std::sort(cand.begin(), cand.end());
+  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+  return cand;
+}
+
+// Autotuner of the single-column plan: first the subtree level (0 = none, and
+// the levels below which there are enough subtrees to fill the GPU twice),
+// each with the default queue split, then the queue split at the best level.
+// Times one solve (right-hand side all ones) per candidate, keeps the fastest.
+static int tune_tree(temf_ctx& c, int slot) {
+  const Symbolic& S = c.sym;
+  TreePlan& T = c.splan.tree;
+  cudaStream_t st = c.stream;
+  const size_t vec = (size_t)c.n_edges;
+  DBuf<double> ones, x;
+  std::vector<double> h(vec, 1.0);
+  ones.upload(h.data(), vec, st);
+  x.alloc(vec);
+  DBuf<double*> lb;
+  lb.alloc(1);
+  double* Lp = c.slots[slot].L.p;
+  TEMF_CUDA(cudaMemcpyAsync(lb.p, &Lp, sizeof(double*), cudaMemcpyHostToDevice, st));
+  cudaEvent_t e0, e1;
+  TEMF_CUDA(cudaEventCreate(&e0));
+  TEMF_CUDA(cudaEventCreate(&e1));
+  std::vector<int> lv_c, sp_c;
+  std::vector<double> ms_c;
+  auto time_plan = [&](int level, int split) {
+    upload_tree_plan(c, level, split);
+    double tot = 0.0;
+    for (int rep = 0; rep < 4; ++rep) {
+      TEMF_CUDA(cudaMemcpyAsync(x.p, ones.p, vec * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      TEMF_CUDA(cudaEventRecord(e0, st));
+      launch_solve(c, lb.p, x.p, 1, st);
+      TEMF_CUDA(cudaEventRecord(e1, st));
+      TEMF_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      TEMF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (rep > 0) tot += ms;  // the first solve warms up
+    }
+    lv_c.push_back(level);
+    sp_c.push_back(split);
+    ms_c.push_back(tot / 3.0);
+    return tot / 3.0;
+  };
+  // levels with at least one subtree per SM (resident warps: about 12 per SM)
+  std::vector<int> levels = {0};
+  const int top = default_tree_level(S, 148);
+  for (int l = 2; l <= top; ++l) levels.push_back(l);
+  int best_level = 0, best_split = default_split(S);
+  double best = 1e30;
+  for (int l : levels) {
+    const int sp = std::max(l, default_split(S));
+    const double ms = time_plan(l, sp);
+    if (ms < best) { best = ms; best_level = l; best_split = sp; }
+  }
+  // the split candidates at the chosen level (at most 6, with the one timed above)
+  std::vector<int> sps = {best_split};
+  std::vector<double> sms = {best};
+  for (int sp : split_candidates(S, best_level)) {
+    if (sp == sps[0]) continue;
+    const double ms = time_plan(best_level, sp);
+    sps.push_back(sp);
+    sms.push_back(ms);
+    if (ms < best) { best = ms; best_split = sp; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  upload_tree_plan(c, best_level, best_split);
+  T.q.tune_ms = sms;
+  T.q.tune_split = sps;
+  T.tune_level = lv_c;
+  T.q.tuned = true;
+  T.tuned = true;
+  return best_split;
+}
+
+void set_tree_plan(temf_ctx& c, int level, int split) {
+  const Symbolic& S = c.sym;
+  if (level < 0 || level > S.nlevels) throw ArgError("subtree level out of range");
+  if (split < 0 || split > S.nlevels) throw ArgError("queue split level out of range");
+  if (level > 0) {
+    const std::string w = check_trees(S, level);
+    if (!w.empty()) throw StateError("subtrees below level " + std::to_string(level) + ": " + w);
+  }
+  upload_tree_plan(c, level, split);
+  c.splan.tree.q.tuned = true;
+  c.splan.tree.tuned = true;
 }
 
 }  // namespace temf

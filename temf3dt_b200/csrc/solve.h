@@ -50,7 +50,7 @@ void ensure_update_buffer(temf_ctx& c, int nrhs);
 // (an indirection so captured graphs can follow the factor slot).
 void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st);
 // kernels launch_solve issues for nrhs columns
-int solve_launch_count(int nrhs);
+int solve_launch_count(const temf_ctx& c, int nrhs);
 // Single right-hand side, every scratch word supplied by the caller: `sync`
 // (4*nsn+4 ints, cleared here), `part` (part_len doubles), `err` (one int).
 void launch_solve_scratch(temf_ctx& c, double* const* Lbase, double* x, int* sync, double* part, int* err,
@@ -87,6 +87,9 @@ int models_grid(bool forward);
 // their panels prefetched): times one solve of nrhs columns with the factor
 // in `slot` per candidate and keeps the fastest.  Returns the chosen level.
 int tune_solve(temf_ctx& c, int slot, int nrhs);
+// The single-column plan set explicitly: subtree level (0: none) and queue
+// split level; checked on the host first.
+void set_tree_plan(temf_ctx& c, int level, int split);
 // Profiling aid: one single-column solve of b (permuted order) in `slot` with
 // a per-task timeline (8 words per task; see solve.cu).
 void solve_timeline(temf_ctx& c, int slot, const double* b_perm, int64_t cap, unsigned long long* out,

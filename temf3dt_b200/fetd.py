@@ -312,6 +312,17 @@ class FetdGPU:
         self._ck(self._L.temf_solve_schedule(self._h, nrhs, C.byref(sp), C.byref(tu)), "temf_solve_schedule")
         return sp.value, bool(tu.value)
 
+    def set_solve_plan(self, tree_level: int, split: int) -> None:
+        """Single-column sweep plan: subtree level (0 = no subtrees) and queue split level."""
+        self._ck(self._L.temf_set_solve_plan(self._h, int(tree_level), int(split)), "temf_set_solve_plan")
+
+    def solve_plan(self) -> Dict[str, int]:
+        """The single-column sweep plan in use: subtree level, queue split, subtrees, tuned."""
+        lv, sp, nt, tu = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
+        self._ck(self._L.temf_solve_plan(self._h, C.byref(lv), C.byref(sp), C.byref(nt), C.byref(tu)),
+                 "temf_solve_plan")
+        return {"tree_level": lv.value, "split": sp.value, "n_trees": nt.value, "tuned": bool(tu.value)}
+
     def solve_timeline(self, slot: int):
         """Per-task timeline of one single-column solve (profiling aid):
         (forward, backward) arrays of rows (start_ns, ready_ns, end_ns, sm,

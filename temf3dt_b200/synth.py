@@ -242,16 +242,22 @@ def build_model(kind: str = "halfspace", seed: int = 0, scale: float = 1.0, **kw
         bx, bz = kw.get("block_xy", 100.0), (kw.get("block_top", 100.0), kw.get("block_top", 100.0) + kw.get("block_h", 100.0))
         h = kw.get("h_core", 40.0) / scale
         req = [-bx, bx]
-        if kind == "block":
-            a = kw.get("loop_half", 500.0)
-            req += [-a, a]
-            core = (-a - 2 * h, a + 2 * h)
-        else:
-            n_l = kw.get("n_loops", 8)
-            sp_, a = kw.get("loop_spacing", 40.0), kw.get("loop_half", 25.0)
-            centers = (np.arange(n_l) - (n_l - 1) / 2.0) * sp_
-            req += list(centers - a) + list(centers + a)
-            core = (min(centers) - a - 2 * h, max(centers) + a + 2 * h)
+        # the large square loop (block) and the grid of small loops (multiloop);
+        # with shared_grid both kinds carry the lines of both, so that they
+        # build the same mesh and differ only in sources and receivers
+        shared = kw.get("shared_grid", False)
+        a_big = kw.get("big_loop_half", 500.0) if shared else kw.get("loop_half", 500.0)
+        n_l = kw.get("n_loops", 8)
+        sp_ = kw.get("loop_spacing", 40.0)
+        a_small = kw.get("small_loop_half", 25.0) if shared else kw.get("loop_half", 25.0)
+        centers = (np.arange(n_l) - (n_l - 1) / 2.0) * sp_
+        if kind == "block" or shared:
+            req += [-a_big, a_big]
+            core = (-a_big - 2 * h, a_big + 2 * h)
+        if kind == "multiloop" or shared:
+            req += list(centers - a_small) + list(centers + a_small)
+            if not shared:
+                core = (min(centers) - a_small - 2 * h, max(centers) + a_small + 2 * h)
         xs = graded_axis(req, core, h, half, kw.get("ratio", 1.5), h_min=kw.get("h_min", 4.0))
         ys = xs.copy()
         hz = kw.get("h_z", 20.0) / scale
@@ -266,16 +272,18 @@ def build_model(kind: str = "halfspace", seed: int = 0, scale: float = 1.0, **kw
         nod, tets, tph = hex_to_tets(g, phys)
         kz = int(np.searchsorted(zs, 0.0))
         domains = [(AIR, sig_air, 1.0, 1.0), (EARTH, host, 1.0, 1.0), (EARTH + 1, blk, 1.0, 1.0)]
+        mesh_loop = None
+        if kind == "block" or shared:
+            mesh_loop = staircase_loop(g, kz, lambda x, y: (np.abs(x) < a_big) & (np.abs(y) < a_big))
         if kind == "block":
-            a = kw.get("loop_half", 500.0)
-            loops0 = [staircase_loop(g, kz, lambda x, y: (np.abs(x) < a) & (np.abs(y) < a))]
+            loops0 = [mesh_loop]
             nrec = kw.get("n_receivers", 64)
             xr = (np.arange(nrec) - (nrec - 1) / 2.0) * kw.get("rec_spacing", 20.0)
             rec = [_nudge((x, 0.0, kw.get("rec_z", 2.5)), g) for x in xr]
             rec_rhs = [0] * nrec
         else:
             loops0, rec, rec_rhs = [], [], []
-            n_l = kw.get("n_loops", 8)
+            a = a_small
             for iy, cy in enumerate(centers):
                 for ix, cx in enumerate(centers):
                     loops0.append(staircase_loop(g, kz, lambda x, y, cx=cx, cy=cy:
@@ -307,9 +315,13 @@ def build_model(kind: str = "halfspace", seed: int = 0, scale: float = 1.0, **kw
         domains = [(AIR, sig_air, 1.0, 1.0)] + [(EARTH + i, float(sig_l[i]), 1.0, 1.0) for i in range(nlay)]
     else:
         raise ValueError("unknown model kind %r" % kind)
-    nod2, tets1, new = _renumber_loop_first(nod, tets, loops0[0])
+    if kind not in ("block", "multiloop") or mesh_loop is None:
+        mesh_loop = loops0[0]
+    # the .mesh source (physical 51) is the large loop on a shared grid, so the
+    # block and multiloop kinds then write identical mesh files
+    nod2, tets1, new = _renumber_loop_first(nod, tets, mesh_loop)
     loops = [[int(new[v]) + 1 for v in lp] for lp in loops0]
-    l0 = loops[0]
+    l0 = [int(new[v]) + 1 for v in mesh_loop]
     src = np.array([[l0[i], l0[(i + 1) % len(l0)]] for i in range(len(l0))])
     mesh = Mesh(nod2, tets1, tph, src.astype(np.int64), np.full(len(src), 51, dtype=np.int64))
     ctl = Control()

@@ -126,3 +126,54 @@ def test_adjoint_refuses_unrecorded_and_turn_off_runs(small):
         g.adjoint_record(0)
         g.set_sources([(info["src_edg"], info["src_drc"])], m.ctl.source_type, m.ctl.pulse_type, m.ctl.t0,
                       m.ctl.current)
+
+
+def test_lognormal_cell_model_gradient_matches_finite_differences_on_32_cells():
+    """The config-3 workload at reduced size: the 3-D block model with its 64
+    line receivers, log-normal cell conductivities (median 0.01 S/m, 0.5
+    decades) on the 32 x 32 x 16 grid of 25 x 25 x 12.5 m cells, observations
+    of a seeded 0.1-decade perturbation at 40 gates, J = 1/2 sum of squared
+    dBz/dt gate residuals.  The adjoint gradient against central differences
+    (log sigma +- 1e-3, decisions replayed) on 32 random cells of the grid:
+    1e-4 relative, plus 1e-6 of the largest cell gradient for cells whose
+    gradient is small (their difference quotient carries the rounding of J)."""
+    import bench
+    from temf3dt_b200 import inversion, synth
+    kw = dict(bench.COMMON)
+    kw.update(h_core=200.0, h_z=60.0, ratio=2.5, time_maximum=2e-4)
+    m = synth.build_model("block", seed=3, **kw)
+    md = bench.config3_media(m)
+    gates = np.logspace(-6, np.log10(1.9e-4), 40)
+    args = (m.ctl.sp_division, m.ctl.sp_double, m.ctl.sp_dblesize, m.ctl.time_maximum)
+    with fetd.FetdGPU(0) as g:
+        fetd.load_case(g, m.mesh, m.ctl)
+        g.set_media(md["sig_true"], md["mu"])
+        g.assemble()
+        o = g.run(*args)
+        d_obs = inversion.gate_matrix(o.times, gates) @ o.fields[:, :, 5]
+        assert o.fields.shape[1] == 64
+        g.set_media(md["sig"], md["mu"])
+        g.assemble()
+        g.adjoint_record(50)
+        o = g.run(*args)
+        J, dJ = inversion.dbdt_misfit(o.fields, o.times, gates, d_obs)
+        grad, _, _ = g.adjoint(dJ, md["cell"], md["ncell"])
+        g.adjoint_record(0)
+        assert J > 0 and np.isfinite(grad).all()
+        forced = o.trial_accepted.astype(np.int32)
+        hit = np.unique(md["cell"][md["cell"] >= 0])
+        pick = np.random.default_rng(32).choice(hit, size=32, replace=False)
+        h = 1e-3
+        scale = np.abs(grad).max()
+        for k in pick:
+            Jpm = []
+            for sgn in (1.0, -1.0):
+                sig = md["sig"].copy()
+                sig[md["cell"] == k] *= np.exp(sgn * h)
+                g.set_media(sig, md["mu"])
+                g.assemble()
+                r = g.run(*args, forced=forced)
+                assert np.array_equal(r.steps, o.steps)
+                Jpm.append(inversion.dbdt_misfit(r.fields, r.times, gates, d_obs)[0])
+            fd = (Jpm[0] - Jpm[1]) / (2 * h)
+            assert abs(grad[k] - fd) <= 1e-4 * abs(fd) + 1e-6 * scale, (int(k), grad[k], fd)

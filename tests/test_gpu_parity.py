@@ -96,6 +96,33 @@ def test_tuned_sweep_schedules_solve_to_backward_error(small, nrhs):
     assert rel.max() <= 1e-12, rel.max()
 
 
+@pytest.mark.parametrize("level", [1, 2, 3, 5, 8])
+def test_subtree_sweeps_solve_to_backward_error(small, level):
+    """Single-column solves with the supernodes below `level` swept as whole
+    subtrees (one warp each, no waits) before and after the persistent task
+    sweeps, with and without the ready queue above them: backward error 1e-12,
+    and the same solution as the plan without subtrees to that tolerance."""
+    m, om, g, info = small
+    dt = 1e-6
+    A = 3 * O.full_from_upper(om.B) + 2 * dt * O.full_from_upper(om.C)
+    assert g.factor(1, dt) == 0
+    L = min(level, int(g.stats()["levels"]) - 1)
+    b = A @ np.random.default_rng(level).standard_normal(om.n)
+    nb = np.linalg.norm(b)
+    try:
+        g.set_solve_plan(0, 0)
+        x0 = g.solve(1, b)
+        for split in (L, L + 3):
+            g.set_solve_plan(L, split)
+            plan = g.solve_plan()
+            assert plan["tree_level"] == L and plan["split"] == split and plan["n_trees"] > 0
+            x = g.solve(1, b)
+            assert np.linalg.norm(A @ x - b) <= 1e-12 * nb
+            assert np.linalg.norm(A @ (x - x0)) <= 2e-12 * nb
+    finally:
+        g.tune_solve(1, 1)
+
+
 def test_block_solve_of_many_columns(small):
     """70 right-hand sides: one full 64-column block through the tensor-core
     block sweeps plus a 6-column remainder; every column to backward error

@@ -248,21 +248,55 @@ def test_topology_on_renumbered_mesh_matches_oracle():
 
 
 def test_fortran_interfaces_cover_the_header():
-    """INTEGRATION.md's ISO_C_BINDING module declares every entry point of
-    include/temf_b200.h with the same number of arguments."""
+    """The ISO_C_BINDING module include/temf_b200.f90 declares every entry
+    point of include/temf_b200.h with the same number of arguments, bound to
+    the same C name."""
     with open(os.path.join(ROOT, "include", "temf_b200.h")) as fh:
         txt = re.sub(r"/\*.*?\*/", "", fh.read(), flags=re.S)
     header = {}
     for m in re.finditer(r"\b(temf_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", txt, flags=re.S):
         args = m.group(2).strip()
         header[m.group(1)] = 0 if args in ("", "void") else len(args.split(","))
-    with open(os.path.join(ROOT, "INTEGRATION.md")) as fh:
-        doc = fh.read()
+    with open(os.path.join(ROOT, "include", "temf_b200.f90")) as fh:
+        src = fh.read().replace("&\n", " ")
     fortran = {m.group(1): (0 if not m.group(2).strip() else len(m.group(2).split(",")))
-               for m in re.finditer(r"function (temf_[a-z0-9_]+)\(([^)]*)\)", doc)}
+               for m in re.finditer(r"function (temf_[a-z0-9_]+)\(([^)]*)\)", src)}
+    bound = dict(re.findall(r"function (temf_[a-z0-9_]+)\([^)]*\)\s*bind\(C, name=\"([a-z0-9_]+)\"\)", src))
     assert set(header) <= set(fortran), sorted(set(header) - set(fortran))
     for name, n in header.items():
         assert fortran[name] == n, name
+        assert bound.get(name) == name, name
+    # the status codes match the header's
+    with open(os.path.join(ROOT, "include", "temf_b200.h")) as fh:
+        codes = dict(re.findall(r"#define (TEMF_E[A-Z]+|TEMF_OK) \(?(-?\d+)\)?", fh.read()))
+    for k, v in codes.items():
+        assert re.search(r"\b%s = %s\b" % (k, re.escape(v)), src), k
+
+
+def test_fortran_pardiso_shim_keeps_the_reference_argument_lists():
+    """include/pardiso_temf.f90 is a module named pardiso_multi_real_mpi with
+    the reference's five public subroutines and their argument lists
+    (src/FETD_UTILITY.f90:833-837,861,879,938,959,977), so adap_euler's calls
+    compile unchanged; each forwards to the matching temf_pardiso_* entry."""
+    with open(os.path.join(ROOT, "include", "pardiso_temf.f90")) as fh:
+        src = re.sub(r"&\s*\n\s*", " ", re.sub(r"!.*", "", fh.read()))
+    assert re.search(r"^module pardiso_multi_real_mpi\b", src, flags=re.M)
+    want = {"pardiso_alloc": ["max_matrix"],
+            "pardiso_direct_1": ["num_m", "symm", "n_in", "nnz_in", "ia", "ja", "va", "log"],
+            "pardiso_direct_2": ["num_m", "b_in", "x_out", "ia", "ja", "va"],
+            "pardiso_direct_3": ["num_m"],
+            "pardiso_dealloc": []}
+    subs = {m.group(1): [a.strip() for a in m.group(2).split(",") if a.strip()] if m.group(2) is not None else []
+            for m in re.finditer(r"^\s*subroutine (pardiso_[a-z0-9_]+)(?:\(([^)]*)\))?", src, flags=re.M)}
+    for name, args in want.items():
+        assert subs.get(name) == args, (name, subs.get(name))
+        body = src.split("subroutine %s" % name, 1)[1].split("end subroutine %s" % name, 1)[0]
+        assert "temf_" + name in body, name
+    public = re.search(r"public ::([^\n]*)", src).group(1)
+    for name in want:
+        assert name in public, name
+    # optional log argument, as in the reference
+    assert re.search(r"logical, optional, intent\(in\) :: log", src)
 
 
 @pytest.mark.parametrize("case", ["single", "disconnected", "isolated_and_chain", "coincident_points"])
@@ -299,3 +333,45 @@ def test_single_tet_topology_follows_ind_tet():
     ev, te, td = fetd.mesh_topology(np.array([[1, 2, 3, 4]]))
     assert ev.tolist() == [[1, 2], [1, 3], [1, 4], [2, 3], [2, 4], [3, 4]]
     assert te.tolist() == [[1, 2, 3, 4, 5, 6]] and td.tolist() == [[1, 1, 1, 1, -1, 1]]
+
+
+def test_gate_matrix_follows_the_field2_interpolation():
+    """inversion.gate_matrix reproduces the .field2 gates (interp_lin between
+    the rows that bracket each gate, src/FETD_FWD.f90:1625-1640 and
+    src/FETD_UTILITY.f90:21-31), and dbdt_misfit's derivative matches a
+    finite difference of its misfit."""
+    from temf3dt_b200 import inversion
+    rng = np.random.default_rng(4)
+    times = np.concatenate([[0.0], np.cumsum(rng.uniform(1e-7, 3e-6, 60))])
+    f = rng.standard_normal((len(times), 3, 9))
+    gates = np.sort(rng.uniform(1e-6, times[-1] * 0.99, 12))
+    W = inversion.gate_matrix(times, gates)
+    for g, tg in enumerate(gates):
+        i = int(np.argmax(times >= tg))
+        want = O.interp_lin(times[i - 1], f[i - 1], times[i], f[i], tg)
+        assert np.allclose(np.tensordot(W[g], f, axes=1), want, rtol=1e-12, atol=1e-12)
+    assert (W[:, :].sum(axis=1) == pytest.approx(1.0))
+    late = inversion.gate_matrix(times, [times[-1] * 2])
+    assert not late.any()
+    d_obs = rng.standard_normal((len(gates), 3))
+    J, dJ = inversion.dbdt_misfit(f, times, gates, d_obs)
+    k = (17, 1, 5)
+    h = 1e-6
+    f2 = f.copy()
+    f2[k] += h
+    J2, _ = inversion.dbdt_misfit(f2, times, gates, d_obs)
+    assert abs((J2 - J) / h - dJ[k]) <= 1e-5 * max(1.0, abs(dJ[k]))
+    assert not dJ[:, :, :5].any() and not dJ[:, :, 6:].any()
+
+
+def test_inversion_grid_cells():
+    """Tet -> cell map by centroid on a regular grid (x slowest, z fastest),
+    -1 outside, and the per-cell conductivity it carries."""
+    from temf3dt_b200 import inversion
+    grid = inversion.InversionGrid((4, 3, 2), ((0.0, 4.0), (0.0, 3.0), (0.0, 2.0)))
+    pts = np.array([[0.5, 0.5, 0.5], [3.5, 2.5, 1.5], [1.2, 0.1, 1.9], [-0.1, 1.0, 1.0], [1.0, 1.0, 2.5]])
+    assert grid.cell_of_points(pts).tolist() == [0, 23, 7, -1, -1]
+    sc = inversion.lognormal_cells(grid.ncell, 0.01, 0.5, 3)
+    assert np.allclose(np.median(np.log10(inversion.lognormal_cells(20000, 0.01, 0.5, 3))), -2.0, atol=0.02)
+    sig = inversion.sigma_with_cells(np.full(5, 1e-12), grid.cell_of_points(pts), sc)
+    assert sig[0] == sc[0] and sig[1] == sc[23] and sig[3] == 1e-12
