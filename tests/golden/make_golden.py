@@ -1,7 +1,7 @@
 """Build the golden fixtures under tests/golden/ from the reference checkout.
 
 Run here (where the reference is mounted) with
-    python tests/golden/make_golden.py [--reference PATH] [--oracle]
+    python tests/golden/make_golden.py --reference PATH [--oracle]
 It packs, for each shipped example of the reference, the mesh (.mesh), the
 control file (.cntl, as text) and the shipped output (.field rows) into one
 compressed .npz, so the GPU tests can run the reference's own examples
@@ -62,7 +62,7 @@ def oracle_src_small(max_rows: int = 700) -> str:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the reference checkout")
     ap.add_argument("--oracle", action="store_true")
     a = ap.parse_args()
     for name, rel in CASES.items():
