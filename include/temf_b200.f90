@@ -147,6 +147,9 @@ module temf_b200
       import; type(c_ptr), value :: ctx; integer(c_int) :: tree_level; integer(c_int) :: split
       integer(c_int) :: n_trees; integer(c_int) :: tuned
     end function
+    integer(c_int) function temf_set_wait_limit(ctx, spins, inject_unmet_wait) bind(C, name="temf_set_wait_limit")
+      import; type(c_ptr), value :: ctx; integer(c_int), value :: spins; integer(c_int), value :: inject_unmet_wait
+    end function
     integer(c_int) function temf_solve_timeline(ctx, slot, cap, out, n_fwd, n_bwd) &
         bind(C, name="temf_solve_timeline")
       import; type(c_ptr), value :: ctx; integer(c_int), value :: slot; integer(c_long_long), value :: cap 

@@ -105,7 +105,12 @@ int temf_get_matrix(temf_ctx* ctx, int which, int* nnz, int* ia, int* ja, double
  * src/FETD_FWD.f90:1288,1354) and its numeric LL^T into slot 1 or 2
  * (pardiso_direct_1, src/FETD_UTILITY.f90:879-936).  Returns 0, a negative
  * error, or a positive value = 1-based edge index of the first non-positive
- * pivot (the case in which the reference retries with mtype -2). */
+ * pivot: the case in which the reference retries with mtype -2
+ * (symmetric indefinite, :923-935).  The slot then holds an indefinite
+ * factor A = L S L^T (S = diag(+-1), pivots that cancel below 1e-13 of their
+ * diagonal entry perturbed), and temf_solve runs two steps of iterative
+ * refinement with A.  temf_run stops on such a step matrix (A(dt) is SPD for
+ * dt > 0); temf_solve_noalloc refuses an indefinite slot. */
 int temf_factor(temf_ctx* ctx, int slot, double dt);
 /* x = A^{-1} b with the factor in `slot` (pardiso_direct_2,
  * src/FETD_UTILITY.f90:938-957).  b and x are host arrays of n_edges x nrhs,
@@ -223,6 +228,16 @@ int temf_solve_schedule(temf_ctx* ctx, int nrhs, int* split, int* tuned);
  * reports the plan in use and its number of subtrees.  No reference
  * counterpart. */
 int temf_set_solve_plan(temf_ctx* ctx, int tree_level, int split);
+/* Failure detection of the device waits.  No reference counterpart.  Every
+ * wait of the persistent sweeps on a flag another CTA sets is bounded: after
+ * `spins` polls (0: the default, about a second) it gives up, records which
+ * wait it was in an error word and lets the kernel finish, so the context
+ * stays usable; temf_solve / temf_run then return TEMF_ESTATE ("a
+ * triangular-solve wait timed out (code k)").  inject_unmet_wait = 1 makes
+ * the next single-column solve outside stream capture expect one input more
+ * than any task provides for the last supernode, so that one wait cannot be
+ * met (a test of this path; it is consumed by that solve). */
+int temf_set_wait_limit(temf_ctx* ctx, int spins, int inject_unmet_wait);
 int temf_solve_plan(temf_ctx* ctx, int* tree_level, int* split, int* n_trees, int* tuned);
 
 /* ---- profiling aid -------------------------------------------------------------
@@ -325,7 +340,11 @@ int temf_schedule_check(int n, const long long* xadj, const int* adj, const doub
  * (src/FETD_UTILITY.f90:826-1028) so adap_euler can keep its five calls.
  * direct_1 takes the 1-based upper CSR (ia, ja, va) of A; its pattern must be
  * the assembled step-matrix pattern of the mesh set on the context (the
- * pattern mkl_add_3 produces), which is checked. */
+ * pattern mkl_add_3 produces), which is checked.  A matrix that is not
+ * positive definite is factored in the indefinite mode as with temf_factor;
+ * direct_1 then returns the first non-positive pivot column (> 0), where the
+ * reference prints its "CHANGE TO INDEFINITE MODE" warning, and direct_2
+ * refines its solves. */
 /* pardiso_checker (src/FETD_UTILITY.f90:993-1027), host only: the CSR
  * structure checks the reference asks of MKL's sparse matrix checker (ia(1) =
  * 1, ia(n+1)-1 = nnz, ia non-decreasing, ja in 1..n and strictly ascending per

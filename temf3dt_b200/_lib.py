@@ -58,6 +58,7 @@ SIGNATURES = {
     "temf_solve_schedule": (_i, [_p, _i, _ip, _ip]),
     "temf_set_solve_plan": (_i, [_p, _i, _i]),
     "temf_solve_plan": (_i, [_p, _ip, _ip, _ip, _ip]),
+    "temf_set_wait_limit": (_i, [_p, _i, _i]),
     "temf_schedule_check": (_i, [_i, C.POINTER(C.c_longlong), _ip, _dp, C.c_char_p, _i]),
     "temf_solve_timeline": (_i, [_p, _i, C.c_longlong, C.POINTER(C.c_ulonglong), _ip, _ip]),
     "temf_batch_create": (_i, [C.POINTER(C.c_void_p), _i, C.POINTER(C.c_void_p)]),

@@ -43,6 +43,7 @@ struct CtxExtra {
   DBuf<int> shim_map_d;
   DBuf<double> vec;           // scratch vectors for host-facing solves
   DBuf<double*> lb;           // device word holding the factor base for host solves
+  DBuf<double> shim_full[2];  // PARDISO shim: the user's matrix of each slot on the permuted pattern
   DBuf<int> perm;             // fill-reducing permutation on the device (perm[new] = old)
 };
 
@@ -616,7 +617,7 @@ int temf_factor(temf_ctx* c, int slot, double dt) {
     need(c->assembled, "temf_factor: assemble first");
     if (slot != 1 && slot != 2) throw ArgError("slot must be 1 or 2");
     if (!(dt > 0.0)) throw ArgError("dt must be positive");
-    return numeric_factor(*c, slot - 1, dt);
+    return numeric_factor_values_fallback(*c, slot - 1, c->d_M.p, 3.0, c->d_K.p, 2.0 * dt);
   });
 }
 
@@ -628,11 +629,22 @@ int temf_release(temf_ctx* c, int slot) {
   });
 }
 
+__global__ void k_axpy(int64_t n, const double* __restrict__ d, double* __restrict__ x) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) x[q] += d[q];
+}
+
+// Iterative refinement steps after a solve with an indefinite factor (the
+// reference's PARDISO runs two by default when pivots were perturbed).
+constexpr int kRefineSteps = 2;
+
 static void host_solve(temf_ctx* c, int slot0, int nrhs, const double* b, double* x, int ld) {
   CtxExtra& X = extra(c);
   const int n = c->n_edges;
   const size_t vec = (size_t)n * nrhs;
-  if (X.vec.n < 2 * vec) X.vec.alloc(2 * vec);
+  const FactorSlot& fs = c->slots[slot0];
+  const bool refine = fs.indefinite;
+  if (X.vec.n < (refine ? 4 : 2) * vec) X.vec.alloc((refine ? 4 : 2) * vec);
   double* dcol = X.vec.p;        // column-major staging
   double* drow = X.vec.p + vec;  // permuted row-major
   cudaStream_t st = c->stream;
@@ -641,9 +653,24 @@ static void host_solve(temf_ctx* c, int slot0, int nrhs, const double* b, double
   k_permute_in<<<ceil_div((int64_t)vec, 256), 256, 0, st>>>(n, nrhs, perm_dev(c).p, dcol, n, drow);
   TEMF_CHECK_LAUNCH();
   if (!X.lb.p) X.lb.alloc(1);
-  double* Lp = c->slots[slot0].L.p;
+  double* Lp = fs.L.p;
   TEMF_CUDA(cudaMemcpyAsync(X.lb.p, &Lp, sizeof(double*), cudaMemcpyHostToDevice, st));
-  launch_solve(*c, X.lb.p, drow, nrhs, st);
+  const double* sgn = fs.indefinite ? fs.sgn.p : nullptr;
+  if (refine) {
+    // x = A^-1 b, then x += A^-1 (b - A x), kRefineSteps times
+    double* bp = X.vec.p + 2 * vec;  // b, permuted
+    double* r = X.vec.p + 3 * vec;   // residual, then correction
+    TEMF_CUDA(cudaMemcpyAsync(bp, drow, vec * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    launch_solve(*c, X.lb.p, drow, nrhs, st, sgn);
+    for (int it = 0; it < kRefineSteps; ++it) {
+      launch_residual(*c, fs, drow, bp, r, nrhs, st);
+      launch_solve(*c, X.lb.p, r, nrhs, st, sgn);
+      k_axpy<<<ceil_div((int64_t)vec, 256), 256, 0, st>>>((int64_t)vec, r, drow);
+      TEMF_CHECK_LAUNCH();
+    }
+  } else {
+    launch_solve(*c, X.lb.p, drow, nrhs, st);
+  }
   k_permute_out<<<ceil_div((int64_t)vec, 256), 256, 0, st>>>(n, nrhs, perm_dev(c).p, drow, n, dcol);
   TEMF_CHECK_LAUNCH();
   for (int q = 0; q < nrhs; ++q)
@@ -1114,6 +1141,15 @@ int temf_solve_schedule(temf_ctx* c, int nrhs, int* split, int* tuned) {
   });
 }
 
+int temf_set_wait_limit(temf_ctx* c, int spins, int inject_unmet_wait) {
+  return guarded(c, [&] {
+    if (spins < 0) throw ArgError("temf_set_wait_limit: spins must be >= 0");
+    c->spin_limit = spins;
+    c->inject_wait = inject_unmet_wait ? 1 : 0;
+    return TEMF_OK;
+  });
+}
+
 int temf_set_solve_plan(temf_ctx* c, int tree_level, int split) {
   return guarded(c, [&] {
     need(c->analysed, "temf_set_solve_plan: call temf_analyse first");
@@ -1384,15 +1420,18 @@ int temf_pardiso_direct_1(temf_ctx* c, int num_m, int symm, int n, int nnz, cons
       X.shim_nnz = nnz;
       X.shim_map_d.upload(X.shim_map.data(), X.shim_map.size(), c->stream);
     }
-    // place the user's values in a CSR-shaped buffer, then load them as "M" with dt = 0
+    // place the user's values on the permuted full pattern (kept with the
+    // slot: the refinement of an indefinite factor applies them)
     DBuf<double> uv;
     uv.upload(va, nnz, c->stream);
-    DBuf<double> full;
-    full.alloc(c->pat.nnz);
+    DBuf<double>& full = X.shim_full[num_m - 1];
+    if (full.n < (size_t)c->pat.nnz) full.alloc(c->pat.nnz);
     TEMF_CUDA(cudaMemsetAsync(full.p, 0, c->pat.nnz * sizeof(double), c->stream));
     k_scatter_user<<<ceil_div(nnz, 256), 256, 0, c->stream>>>(nnz, X.shim_map_d.p, uv.p, full.p);
     TEMF_CHECK_LAUNCH();
-    return numeric_factor_values(*c, num_m - 1, full.p, 1.0, full.p, 0.0);
+    // not positive definite: the indefinite mode, as the reference retries with
+    // mtype -2 (src/FETD_UTILITY.f90:923-935); the positive return is its warning
+    return numeric_factor_values_fallback(*c, num_m - 1, full.p, 1.0, nullptr, 0.0);
   });
 }
 

@@ -126,6 +126,15 @@ struct FactorSlot {
   bool valid = false;
   double dt = 0.0;
   int status = 0;
+  // the matrix factored, a X + b Y on the permuted full pattern (device
+  // arrays that outlive the factor: the iterative refinement applies it)
+  const double* X = nullptr;
+  const double* Y = nullptr;
+  double a = 0.0, b = 0.0;
+  // indefinite mode (the reference's mtype -2 retry): A = L S L^T, S = diag(sgn)
+  bool indefinite = false;
+  int perturbed = 0;          // pivots perturbed to +-tau
+  DBuf<double> sgn;           // n, permuted order
 };
 
 struct Source {
@@ -226,4 +235,9 @@ struct temf_ctx {
   temf::AdjointRecord adj;
   temf::MeshFieldPlan mf;
   int u_nrhs = 0;
+  // device waits of the sweeps: iterations before a wait gives up (0: the
+  // default, about a second); inject_wait: the next single-column solve waits
+  // once on a count that nothing completes (failure-detection test)
+  int spin_limit = 0;
+  int inject_wait = 0;
 };

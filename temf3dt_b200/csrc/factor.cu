@@ -37,18 +37,30 @@ __global__ void k_load_A(int64_t n, const int* __restrict__ src, const int64_t* 
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const int p = src[q];
-  L[dst[q]] = a * M[p] + b * K[p];
+  L[dst[q]] = a * M[p] + (K ? b * K[p] : 0.0);
 }
 
 constexpr int kFacThreads = 128;
 
 // Dense Cholesky of the (<= 64 x 64) diagonal block of each supernode of a level.
+//
+// sgn != null: the indefinite mode, A = L S L^T with S = diag(+-1) (sgn, in
+// the permuted order) and L_kk = sqrt(|d_k|) > 0, the sign of the pivot d_k in
+// s_k.  A pivot that cancels below kPivotTol of its column's diagonal entry
+// as the block's elimination starts (or is not finite) is perturbed to that
+// size (static pivot perturbation, counted in status[2]); the iterative
+// refinement of the solves recovers the accuracy.  The first non-positive
+// pivot is recorded in status[0] in both modes.
+constexpr double kPivotTol = 1e-13;
+
 __global__ void __launch_bounds__(kFacThreads) k_potrf(
     const int* __restrict__ level_sn, const int* __restrict__ sn_first,
     const int64_t* __restrict__ rows_ptr, const int64_t* __restrict__ Lptr, double* __restrict__ L,
-    int* __restrict__ status) {
+    int* __restrict__ status, double* __restrict__ sgn) {
   constexpr int CB = kSnCols;
   __shared__ double D[CB][CB + 1];
+  __shared__ double sk[CB];
+  __shared__ double d0[CB];
   const int s = level_sn[blockIdx.x];
   const int f = sn_first[s];
   const int c = sn_first[s + 1] - f;
@@ -61,23 +73,37 @@ __global__ void __launch_bounds__(kFacThreads) k_potrf(
     D[i][j] = (i >= j) ? P[(int64_t)j * ld + i] : 0.0;
   }
   __syncthreads();
+  if (tid < c) d0[tid] = fabs(D[tid][tid]);
+  __syncthreads();
   for (int k = 0; k < c; ++k) {
     if (tid == 0) {
       double d = D[k][k];
-      if (!(d > 0.0)) {  // non-positive or NaN pivot: record and continue with 1
-        atomicMin(status, f + k + 1);
-        d = 1.0;
+      double s = 1.0;
+      if (!(d > 0.0)) atomicMin(status, f + k + 1);  // non-positive or NaN pivot: record
+      if (sgn) {
+        s = d < 0.0 ? -1.0 : 1.0;
+        d = fabs(d);
+        const double tau = kPivotTol * (d0[k] > 0.0 ? d0[k] : 1.0);
+        if (!(d >= tau) || !(d <= 1e300)) {  // cancelled, NaN or infinite pivot: perturb
+          d = tau;
+          atomicAdd(status + 2, 1);
+        }
+        sgn[f + k] = s;
+      } else if (!(d > 0.0)) {
+        d = 1.0;  // continue with 1; the factor is reported invalid
       }
       D[k][k] = sqrt(d);
+      sk[k] = s;
     }
     __syncthreads();
-    const double piv = D[k][k];
+    const double piv = D[k][k] * sk[k];
     for (int i = k + 1 + tid; i < c; i += blockDim.x) D[i][k] /= piv;
     __syncthreads();
     const int m = c - k - 1;
+    const double s = sk[k];
     for (int idx = tid; idx < m * m; idx += blockDim.x) {
       const int jj = k + 1 + idx / m, ii = k + 1 + idx % m;
-      if (ii >= jj) D[ii][jj] -= D[ii][k] * D[jj][k];
+      if (ii >= jj) D[ii][jj] -= D[ii][k] * s * D[jj][k];
     }
     __syncthreads();
   }
@@ -95,10 +121,12 @@ struct TrsmChunk {
 };
 constexpr int kTrsmRows = kFacThreads;
 
+// Indefinite mode (sgn != null): L21 = A21 L11^{-T} S11.
 __global__ void __launch_bounds__(kFacThreads) k_trsm(const TrsmChunk* __restrict__ chunks,
                                                       const int* __restrict__ sn_first,
                                                       const int64_t* __restrict__ rows_ptr,
-                                                      const int64_t* __restrict__ Lptr, double* __restrict__ L) {
+                                                      const int64_t* __restrict__ Lptr, double* __restrict__ L,
+                                                      const double* __restrict__ sgn) {
   constexpr int CB = kSnCols;
   __shared__ double D[CB][CB + 1];
   const TrsmChunk ch = chunks[blockIdx.x];
@@ -128,6 +156,11 @@ __global__ void __launch_bounds__(kFacThreads) k_trsm(const TrsmChunk* __restric
       x[j] = v / D[j][j];
     }
   }
+  if (sgn) {
+#pragma unroll
+    for (int j = 0; j < CB; ++j)
+      if (j < c) x[j] *= sgn[f + j];
+  }
 #pragma unroll
   for (int j = 0; j < CB; ++j)
     if (j < c) P[(int64_t)j * ld + c + i] = x[j];
@@ -154,7 +187,7 @@ __global__ void __launch_bounds__(128) k_update(
     const int64_t* __restrict__ Lptr, const int* __restrict__ row_grp,
     const int* __restrict__ grp_target, const int* __restrict__ grp_jfirst,
     const int64_t* __restrict__ grp_relind, const int* __restrict__ relind, double* __restrict__ L,
-    int use_atomics) {
+    int use_atomics, const double* __restrict__ sgn) {
   extern __shared__ double sm[];
   double* As = sm;                       // [kSnCols][kLdsU]
   double* Bs = sm + kSnCols * kLdsU;     // [kSnCols][kLdsU]
@@ -180,6 +213,13 @@ __global__ void __launch_bounds__(128) k_update(
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
+  if (sgn) {  // indefinite mode: A22 -= L21 S11 L21^T
+    for (int idx = tid; idx < c * kUpdTile; idx += blockDim.x) {
+      const int k = idx / kUpdTile, ii = idx % kUpdTile;
+      As[k * kLdsU + ii] *= sgn[f + k];
+    }
+    __syncthreads();
+  }
   const int warp = tid >> 5, lane = tid & 31;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
   const int g = lane >> 2, q = lane & 3;
@@ -331,14 +371,28 @@ int numeric_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
   return finish_factor(c, slot);
 }
 
+int numeric_factor_values_fallback(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b) {
+  const int st = numeric_factor_values(c, slot, X, a, Y, b);
+  if (st <= 0) return st;
+  // not positive definite: refactor in the indefinite mode (the reference
+  // retries PARDISO with mtype -2, src/FETD_UTILITY.f90:923-935)
+  launch_factor_values(c, slot, X, a, Y, b, true);
+  finish_factor(c, slot);
+  return st;
+}
+
 int finish_factor(temf_ctx& c, int slot) {
   FactorSlot& fs = c.slots[slot];
-  int status = 0;
-  TEMF_CUDA(cudaMemcpyAsync(&status, c.d_status.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  int words[3] = {0, 0, 0};
+  TEMF_CUDA(cudaMemcpyAsync(words, c.d_status.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   TEMF_CUDA(cudaStreamSynchronize(c.stream));
+  const int status = words[0];
+  fs.perturbed = fs.indefinite ? words[2] : 0;
   if (status != INT_MAX) {
-    fs.valid = false;
+    // the first non-positive pivot (original numbering); an indefinite-mode
+    // factor is valid nonetheless
     fs.status = c.sym.perm[status - 1] + 1;
+    fs.valid = fs.indefinite;
     return fs.status;
   }
   fs.valid = true;
@@ -350,15 +404,27 @@ void launch_factor(temf_ctx& c, int slot, double dt) {
   launch_factor_values(c, slot, c.d_M.p, 3.0, c.d_K.p, 2.0 * dt);
 }
 
-void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b) {
+void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b,
+                          bool indefinite) {
   const Symbolic& S = c.sym;
   FactorPlan& F = c.fplan;
   FactorSlot& fs = c.slots[slot];
   cudaStream_t st = c.stream;
   if (fs.L.n < (size_t)S.stored) fs.L.alloc(S.stored);
   TEMF_CUDA(cudaMemsetAsync(fs.L.p, 0, S.stored * sizeof(double), st));
-  int init = INT_MAX;
-  TEMF_CUDA(cudaMemcpyAsync(c.d_status.p, &init, sizeof(int), cudaMemcpyHostToDevice, st));
+  int init[3] = {INT_MAX, 0, 0};
+  TEMF_CUDA(cudaMemcpyAsync(c.d_status.p, &init[0], sizeof(int), cudaMemcpyHostToDevice, st));
+  TEMF_CUDA(cudaMemcpyAsync(c.d_status.p + 2, &init[2], sizeof(int), cudaMemcpyHostToDevice, st));
+  fs.X = X;
+  fs.a = a;
+  fs.Y = Y;
+  fs.b = b;
+  fs.indefinite = indefinite;
+  double* sgn = nullptr;
+  if (indefinite) {
+    if (fs.sgn.n < (size_t)S.n) fs.sgn.alloc(S.n);
+    sgn = fs.sgn.p;
+  }
   if (F.n_a2l) {
     k_load_A<<<ceil_div(F.n_a2l, 256), 256, 0, st>>>(F.n_a2l, F.a2l_src.p, F.a2l_dst.p, X, a, Y, b, fs.L.p);
     TEMF_CHECK_LAUNCH();
@@ -369,13 +435,13 @@ void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
     const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
     if (cnt > 0) {
       k_potrf<<<cnt, kFacThreads, 0, st>>>(F.level_sn.p + S.level_ptr[l], F.sn_first.p, F.sn_rows_ptr.p,
-                                           F.sn_Lptr.p, fs.L.p, c.d_status.p);
+                                           F.sn_Lptr.p, fs.L.p, c.d_status.p, sgn);
       TEMF_CHECK_LAUNCH();
     }
     const int64_t c0 = F.trsm_level_ptr[l], c1 = F.trsm_level_ptr[l + 1];
     if (c1 > c0) {
       k_trsm<<<(unsigned)(c1 - c0), kFacThreads, 0, st>>>(reinterpret_cast<const TrsmChunk*>(F.trsm.p) + c0,
-                                                          F.sn_first.p, F.sn_rows_ptr.p, F.sn_Lptr.p, fs.L.p);
+                                                          F.sn_first.p, F.sn_rows_ptr.p, F.sn_Lptr.p, fs.L.p, sgn);
       TEMF_CHECK_LAUNCH();
     }
     const int64_t t0 = F.tile_level_ptr[l], t1 = F.tile_level_ptr[l + 1];
@@ -384,7 +450,7 @@ void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
       k_update<<<(unsigned)(t1 - t0), 128, upd_smem, st>>>(F.tiles.p + t0, F.sn_first.p, F.sn_rows_ptr.p,
                                                           F.sn_rows.p, F.sn_Lptr.p, F.row_grp.p, F.grp_target.p,
                                                           F.grp_jfirst.p, F.grp_relind.p, F.relind.p, fs.L.p,
-                                                          cnt > 1 ? 1 : 0);
+                                                          cnt > 1 ? 1 : 0, sgn);
       TEMF_CHECK_LAUNCH();
     }
   }

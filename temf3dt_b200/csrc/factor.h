@@ -16,6 +16,13 @@ int numeric_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
 // (finish) wait for the stream and read the pivot status.  Factorisations of
 // different contexts can run concurrently between the two calls.
 void launch_factor(temf_ctx& c, int slot, double dt);
-void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b);
+// indefinite: A = L S L^T with S = diag(+-1) (the reference's mtype -2 retry)
+void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b,
+                          bool indefinite = false);
 int finish_factor(temf_ctx& c, int slot);
+// numeric_factor_values, and when A is not positive definite the indefinite
+// factorisation into the same slot: returns 0 (LL^T) or the first
+// non-positive pivot column (original numbering, 1-based) with a valid
+// indefinite factor.
+int numeric_factor_values_fallback(temf_ctx& c, int slot, const double* X, double a, const double* Y, double b);
 }  // namespace temf

@@ -76,6 +76,8 @@ extern "C" int temf_solve_noalloc(temf_ctx* c, int slot, const double* b_dev, do
     c->err.clear();
     if (slot != 1 && slot != 2) throw ArgError("slot must be 1 or 2");
     if (!c->slots[slot - 1].valid) throw StateError("temf_solve_noalloc: the slot holds no valid factor");
+    if (c->slots[slot - 1].indefinite)
+      throw StateError("temf_solve_noalloc: the slot holds an indefinite factor (refined solves: use temf_solve)");
     if (!b_dev || !x_dev) throw ArgError("temf_solve_noalloc: NULL device pointer");
     const SolvePlan& P = c->splan;
     const int n = c->n_edges;

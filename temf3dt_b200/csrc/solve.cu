@@ -29,7 +29,7 @@ constexpr int kSolveThreads = 128;
 constexpr int kChunkRows = 128;        // rows of a panel handled by one task (= threads per CTA)
 constexpr int kChunkRowsMulti = 64;    // rows per task when solving blocks of right-hand sides
 constexpr int kMultiCols = 64;         // right-hand sides per block
-constexpr int kSpinLimit = 1 << 22;    // bounded waits: ~seconds, then the error flag
+constexpr int kSpinLimit = 1 << 22;    // bounded waits: ~seconds, then the error flag (default)
 
 // Optional per-task timeline of the single-model sweeps (profiling aid; null
 // unless temf_solve_timeline is running): per task start, dependency
@@ -59,11 +59,12 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // kernel).  Polls tightly first, then with a short sleep.  On timeout the
 // error word is set and the wait gives up, so the kernel always terminates;
 // the host reports the error.
-__device__ __forceinline__ void wait_geq(const int* flag, int target, int* err, int code) {
+__device__ __forceinline__ int spin_limit(const SweepView& V) { return V.spin > 0 ? V.spin : kSpinLimit; }
+__device__ __forceinline__ void wait_geq(const int* flag, int target, int* err, int code, int limit) {
   const volatile int* f = flag;
   int it = 0;
   while (*f < target) {
-    if (++it > kSpinLimit) {
+    if (++it > limit) {
       atomicExch(err, code);
       break;
     }
@@ -216,13 +217,13 @@ __device__ __forceinline__ void q_push(const SweepView& V, int task) {
 }
 // thread 0 only: next ready task, or -1 when all ntask tasks are handed out
 // (or a wait timed out: error word set)
-__device__ __forceinline__ int q_pop(int* qhead, const int* queue, int limit, int* err) {
+__device__ __forceinline__ int q_pop(int* qhead, const int* queue, int limit, int* err, int spin) {
   const int idx = atomicAdd(qhead, 1);
   if (idx >= limit) return -1;
   const volatile int* slot = queue + idx;
   int it = 0, v;
   while ((v = *slot) == 0) {
-    if (++it > kSpinLimit) {
+    if (++it > spin) {
       atomicExch(err, 5);
       return -1;
     }
@@ -245,7 +246,7 @@ __device__ __forceinline__ int next_task(const SweepView& V, int* counter, bool 
     if (threadIdx.x == 0) {
       int t = -1;
       if (use_q) {
-        if (V.queue) t = q_pop(V.qhead, V.queue, V.q_hi - V.q_lo, err);
+        if (V.queue) t = q_pop(V.qhead, V.queue, V.q_hi - V.q_lo, err, spin_limit(V));
       } else {
         const bool front = V.queue == nullptr || V.q_lo > 0;  // static tasks before the queue range
         const int lo = front ? 0 : V.q_hi, hi = V.queue == nullptr ? V.ntask : (front ? V.q_lo : V.ntask);
@@ -295,7 +296,7 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
   const bool queued = in_queue(V, t);
   if (T.kind == 0) {
     load_diag_start(D, P, c, ld);
-    if (tid == 0 && !queued) wait_geq(ready + s, V.expect[s], err, 1);
+    if (tid == 0 && !queued) wait_geq(ready + s, V.expect[s], err, 1, spin_limit(V));
     __syncthreads();
     if (stamp && tid == 0) *stamp = gtime();
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) ys[idx] = __ldcg(x + (int64_t)f * nrhs + idx);
@@ -304,7 +305,7 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = ys[idx];
     // y_s is published together with the first chunk's pushes below: one fence for both
   } else {
-    if (tid == 0 && !queued) wait_geq(ydone + s, 1, err, 2);
+    if (tid == 0 && !queued) wait_geq(ydone + s, 1, err, 2, spin_limit(V));
     __syncthreads();
     if (stamp && tid == 0) *stamp = gtime();
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) ys[idx] = __ldcg(x + (int64_t)f * nrhs + idx);
@@ -403,8 +404,8 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
   // the chunk's rows need their owners' x; the diagonal task also its other chunks
   if (!queued) {  // one polling thread per owner (and one for the chunk count)
     const int q0 = V.tgt_ptr[t], nq = V.tgt_ptr[t + 1] - q0;
-    for (int q = tid; q < nq; q += blockDim.x) wait_geq(xdone + V.tgt[q0 + q], 1, err, 3);
-    if (T.kind == 0 && tid == blockDim.x - 1) wait_geq(cdone + s, V.nchunk[s] - (nr > 0 ? 1 : 0), err, 4);
+    for (int q = tid; q < nq; q += blockDim.x) wait_geq(xdone + V.tgt[q0 + q], 1, err, 3, spin_limit(V));
+    if (T.kind == 0 && tid == blockDim.x - 1) wait_geq(cdone + s, V.nchunk[s] - (nr > 0 ? 1 : 0), err, 4, spin_limit(V));
   }
   __syncthreads();
   if (stamp && tid == 0) *stamp = gtime();
@@ -821,14 +822,14 @@ __global__ void __launch_bounds__(kTreeThreads, 3) k_bwd_subtrees(const TreeView
 __device__ __forceinline__ int2 next_model_task(int nstatic, const int2* __restrict__ order,
                                                 const int* __restrict__ active, int* counter, int* qhead,
                                                 const int* queue, int qlim, bool queue_first, int* err, int& phase,
-                                                int2* sh) {
+                                                int2* sh, int spin) {
   for (;;) {
     const bool use_q = (phase == 0) == queue_first;
     if (threadIdx.x == 0) {
       int2 r = make_int2(-1, -1);
       if (use_q) {
         if (queue) {
-          const int v = q_pop(qhead, queue, qlim, err);
+          const int v = q_pop(qhead, queue, qlim, err, spin);
           if (v >= 0) r = make_int2(v >> 24, v & 0xFFFFFF);
         }
       } else {
@@ -865,7 +866,7 @@ __global__ void __launch_bounds__(kSolveThreads, 3) k_fwd_models(int nstatic, co
   int phase = 0;
   for (;;) {
     const int2 mt = next_model_task(nstatic, order, active, counter, V0.qhead, V0.queue, qlim, true, err, phase,
-                                    &mt_sh);
+                                    &mt_sh, spin_limit(V0));
     if (mt.x < 0) break;
     const SweepView V = views[mt.x];
     fwd_task(V, mt.y, *V.Lbase, 1, err, D, rinv, ys);
@@ -885,7 +886,7 @@ __global__ void __launch_bounds__(kSolveThreads, 3) k_bwd_models(int nstatic, co
   int phase = 0;
   for (;;) {
     const int2 mt = next_model_task(nstatic, order, active, counter, V0.qhead, V0.queue, qlim, false, err, phase,
-                                    &mt_sh);
+                                    &mt_sh, spin_limit(V0));
     if (mt.x < 0) break;
     const SweepView V = views[mt.x];
     bwd_task(V, mt.y, *V.Lbase, 1, err, D, rinv, seg, zs);
@@ -1055,8 +1056,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_multi(const SweepView V, 
     if (nr > 0) load_panel_block_async(M.A, P, c, ld, T.r0, nr);
     if (T.kind == 0) load_diag_async(M.D, P, c, ld);
     if (tid == 0 && !in_queue(V, t)) {  // claimed in order: wait for the inputs
-      if (T.kind == 0) wait_geq(ready + s, V.expect[s], err, 1);
-      else wait_geq(ydone + s, 1, err, 2);
+      if (T.kind == 0) wait_geq(ready + s, V.expect[s], err, 1, spin_limit(V));
+      else wait_geq(ydone + s, 1, err, 2, spin_limit(V));
     }
     __syncthreads();
     load_rows<true>(M.Y, x, ldx, k, c, f, nullptr);
@@ -1128,8 +1129,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(const SweepView V, 
     if (T.kind == 0) load_diag_async(M.D, P, c, ld);
     if (!in_queue(V, t)) {  // claimed in order: wait for the inputs, one polling thread each
       const int q0 = V.tgt_ptr[t], nq = V.tgt_ptr[t + 1] - q0;
-      for (int q = tid; q < nq; q += blockDim.x) wait_geq(xdone + V.tgt[q0 + q], 1, err, 3);
-      if (T.kind == 0 && tid == blockDim.x - 1) wait_geq(cdone + s, max(V.nchunk[s], 1) - 1, err, 4);
+      for (int q = tid; q < nq; q += blockDim.x) wait_geq(xdone + V.tgt[q0 + q], 1, err, 3, spin_limit(V));
+      if (T.kind == 0 && tid == blockDim.x - 1) wait_geq(cdone + s, max(V.nchunk[s], 1) - 1, err, 4, spin_limit(V));
     }
     __syncthreads();
     // Xr = x[rows] (64 x k); C = L21[rows]^T Xr (c x k)
@@ -1239,6 +1240,8 @@ __global__ void k_spmv_multi(int n, int nrhs, const int* __restrict__ rowptr, co
   for (int p = rowptr[row]; p < rowptr[row + 1]; ++p) acc += M[p] * x[(int64_t)col[p] * nrhs + cc];
   y[gid] = acc;
 }
+
+__global__ void k_add_int(int* p, int d) { *p += d; }
 
 __global__ void k_source(int nent, const int* __restrict__ idx, const int* __restrict__ rcol,
                          const double* __restrict__ coef, const double* __restrict__ scal, int nrhs,
@@ -1717,7 +1720,10 @@ static int persistent_grid(K kernel, size_t smem) {
 static void queued_views(temf_ctx& c, bool block, double* const* Lbase, double* x, SweepView& vf, SweepView& vb);
 static void reset_queues(temf_ctx& c, bool block, cudaStream_t st);
 
-static void launch_solve_multi(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st) {
+static void scale_rows(temf_ctx& c, const double* sgn, double* x, int ld, int ncol, cudaStream_t st);
+
+static void launch_solve_multi(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st,
+                               const double* sgn) {
   SolvePlan& P = c.splan;
   const size_t smem = sizeof(MultiSmem);
   TEMF_CUDA(cudaFuncSetAttribute(k_fwd_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1731,6 +1737,7 @@ static void launch_solve_multi(temf_ctx& c, double* const* Lbase, double* x, int
     reset_queues(c, true, st);
     k_fwd_multi<<<gridf, kSolveThreads, smem, st>>>(vf, nrhs, k, c.d_status.p + 1);
     TEMF_CHECK_LAUNCH();
+    if (sgn) scale_rows(c, sgn, x + c0, nrhs, k, st);  // indefinite factor: L S L^T
     TEMF_CUDA(cudaMemsetAsync(c.d_part.p, 0, (size_t)std::max<int64_t>(P.macc_len, 1) * kMultiCols * sizeof(double), st));
     k_bwd_multi<<<gridb, kSolveThreads, smem, st>>>(vb, nrhs, k, c.d_status.p + 1);
     TEMF_CHECK_LAUNCH();
@@ -1756,12 +1763,13 @@ static void queued_views(temf_ctx& c, bool block, double* const* Lbase, double* 
   vf = SweepView{block ? P.mftask.p : P.ftask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x,
                  block ? P.mftgt_ptr.p : P.ftgt_ptr.p, block ? P.mftgt.p : P.ftgt.p,
                  block ? P.mfexpect.p : P.fexpect.p, nullptr, nullptr, nullptr, P.sync.p, P.nsn, nf,
-                 q, words + 0, words + 2, Q.fdiag.p, nullptr, nullptr, nullptr, nullptr, 0, Q.f_hi};
+                 q, words + 0, words + 2, Q.fdiag.p, nullptr, nullptr, nullptr, nullptr, 0, Q.f_hi, 0,
+                 c.spin_limit};
   vb = SweepView{block ? P.mbtask.p : P.btask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x,
                  block ? P.mbtgt_ptr.p : P.btgt_ptr.p, block ? P.mbtgt.p : P.btgt.p, nullptr,
                  block ? P.mnchunk.p : P.nchunk.p, block ? P.macc_off.p : P.part_off.p, c.d_part.p, P.sync.p, P.nsn,
                  nb, q + nf, words + 1, words + 3, Q.bdiag.p, Q.bdep_ptr.p, Q.bdep.p, Q.bneed.p, q + nf + nb,
-                 Q.b_lo, nb};
+                 Q.b_lo, nb, 0, c.spin_limit};
 }
 
 // clear the sweep words and seed both queues with their initially ready tasks
@@ -1792,11 +1800,12 @@ static void tree_views(temf_ctx& c, double* const* Lbase, double* x, SweepView& 
   int* words = q + (size_t)nf + 2 * (size_t)nb;  // fhead, bhead, ftail, btail
   vf = SweepView{T.ftask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x, T.ftgt_ptr.p,
                  T.ftgt.p, T.fexpect.p, nullptr, nullptr, nullptr, P.sync.p, P.nsn, nf,
-                 q, words + 0, words + 2, Q.fdiag.p, nullptr, nullptr, nullptr, nullptr, 0, Q.f_hi};
+                 q, words + 0, words + 2, Q.fdiag.p, nullptr, nullptr, nullptr, nullptr, 0, Q.f_hi, 0,
+                 c.spin_limit};
   vb = SweepView{T.btask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x, T.btgt_ptr.p,
                  T.btgt.p, nullptr, P.nchunk.p, P.part_off.p, c.d_part.p, P.sync.p, P.nsn, nb,
                  q + nf, words + 1, words + 3, Q.bdiag.p, Q.bdep_ptr.p, Q.bdep.p, Q.bneed.p, q + nf + nb,
-                 Q.b_lo, nb};
+                 Q.b_lo, nb, 0, c.spin_limit};
 }
 
 static void reset_tree_queues(temf_ctx& c, cudaStream_t st) {
@@ -1829,11 +1838,46 @@ static int tree_grid() {
   return g;
 }
 
-void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st) {
+// x[i * ld + k] *= sgn[i] for the k < ncol columns of a row-major block
+__global__ void k_scale_rows(int64_t n, int ld, int ncol, const double* __restrict__ sgn, double* __restrict__ x) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n * ncol) x[(q / ncol) * ld + q % ncol] *= sgn[q / ncol];
+}
+
+static void scale_rows(temf_ctx& c, const double* sgn, double* x, int ld, int ncol, cudaStream_t st) {
+  const int64_t n = c.pat.n;
+  k_scale_rows<<<ceil_div(n * ncol, 256), 256, 0, st>>>(n, ld, ncol, sgn, x);
+  TEMF_CHECK_LAUNCH();
+}
+
+// r = b - (a X + b2 Y) x on the permuted full pattern, nrhs columns (row-major)
+__global__ void k_residual(int n, int nrhs, const int* __restrict__ rowptr, const int* __restrict__ col,
+                           const double* __restrict__ X, double a, const double* __restrict__ Y, double b2,
+                           const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ r) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (int64_t)n * nrhs) return;
+  const int i = (int)(q / nrhs), k = (int)(q % nrhs);
+  double acc = 0.0;
+  for (int p = rowptr[i]; p < rowptr[i + 1]; ++p) {
+    const double v = a * X[p] + (Y ? b2 * Y[p] : 0.0);
+    acc += v * x[(int64_t)col[p] * nrhs + k];
+  }
+  r[q] = b[q] - acc;
+}
+
+void launch_residual(temf_ctx& c, const FactorSlot& fs, const double* x, const double* b, double* r, int nrhs,
+                     cudaStream_t st) {
+  const int n = c.pat.n;
+  k_residual<<<ceil_div((int64_t)n * nrhs, 256), 256, 0, st>>>(n, nrhs, c.d_rowptr.p, c.d_col.p, fs.X, fs.a,
+                                                               fs.Y, fs.b, x, b, r);
+  TEMF_CHECK_LAUNCH();
+}
+
+void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st, const double* sgn) {
   SolvePlan& P = c.splan;
   ensure_update_buffer(c, nrhs);
   if (nrhs > 1) {
-    launch_solve_multi(c, Lbase, x, nrhs, st);
+    launch_solve_multi(c, Lbase, x, nrhs, st, sgn);
     return;
   }
   // single column: subtrees (forward), task kernels above the subtree level
@@ -1842,6 +1886,17 @@ void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaSt
   SweepView vf, vb;
   tree_views(c, Lbase, x, vf, vb);
   reset_tree_queues(c, st);
+  // failure-detection test: one more input expected for the last supernode
+  // than any task provides, so its wait (or its queue slot) runs out
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  TEMF_CUDA(cudaStreamIsCapturing(st, &cap));
+  const bool inject = c.inject_wait && T.n_ftask > 0 && cap == cudaStreamCaptureStatusNone;
+  int* inject_word = inject ? T.fexpect.p + (P.nsn - 1) : nullptr;
+  if (inject) {
+    c.inject_wait = 0;
+    k_add_int<<<1, 1, 0, st>>>(inject_word, 1);
+    TEMF_CHECK_LAUNCH();
+  }
   int* tcount = P.sync.p + 4 * (size_t)P.nsn + 4;
   const int tgrid = std::min(tree_grid(), std::max(1, ceil_div(T.ntree, kTreeThreads / 32)));
   if (T.ntree) {
@@ -1855,6 +1910,11 @@ void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaSt
     k_fwd_queued<<<grid, kSolveThreads, 0, st>>>(vf, c.d_status.p + 1);
     TEMF_CHECK_LAUNCH();
   }
+  if (inject) {
+    k_add_int<<<1, 1, 0, st>>>(inject_word, -1);
+    TEMF_CHECK_LAUNCH();
+  }
+  if (sgn) scale_rows(c, sgn, x, 1, 1, st);  // indefinite factor: L S L^T
   if (T.n_btask) {
     const int gridb = std::min(persistent_grid(k_bwd_queued, 0), T.n_btask);
     k_bwd_queued<<<gridb, kSolveThreads, 0, st>>>(vb, c.d_status.p + 1);
@@ -1944,16 +2004,20 @@ void launch_two_error(temf_ctx& c, const double* a, const double* b, int nrhs, d
 SweepView fwd_view(temf_ctx& c, double* const* Lbase, double* x, int* sync) {
   FactorPlan& F = c.fplan;
   SolvePlan& P = c.splan;
-  return SweepView{P.ftask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x, P.ftgt_ptr.p,
-                   P.ftgt.p, P.fexpect.p, nullptr, nullptr, nullptr, sync, P.nsn, P.n_ftask};
+  SweepView v{P.ftask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x, P.ftgt_ptr.p,
+              P.ftgt.p, P.fexpect.p, nullptr, nullptr, nullptr, sync, P.nsn, P.n_ftask};
+  v.spin = c.spin_limit;
+  return v;
 }
 
 SweepView bwd_view(temf_ctx& c, double* const* Lbase, double* x, int* sync) {
   FactorPlan& F = c.fplan;
   SolvePlan& P = c.splan;
   ensure_update_buffer(c, 1);
-  return SweepView{P.btask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x, P.btgt_ptr.p,
-                   P.btgt.p, nullptr, P.nchunk.p, P.part_off.p, c.d_part.p, sync, P.nsn, P.n_btask};
+  SweepView v{P.btask.p, F.sn_first.p, F.sn_rows_ptr.p, F.sn_rows.p, F.sn_Lptr.p, Lbase, x, P.btgt_ptr.p,
+              P.btgt.p, nullptr, P.nchunk.p, P.part_off.p, c.d_part.p, sync, P.nsn, P.n_btask};
+  v.spin = c.spin_limit;
+  return v;
 }
 
 int models_grid(bool forward) {

@@ -36,6 +36,7 @@ struct SweepView {
   int* cnt;                // backward: per task, completions so far
   int q_lo, q_hi;          // tasks [q_lo, q_hi) go through the queue, the rest are claimed in order
   int tag;                 // model id << 24 when several models share one queue (0 otherwise)
+  int spin = 0;            // iterations a device wait may spin before it gives up (0: the default)
 };
 
 void build_solve_plan(temf_ctx& c);
@@ -48,7 +49,13 @@ void ensure_update_buffer(temf_ctx& c, int nrhs);
 // x (device, permuted order, row-major n x nrhs) is overwritten: b -> A^{-1} b.
 // `Lbase` points at a device word holding the panel base of the factor to use
 // (an indirection so captured graphs can follow the factor slot).
-void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st);
+// sgn != null: the factor is indefinite, L S L^T with S = diag(sgn) (applied
+// between the sweeps).
+void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaStream_t st,
+                  const double* sgn = nullptr);
+// r = b - A x for the matrix factored in fs (permuted order, nrhs columns row-major)
+void launch_residual(temf_ctx& c, const FactorSlot& fs, const double* x, const double* b, double* r, int nrhs,
+                     cudaStream_t st);
 // kernels launch_solve issues for nrhs columns
 int solve_launch_count(const temf_ctx& c, int nrhs);
 // Single right-hand side, every scratch word supplied by the caller: `sync`

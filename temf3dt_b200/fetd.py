@@ -316,6 +316,13 @@ class FetdGPU:
         """Single-column sweep plan: subtree level (0 = no subtrees) and queue split level."""
         self._ck(self._L.temf_set_solve_plan(self._h, int(tree_level), int(split)), "temf_set_solve_plan")
 
+    def set_wait_limit(self, spins: int = 0, inject_unmet_wait: bool = False) -> None:
+        """Polls a device wait may spin before it gives up (0: the default);
+        inject_unmet_wait: the next single-column solve waits once on a count
+        nothing completes (tests the timeout path)."""
+        self._ck(self._L.temf_set_wait_limit(self._h, int(spins), 1 if inject_unmet_wait else 0),
+                 "temf_set_wait_limit")
+
     def solve_plan(self) -> Dict[str, int]:
         """The single-column sweep plan in use: subtree level, queue split, subtrees, tuned."""
         lv, sp, nt, tu = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)

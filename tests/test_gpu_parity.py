@@ -311,6 +311,52 @@ def test_pardiso_shim_and_pivot_status(small):
     g.pardiso_dealloc()
 
 
+@pytest.mark.parametrize("case", ["one_negative_pivot", "shifted"])
+def test_pardiso_indefinite_fallback(small, case):
+    """A matrix that is not positive definite: pardiso_direct_1 reports the
+    first non-positive pivot (the reference's warning before it retries with
+    mtype -2, src/FETD_UTILITY.f90:923-935) and factors it in the indefinite
+    mode (L S L^T, S = diag(+-1), static pivot perturbation); pardiso_direct_2
+    with two refinement steps solves it to backward error 1e-10 and agrees
+    with SuperLU (pivoting LU) on the same matrix.  Cases: one planted
+    negative diagonal entry, and 3 M - 2 dt K with dt = 2e-6 (many negative
+    eigenvalues).  The other slot and the next SPD factorisation stay usable."""
+    import scipy.sparse.linalg as spla
+    m, om, g, info = small
+    if case == "one_negative_pivot":
+        A = (3 * om.B + 2 * 1e-6 * om.C).tocsr()
+    else:
+        A = (3 * om.B - 2 * 2e-6 * om.C).tocsr()
+    A.sort_indices()
+    ia, ja, va = A.indptr + 1, A.indices + 1, A.data.copy()
+    if case == "one_negative_pivot":
+        diag = np.nonzero(ja - 1 == np.repeat(np.arange(om.n), np.diff(A.indptr)))[0]
+        va[diag[17]] = -abs(va[diag[17]])
+    Au = sp.csr_matrix((va, ja - 1, ia - 1), shape=(om.n, om.n))
+    Af = O.full_from_upper(Au)
+    g.pardiso_alloc(2)
+    try:
+        st = g.pardiso_direct_1(2, ia, ja, va)
+        assert st > 0
+        rng = np.random.default_rng(23)
+        b = Af @ rng.standard_normal(om.n)
+        x = g.pardiso_direct_2(2, b)
+        nb = np.linalg.norm(b)
+        assert np.linalg.norm(Af @ x - b) <= 1e-10 * nb
+        ref = spla.splu(Af.tocsc()).solve(b)
+        assert np.linalg.norm(Af @ (x - ref)) <= 2e-10 * nb
+        # an SPD matrix in the other slot, then again in this one
+        As = (3 * om.B + 2 * 1e-6 * om.C).tocsr()
+        As.sort_indices()
+        for slot in (1, 2):
+            assert g.pardiso_direct_1(slot, As.indptr + 1, As.indices + 1, As.data) == 0
+            Asf = O.full_from_upper(As)
+            y = g.pardiso_direct_2(slot, Asf @ np.ones(om.n))
+            assert np.linalg.norm(Asf @ y - Asf @ np.ones(om.n)) <= 1e-12 * np.linalg.norm(Asf @ np.ones(om.n))
+    finally:
+        g.pardiso_dealloc()
+
+
 def test_halfspace_central_loop_matches_analytic_response():
     """dBz/dt at the centre of a 500 m loop on a 0.001 S/m half-space against
     the closed-form response (Ward & Hohmann eq. 4.98) convolved with the erf
@@ -332,3 +378,27 @@ def test_halfspace_central_loop_matches_analytic_response():
     ana = erf_step_on_dbzdt(gates, 1e-3, a_eff, m.ctl.t0)
     rel = np.abs(v[:, 0, 5] - ana) / np.abs(ana)
     assert rel.max() <= 0.02, rel
+
+
+def test_device_wait_timeout_is_reported_and_the_context_recovers(small):
+    """A device wait that can never be met (one input more expected than any
+    task provides) gives up after the context's spin limit: the kernel
+    finishes, temf_solve reports the timeout, and the next solve on the same
+    context is correct (failure detection without a GPU fault)."""
+    m, om, g, info = small
+    dt = 1e-6
+    A = 3 * O.full_from_upper(om.B) + 2 * dt * O.full_from_upper(om.C)
+    assert g.factor(1, dt) == 0
+    b = A @ np.random.default_rng(9).standard_normal(om.n)
+    try:
+        for split in (0, int(g.stats()["levels"])):   # the wait claimed in order, then the queue slot
+            g.set_solve_plan(2, split)
+            g.set_wait_limit(1 << 12, inject_unmet_wait=True)
+            with pytest.raises(RuntimeError, match="timed out"):
+                g.solve(1, b)
+            g.set_wait_limit(0)
+            x = g.solve(1, b)
+            assert np.linalg.norm(A @ x - b) <= 1e-12 * np.linalg.norm(b)
+    finally:
+        g.set_wait_limit(0)
+        g.tune_solve(1, 1)
