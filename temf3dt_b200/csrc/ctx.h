@@ -22,11 +22,14 @@ struct Pattern {
 };
 
 // One entry of the factor update schedule: a 64x64 tile (rows i0.., cols j0..)
-// of the Schur update L21 * L21^T of supernode s (indices into its row list).
+// of the Schur update L21 * L21^T of supernode s (indices into its row list),
+// summed over the m = mj & 15 supernodes s-m+1 .. s (a run of column blocks
+// of one wider supernode), restricted to columns j < mj >> 4 when that is > 0.
 struct UpdTile {
   int s;
   int i0;
   int j0;
+  int mj;
 };
 
 struct FactorPlan {
@@ -50,6 +53,7 @@ struct FactorPlan {
   int64_t n_trsm = 0;
   int64_t n_relind = 0;
   int64_t n_tiles = 0;
+  int n_runs = 0;              // runs of column blocks whose updates are summed
 };
 
 // A task of the persistent triangular-solve kernels: the diagonal block of

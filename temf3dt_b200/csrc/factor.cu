@@ -181,6 +181,20 @@ __device__ __forceinline__ void cp_async8_f(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
 
+// Schur update tiles.  A tile (s, i0, j0, members m, column limit jl) holds
+// C = sum over the m supernodes q = s-m+1 .. s of L21_q[rows beyond] *
+// L21_q[rows beyond]^T for the 64 x 64 block (i0.., j0..) of s's row list:
+// m > 1 for the column blocks of one wider supernode (a run), whose updates
+// beyond the run are summed in one pass (K = the run's columns, each member's
+// rows beyond the run are the rows of s, at offset r_q - r_s of its list);
+// m = 1 otherwise.  jl > 0 restricts the tile to columns j < jl (inside a run,
+// a member updates the later members' columns only).  C is scattered into the
+// ancestors' panels through the relative indices of s.  The K loop runs over
+// 32-column chunks of the members, double-buffered: the next chunk's copies
+// are in flight while the DMMA tiles consume the current one.
+constexpr int kUpdChunk = 32;
+constexpr int kUpdMaxMembers = 4;
+
 __global__ void __launch_bounds__(128) k_update(
     const UpdTile* __restrict__ tiles, const int* __restrict__ sn_first,
     const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows,
@@ -189,63 +203,99 @@ __global__ void __launch_bounds__(128) k_update(
     const int64_t* __restrict__ grp_relind, const int* __restrict__ relind, double* __restrict__ L,
     int use_atomics, const double* __restrict__ sgn) {
   extern __shared__ double sm[];
-  double* As = sm;                       // [kSnCols][kLdsU]
-  double* Bs = sm + kSnCols * kLdsU;     // [kSnCols][kLdsU]
+  // [buffer][A | B][kUpdChunk][kLdsU]
+  auto As = [&](int buf) { return sm + (size_t)buf * 2 * kUpdChunk * kLdsU; };
+  auto Bs = [&](int buf) { return sm + (size_t)buf * 2 * kUpdChunk * kLdsU + kUpdChunk * kLdsU; };
   const UpdTile tile = tiles[blockIdx.x];
   const int s = tile.s;
-  const int f = sn_first[s];
-  const int c = sn_first[s + 1] - f;
+  const int m = tile.mj & 15;
+  const int jl = tile.mj >> 4;
   const int64_t rp = rows_ptr[s];
   const int r = (int)(rows_ptr[s + 1] - rp);
-  const int64_t ld = c + r;
-  const double* P = L + Lptr[s] + c;  // row 0 of L21
-  const int kpad = (c + 3) & ~3;
   const int tid = threadIdx.x;
-  // the panel of s is final at this level (its targets are ancestors): copy
-  // both 64-row blocks asynchronously, every copy of a thread in flight at once
-  for (int idx = tid; idx < kpad * kUpdTile; idx += blockDim.x) {
-    const int k = idx / kUpdTile, ii = idx % kUpdTile;
-    const int gi = tile.i0 + ii, gj = tile.j0 + ii;
-    if (k < c && gi < r) cp_async8_f(As + k * kLdsU + ii, P + (int64_t)k * ld + gi);
-    else As[k * kLdsU + ii] = 0.0;
-    if (k < c && gj < r) cp_async8_f(Bs + k * kLdsU + ii, P + (int64_t)k * ld + gj);
-    else Bs[k * kLdsU + ii] = 0.0;
-  }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  __syncthreads();
-  if (sgn) {  // indefinite mode: A22 -= L21 S11 L21^T
-    for (int idx = tid; idx < c * kUpdTile; idx += blockDim.x) {
-      const int k = idx / kUpdTile, ii = idx % kUpdTile;
-      As[k * kLdsU + ii] *= sgn[f + k];
+  // chunks of the members: (member, first column)
+  int nch = 0;
+  int ch_q[2 * kUpdMaxMembers], ch_k0[2 * kUpdMaxMembers];
+  for (int u = 0; u < m; ++u) {
+    const int q = s - m + 1 + u;
+    const int cq = sn_first[q + 1] - sn_first[q];
+    for (int k0 = 0; k0 < cq; k0 += kUpdChunk) {
+      ch_q[nch] = q;
+      ch_k0[nch] = k0;
+      ++nch;
     }
-    __syncthreads();
   }
+  auto issue = [&](int ch, int buf) {
+    const int q = ch_q[ch], k0 = ch_k0[ch];
+    const int fq = sn_first[q];
+    const int cq = sn_first[q + 1] - fq;
+    const int rq = (int)(rows_ptr[q + 1] - rows_ptr[q]);
+    const int64_t ldq = cq + rq;
+    const double* P = L + Lptr[q] + cq + (rq - r);  // row 0 of the rows beyond the run
+    double* A = As(buf);
+    double* B = Bs(buf);
+    for (int idx = tid; idx < kUpdChunk * kUpdTile; idx += blockDim.x) {
+      const int k = idx / kUpdTile, ii = idx % kUpdTile;
+      const int kk = k0 + k;
+      const int gi = tile.i0 + ii, gj = tile.j0 + ii;
+      if (kk < cq && gi < r) cp_async8_f(A + k * kLdsU + ii, P + (int64_t)kk * ldq + gi);
+      else A[k * kLdsU + ii] = 0.0;
+      if (kk < cq && gj < r) cp_async8_f(B + k * kLdsU + ii, P + (int64_t)kk * ldq + gj);
+      else B[k * kLdsU + ii] = 0.0;
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
   const int warp = tid >> 5, lane = tid & 31;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
-  const int g = lane >> 2, q = lane & 3;
+  const int g = lane >> 2, qd = lane & 3;
   double acc[4][4][2];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
-  for (int k0 = 0; k0 < kpad; k0 += 4) {
-    double fa[4], fb[4];
+  issue(0, 0);
+  for (int ch = 0; ch < nch; ++ch) {
+    const int buf = ch & 1;
+    if (ch + 1 < nch) {
+      issue(ch + 1, buf ^ 1);
+      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    __syncthreads();
+    double* A = As(buf);
+    const double* B = Bs(buf);
+    if (sgn) {  // indefinite mode: A22 -= L21 S11 L21^T
+      const int fq = sn_first[ch_q[ch]];
+      const int cq = sn_first[ch_q[ch] + 1] - fq;
+      for (int idx = tid; idx < kUpdChunk * kUpdTile; idx += blockDim.x) {
+        const int k = idx / kUpdTile, ii = idx % kUpdTile;
+        if (ch_k0[ch] + k < cq) A[k * kLdsU + ii] *= sgn[fq + ch_k0[ch] + k];
+      }
+      __syncthreads();
+    }
+#pragma unroll 2
+    for (int k0 = 0; k0 < kUpdChunk; k0 += 4) {
+      double fa[4], fb[4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) fa[a] = As[(k0 + q) * kLdsU + wr + a * 8 + g];
+      for (int a = 0; a < 4; ++a) fa[a] = A[(k0 + qd) * kLdsU + wr + a * 8 + g];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) fb[b] = Bs[(k0 + q) * kLdsU + wc + b * 8 + g];
+      for (int b = 0; b < 4; ++b) fb[b] = B[(k0 + qd) * kLdsU + wc + b * 8 + g];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) dmma_8x8x4(acc[a][b][0], acc[a][b][1], fa[a], fb[b]);
+        for (int b = 0; b < 4; ++b) dmma_8x8x4(acc[a][b][0], acc[a][b][1], fa[a], fb[b]);
+    }
+    __syncthreads();  // the buffer is refilled by the next issue
   }
   // scatter-subtract into the ancestors
+  const int jend = jl > 0 ? min(jl, r) : r;
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
-      const int j = tile.j0 + wc + b * 8 + 2 * q + e;
-      if (j >= r) continue;
+      const int j = tile.j0 + wc + b * 8 + 2 * qd + e;
+      if (j >= jend) continue;
       const int grp = row_grp[rp + j];
       const int t = grp_target[grp];
       const int ft = sn_first[t];
@@ -269,6 +319,34 @@ __global__ void __launch_bounds__(128) k_update(
 // ---------------------------------------------------------------------------
 // host plan
 // ---------------------------------------------------------------------------
+// Runs of the factor's Schur updates: up to `max_members` consecutive
+// supernodes that are the column blocks of one wider supernode -- each the
+// parent of the previous, and each one's rows exactly the next block's
+// columns followed by the next block's rows.  run_end[s] = the last member
+// of s's run (s itself outside runs).
+std::vector<int> update_runs(const Symbolic& S, int max_members) {
+  const int nsn = S.nsn;
+  std::vector<int> end(nsn);
+  for (int s = 0; s < nsn; ++s) end[s] = s;
+  auto chained = [&](int q) {  // q and q + 1 are consecutive blocks of one supernode
+    if (q + 1 >= nsn || S.sn_parent[q] != q + 1) return false;
+    const int f1 = S.sn_first[q + 1], c1 = S.sn_first[q + 2] - f1;
+    const int64_t b0 = S.sn_rows_ptr[q], r0 = S.sn_rows_ptr[q + 1] - b0;
+    const int64_t b1 = S.sn_rows_ptr[q + 1], r1 = S.sn_rows_ptr[q + 2] - b1;
+    if (r0 != c1 + r1) return false;
+    for (int k = 0; k < c1; ++k)
+      if (S.sn_rows[b0 + k] != f1 + k) return false;
+    return std::equal(S.sn_rows.begin() + b0 + c1, S.sn_rows.begin() + b0 + r0, S.sn_rows.begin() + b1);
+  };
+  for (int s = 0; s < nsn;) {
+    int e = s;
+    while (e - s + 1 < max_members && chained(e)) ++e;
+    for (int q = s; q <= e; ++q) end[q] = e;
+    s = e + 1;
+  }
+  return end;
+}
+
 void build_factor_plan(temf_ctx& c) {
   const Symbolic& S = c.sym;
   FactorPlan& F = c.fplan;
@@ -341,17 +419,30 @@ void build_factor_plan(temf_ctx& c) {
     F.n_trsm = (int64_t)ch.size();
     F.trsm.upload(reinterpret_cast<const int2*>(ch.data()), ch.size(), st);
   }
-  // tiles per level
+  // tiles per level, with runs of column blocks summed (see k_update)
   {
+    const std::vector<int> run_end = update_runs(S, kUpdMaxMembers);
+    F.n_runs = 0;
     std::vector<UpdTile> tiles;
     F.tile_level_ptr.assign(S.nlevels + 1, 0);
     for (int l = 0; l < S.nlevels; ++l) {
       for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
         const int s = S.level_sn[q];
         const int r = (int)nrows(s);
+        const int e = run_end[s];
+        if (e != s) {
+          // a run member before its last: only the later members' columns
+          const int g = S.sn_first[e + 1] - S.sn_first[s + 1];
+          for (int tj = 0; tj * kUpdTile < g; ++tj)
+            for (int ti = tj; ti * kUpdTile < r; ++ti) tiles.push_back({s, ti * kUpdTile, tj * kUpdTile, 1 | (g << 4)});
+          continue;
+        }
+        int m = 1;  // members of the run ending at s
+        while (s - m >= 0 && run_end[s - m] == s) ++m;
+        if (m > 1) ++F.n_runs;
         const int nt = ceil_div(r, kUpdTile);
         for (int ti = 0; ti < nt; ++ti)
-          for (int tj = 0; tj <= ti; ++tj) tiles.push_back({s, ti * kUpdTile, tj * kUpdTile});
+          for (int tj = 0; tj <= ti; ++tj) tiles.push_back({s, ti * kUpdTile, tj * kUpdTile, m});
       }
       F.tile_level_ptr[l + 1] = (int64_t)tiles.size();
     }
@@ -429,7 +520,7 @@ void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
     k_load_A<<<ceil_div(F.n_a2l, 256), 256, 0, st>>>(F.n_a2l, F.a2l_src.p, F.a2l_dst.p, X, a, Y, b, fs.L.p);
     TEMF_CHECK_LAUNCH();
   }
-  const size_t upd_smem = 2 * kSnCols * kLdsU * sizeof(double);
+  const size_t upd_smem = 2 * 2 * kUpdChunk * kLdsU * sizeof(double);
   TEMF_CUDA(cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem));
   for (int l = 0; l < S.nlevels; ++l) {
     const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
