@@ -43,8 +43,8 @@ struct FactorPlan {
   int64_t n_a2l = 0;
   // update scatter metadata
   DBuf<int> row_grp;           // per below-diagonal row entry: global target-group id
-  DBuf<int> grp_target, grp_jfirst;
-  DBuf<int64_t> grp_relind;    // offset of the group's relative-index run
+  DBuf<int> grp_target, grp_shift;
+  DBuf<int64_t> grp_relind;    // rel index of row 0 of the source (tables shared by the blocks of a run)
   DBuf<int> relind;
   DBuf<UpdTile> tiles;
   std::vector<int64_t> tile_level_ptr;  // host, nlevels+1

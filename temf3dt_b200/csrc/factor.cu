@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(128) k_update(
     const UpdTile* __restrict__ tiles, const int* __restrict__ sn_first,
     const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows,
     const int64_t* __restrict__ Lptr, const int* __restrict__ row_grp,
-    const int* __restrict__ grp_target, const int* __restrict__ grp_jfirst,
+    const int* __restrict__ grp_target, const int* __restrict__ grp_shift,
     const int64_t* __restrict__ grp_relind, const int* __restrict__ relind, double* __restrict__ L,
     int use_atomics, const double* __restrict__ sgn) {
   extern __shared__ double sm[];
@@ -301,8 +301,8 @@ __global__ void __launch_bounds__(128) k_update(
       const int ft = sn_first[t];
       const int ct = sn_first[t + 1] - ft;
       const int64_t ldt = ct + (rows_ptr[t + 1] - rows_ptr[t]);
-      double* dstcol = L + Lptr[t] + (int64_t)(sn_rows[rp + j] - ft) * ldt;
-      const int* rel = relind + grp_relind[grp] - grp_jfirst[grp];
+      double* dstcol = L + Lptr[t] + (int64_t)(sn_rows[rp + j] - ft) * ldt - grp_shift[grp];
+      const int* rel = relind + grp_relind[grp];
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
         const int i = tile.i0 + wr + a * 8 + g;
@@ -326,21 +326,11 @@ __global__ void __launch_bounds__(128) k_update(
 // of s's run (s itself outside runs).
 std::vector<int> update_runs(const Symbolic& S, int max_members) {
   const int nsn = S.nsn;
+  const std::vector<int> run_first = block_run_first(S);
   std::vector<int> end(nsn);
-  for (int s = 0; s < nsn; ++s) end[s] = s;
-  auto chained = [&](int q) {  // q and q + 1 are consecutive blocks of one supernode
-    if (q + 1 >= nsn || S.sn_parent[q] != q + 1) return false;
-    const int f1 = S.sn_first[q + 1], c1 = S.sn_first[q + 2] - f1;
-    const int64_t b0 = S.sn_rows_ptr[q], r0 = S.sn_rows_ptr[q + 1] - b0;
-    const int64_t b1 = S.sn_rows_ptr[q + 1], r1 = S.sn_rows_ptr[q + 2] - b1;
-    if (r0 != c1 + r1) return false;
-    for (int k = 0; k < c1; ++k)
-      if (S.sn_rows[b0 + k] != f1 + k) return false;
-    return std::equal(S.sn_rows.begin() + b0 + c1, S.sn_rows.begin() + b0 + r0, S.sn_rows.begin() + b1);
-  };
   for (int s = 0; s < nsn;) {
     int e = s;
-    while (e - s + 1 < max_members && chained(e)) ++e;
+    while (e - s + 1 < max_members && e + 1 < nsn && run_first[e + 1] == run_first[s]) ++e;
     for (int q = s; q <= e; ++q) end[q] = e;
     s = e + 1;
   }
@@ -398,7 +388,7 @@ void build_factor_plan(temf_ctx& c) {
     F.n_relind = G.n_rel;
     F.row_grp.upload(G.row_grp.data(), G.row_grp.size(), st);
     F.grp_target.upload(G.grp_target.data(), G.grp_target.size(), st);
-    F.grp_jfirst.upload(G.grp_jfirst.data(), G.grp_jfirst.size(), st);
+    F.grp_shift.upload(G.grp_shift.data(), G.grp_shift.size(), st);
     F.grp_relind.upload(G.grp_rel.data(), G.grp_rel.size(), st);
     F.relind.upload(G.rel.get(), (size_t)G.n_rel, st);
     TEMF_CUDA(cudaStreamSynchronize(st));  // G's host arrays go out of scope
@@ -540,7 +530,7 @@ void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
       if (t1 - t0 > INT_MAX) throw StateError("too many update tiles in one level");
       k_update<<<(unsigned)(t1 - t0), 128, upd_smem, st>>>(F.tiles.p + t0, F.sn_first.p, F.sn_rows_ptr.p,
                                                           F.sn_rows.p, F.sn_Lptr.p, F.row_grp.p, F.grp_target.p,
-                                                          F.grp_jfirst.p, F.grp_relind.p, F.relind.p, fs.L.p,
+                                                          F.grp_shift.p, F.grp_relind.p, F.relind.p, fs.L.p,
                                                           cnt > 1 ? 1 : 0, sgn);
       TEMF_CHECK_LAUNCH();
     }

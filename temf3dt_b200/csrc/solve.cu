@@ -2162,6 +2162,10 @@ std::string check_schedules(const Symbolic& S) {
     const std::string w = check_structure(S);
     if (!w.empty()) return "supernode structure: " + w;
   }
+  {
+    const std::string w = check_update_groups(S);
+    if (!w.empty()) return "factor update groups: " + w;
+  }
   const int splits[5] = {0, level_below_width(S, 2048), default_split(S), level_below_width(S, 64), S.nlevels};
   for (int sp : splits) {
     std::string w = check_schedule(S, kChunkRows, sp);

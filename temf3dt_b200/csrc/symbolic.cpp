@@ -371,19 +371,47 @@ int host_threads(int requested) {
   return std::min(n, 64);
 }
 
+std::vector<int> block_run_first(const Symbolic& S) {
+  const int nsn = S.nsn;
+  std::vector<int> first(nsn);
+  for (int s = 0; s < nsn; ++s) first[s] = s;
+  for (int q = 0; q + 1 < nsn; ++q) {
+    if (S.sn_parent[q] != q + 1) continue;
+    const int f1 = S.sn_first[q + 1], c1 = S.sn_first[q + 2] - f1;
+    const int64_t b0 = S.sn_rows_ptr[q], r0 = S.sn_rows_ptr[q + 1] - b0;
+    const int64_t b1 = S.sn_rows_ptr[q + 1], r1 = S.sn_rows_ptr[q + 2] - b1;
+    if (r0 != c1 + r1) continue;
+    bool ok = true;
+    for (int k = 0; k < c1 && ok; ++k) ok = S.sn_rows[b0 + k] == f1 + k;
+    if (!ok || !std::equal(S.sn_rows.begin() + b0 + c1, S.sn_rows.begin() + b0 + r0, S.sn_rows.begin() + b1))
+      continue;
+    first[q + 1] = first[q];
+  }
+  return first;
+}
+
 void update_groups(const Symbolic& S, UpdateGroups& G, int threads) {
   const int nsn = S.nsn;
-  // pass 1: groups and relative positions per supernode
+  const std::vector<int> run_first = block_run_first(S);
+  std::vector<int> run_last(nsn);  // last block of each run, indexed by any block
+  for (int s = nsn - 1; s >= 0; --s)
+    run_last[s] = (s + 1 < nsn && run_first[s + 1] == run_first[s]) ? run_last[s + 1] : s;
+  auto owner = [&](int64_t rp, int64_t j) { return S.col2sn[S.sn_rows[rp + j]]; };
+  // pass 1: groups and relative positions per supernode (one table per target run)
   std::vector<int64_t> goff(nsn + 1, 0), roff(nsn + 1, 0);
   for (int s = 0; s < nsn; ++s) {
     const int64_t rp = S.sn_rows_ptr[s], r = S.sn_rows_ptr[s + 1] - rp;
     int64_t ng = 0, nr = 0;
+    int last_run = -1;
     for (int64_t j = 0; j < r;) {
-      const int t = S.col2sn[S.sn_rows[rp + j]];
+      const int t = owner(rp, j);
       int64_t j2 = j;
-      while (j2 < r && S.col2sn[S.sn_rows[rp + j2]] == t) ++j2;
+      while (j2 < r && owner(rp, j2) == t) ++j2;
       ++ng;
-      nr += r - j;
+      if (run_first[t] != last_run) {  // a new table from row j
+        nr += r - j;
+        last_run = run_first[t];
+      }
       j = j2;
     }
     goff[s + 1] = goff[s] + ng;
@@ -393,7 +421,7 @@ void update_groups(const Symbolic& S, UpdateGroups& G, int threads) {
   if (ngrp > INT32_MAX) throw std::runtime_error("too many update groups for int32 indices");
   G.row_grp.assign(S.sn_rows.size(), 0);
   G.grp_target.assign(ngrp, 0);
-  G.grp_jfirst.assign(ngrp, 0);
+  G.grp_shift.assign(ngrp, 0);
   G.grp_rel.assign(ngrp, 0);
   G.n_rel = roff[nsn];
   G.rel.reset(new int[std::max<int64_t>(G.n_rel, 1)]);
@@ -402,29 +430,38 @@ void update_groups(const Symbolic& S, UpdateGroups& G, int threads) {
     for (int s = s0; s < s1; ++s) {
       const int64_t rp = S.sn_rows_ptr[s], r = S.sn_rows_ptr[s + 1] - rp;
       int64_t g = goff[s], q = roff[s];
+      int last_run = -1;
+      int64_t table = 0;  // rel index of row 0 of s in the current table
       for (int64_t j = 0; j < r;) {
-        const int t = S.col2sn[S.sn_rows[rp + j]];
+        const int t = owner(rp, j);
         int64_t j2 = j;
-        while (j2 < r && S.col2sn[S.sn_rows[rp + j2]] == t) ++j2;
-        G.grp_target[g] = t;
-        G.grp_jfirst[g] = (int)j;
-        G.grp_rel[g] = q;
-        for (int64_t jj = j; jj < j2; ++jj) G.row_grp[rp + jj] = (int)g;
-        // relative positions of rows j..r-1 inside t's panel (merge of sorted lists)
-        const int ft = S.sn_first[t], ct = S.sn_first[t + 1] - ft;
-        const int* tb = S.sn_rows.data() + S.sn_rows_ptr[t];
-        const int64_t tr = S.sn_rows_ptr[t + 1] - S.sn_rows_ptr[t];
-        int64_t k = 0;
-        for (int64_t i = j; i < r; ++i) {
-          const int gi = S.sn_rows[rp + i];
-          if (gi < ft + ct) {
-            G.rel[q++] = gi - ft;
-            continue;
+        while (j2 < r && owner(rp, j2) == t) ++j2;
+        const int t0 = run_first[t];
+        if (t0 != last_run) {
+          // positions of rows j..r-1 in the panel of the run's first block t0:
+          // its columns, the later blocks' columns, then the last block's rows
+          const int te = run_last[t0];
+          const int f0 = S.sn_first[t0], fend = S.sn_first[te + 1];
+          const int* tb = S.sn_rows.data() + S.sn_rows_ptr[te];
+          const int64_t tr = S.sn_rows_ptr[te + 1] - S.sn_rows_ptr[te];
+          table = q - j;
+          int64_t k = 0;
+          for (int64_t i = j; i < r; ++i) {
+            const int gi = S.sn_rows[rp + i];
+            if (gi < fend) {
+              G.rel[q++] = gi - f0;
+              continue;
+            }
+            while (k < tr && tb[k] < gi) ++k;
+            if (k >= tr || tb[k] != gi) throw std::runtime_error("symbolic structure inconsistent (update row)");
+            G.rel[q++] = (int)((fend - f0) + k);
           }
-          while (k < tr && tb[k] < gi) ++k;
-          if (k >= tr || tb[k] != gi) throw std::runtime_error("symbolic structure inconsistent (update row)");
-          G.rel[q++] = (int)(ct + k);
+          last_run = t0;
         }
+        G.grp_target[g] = t;
+        G.grp_shift[g] = S.sn_first[t] - S.sn_first[t0];
+        G.grp_rel[g] = table;
+        for (int64_t jj = j; jj < j2; ++jj) G.row_grp[rp + jj] = (int)g;
         ++g;
         j = j2;
       }
@@ -443,6 +480,35 @@ void update_groups(const Symbolic& S, UpdateGroups& G, int threads) {
     cut[k] = s;
   }
   parallel_for_each(nt, [&](int k) { fill(cut[k], cut[k + 1]); });
+}
+
+std::string check_update_groups(const Symbolic& S) {
+  UpdateGroups G;
+  try {
+    update_groups(S, G);
+  } catch (const std::exception& e) {
+    return e.what();
+  }
+  for (int s = 0; s < S.nsn; ++s) {
+    const int64_t rp = S.sn_rows_ptr[s], r = S.sn_rows_ptr[s + 1] - rp;
+    for (int64_t j = 0; j < r; ++j) {
+      const int g = G.row_grp[rp + j];
+      const int t = G.grp_target[g];
+      if (S.col2sn[S.sn_rows[rp + j]] != t) return "a row's group targets another supernode";
+      if (j > 0 && G.row_grp[rp + j - 1] == g) continue;
+      // rows i >= j of s land on their own rows of t's panel
+      const int ft = S.sn_first[t], ct = S.sn_first[t + 1] - ft;
+      const int* tb = S.sn_rows.data() + S.sn_rows_ptr[t];
+      const int64_t tr = S.sn_rows_ptr[t + 1] - S.sn_rows_ptr[t];
+      for (int64_t i = j; i < r; ++i) {
+        const int64_t pos = (int64_t)G.rel[G.grp_rel[g] + i] - G.grp_shift[g];
+        const int gi = S.sn_rows[rp + i];
+        const int at = pos < 0 ? -1 : pos < ct ? ft + (int)pos : (pos - ct < tr ? tb[pos - ct] : -1);
+        if (at != gi) return "an update row scatters to the wrong row of its target panel";
+      }
+    }
+  }
+  return std::string();
 }
 
 std::vector<int> nested_dissection(int n, const int64_t* xadj, const int* adj,

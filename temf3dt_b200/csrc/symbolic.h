@@ -61,17 +61,29 @@ struct Symbolic {
 std::vector<int> nested_dissection(int n, const int64_t* xadj, const int* adj,
                                    const double* xyz, int leaf_size, int threads = 0);
 
+// Runs of column blocks: the supernodes that come from splitting one wider
+// supernode into blocks of at most max_sn_cols columns.  q and q + 1 are
+// consecutive blocks when q's parent is q + 1 and q's rows are exactly q + 1's
+// columns followed by q + 1's rows.  run_first[s] = the first block of s's
+// (maximal) run.
+std::vector<int> block_run_first(const Symbolic& S);
+
 // Update groups of the numeric factorisation.  The below-diagonal rows of a
 // supernode s fall into runs owned by one ancestor t each (a group); the
-// update of s scatters its rows j.. (j = the group's first row) into t's
-// panel at relative positions rel[grp_rel[g] + (i - j)]: the column offset
-// for rows inside t's columns, c_t + (position in t's row list) for rows
-// below them.
+// update of s scatters its rows i >= j (j = the group's first row) into t's
+// panel at
+//     column (sn_rows[j'] - first column of t), row rel[grp_rel[g] + i] - grp_shift[g].
+// One relative-index table serves all the groups of s whose targets are
+// blocks of one run T (t_0 .. t_e): it holds, for the rows of s from the
+// first one owned by T, their positions in t_0's panel; a block t_q of the
+// run shares the same order shifted by grp_shift = (first column of t_q) -
+// (first column of t_0), since each block's rows are the later blocks'
+// columns followed by the last block's rows.
 struct UpdateGroups {
   std::vector<int> row_grp;      // per entry of Symbolic::sn_rows: its group
   std::vector<int> grp_target;   // per group: t
-  std::vector<int> grp_jfirst;   // per group: j
-  std::vector<int64_t> grp_rel;  // per group: offset into rel
+  std::vector<int> grp_shift;    // per group: first column of t - first column of its run's first block
+  std::vector<int64_t> grp_rel;  // per group: rel index of row 0 of s (the table's start minus its first row)
   std::unique_ptr<int[]> rel;    // relative positions (uninitialised storage, all written)
   int64_t n_rel = 0;
 };
@@ -80,6 +92,9 @@ struct UpdateGroups {
 // $TEMF_HOST_THREADS, else all cores); the result does not depend on the
 // count.  Throws if a row of s is missing from its ancestor's structure.
 void update_groups(const Symbolic& S, UpdateGroups& G, int threads = 0);
+// Host check of the update groups: every row a supernode's update scatters
+// lands on that row of its target panel.  Empty string, or the violation.
+std::string check_update_groups(const Symbolic& S);
 
 // Host threads to use for a request (0: $TEMF_HOST_THREADS, else the cores
 // this process may run on, bounded by the cgroup CPU quota, at most 64).

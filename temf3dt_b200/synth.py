@@ -212,6 +212,10 @@ def build_model(kind: str = "halfspace", seed: int = 0, scale: float = 1.0, **kw
       "block"     -- conductive block in a host, square loop, receivers on a line;
       "multiloop" -- the block model with an nx*ny grid of small square loops,
                      one RHS column and one central receiver each;
+      "ellipsoids" -- a 0.005 S/m host with 4 random ellipsoidal conductors
+                     (0.05-1 S/m, semi-axes 50-300 m, centres 50-400 m deep)
+                     under a 16 x 16 grid of 50 m loops at 40 m spacing, one
+                     RHS column and one central receiver each;
       "layered"   -- a 1-D layered earth (3-6 layers, conductivities
                      log-uniform in [1e-4, 1e-1] S/m, thicknesses log-uniform
                      in [10, 300] m, all drawn from the seed) under air, a
@@ -290,6 +294,47 @@ def build_model(kind: str = "halfspace", seed: int = 0, scale: float = 1.0, **kw
                                                  (np.abs(x - cx) < a) & (np.abs(y - cy) < a)))
                     rec.append(_nudge((cx, cy, kw.get("rec_z", 2.5)), g))
                     rec_rhs.append(len(loops0) - 1)
+    elif kind == "ellipsoids":
+        # host with random ellipsoidal conductors under an n x n grid of small
+        # square loops (one RHS column and one central receiver each)
+        host = kw.get("sigma", 0.005)
+        n_ell = kw.get("n_ellipsoids", 4)
+        ell_sig = 10.0 ** rng.uniform(np.log10(0.05), 0.0, n_ell)          # 0.05 .. 1 S/m
+        ell_ax = rng.uniform(50.0, 300.0, (n_ell, 3))                      # semi-axes (m)
+        ell_ctr = np.column_stack([rng.uniform(-300.0, 300.0, n_ell), rng.uniform(-300.0, 300.0, n_ell),
+                                   rng.uniform(50.0, 400.0, n_ell)])       # centre depth 50 .. 400 m
+        h = kw.get("h_core", 20.0) / scale
+        n_l = kw.get("n_loops", 16)
+        sp_, a = kw.get("loop_spacing", 40.0), kw.get("loop_half", 25.0)
+        centers = (np.arange(n_l) - (n_l - 1) / 2.0) * sp_
+        req = list(centers - a) + list(centers + a)
+        core = (min(centers) - a - 2 * h, max(centers) + a + 2 * h)
+        xs = graded_axis(req, core, h, half, kw.get("ratio", 1.5), h_min=kw.get("h_min", 4.0))
+        ys = xs.copy()
+        hz = kw.get("h_z", 20.0) / scale
+        deepest = float(np.max(ell_ctr[:, 2] + ell_ax[:, 2]))
+        zs = graded_axis([0.0], (-2 * hz, min(deepest, kw.get("z_core", 700.0))), hz, half, kw.get("ratio", 1.5))
+        g = Grid(xs, ys, zs)
+
+        def phys(x, y, z):
+            p = np.where(z > 0, EARTH, AIR)
+            for k in range(n_ell):
+                d = ((x - ell_ctr[k, 0]) / ell_ax[k, 0]) ** 2 + ((y - ell_ctr[k, 1]) / ell_ax[k, 1]) ** 2 + \
+                    ((z - ell_ctr[k, 2]) / ell_ax[k, 2]) ** 2
+                p = np.where((d <= 1.0) & (z > 0), EARTH + 1 + k, p)
+            return p
+
+        nod, tets, tph = hex_to_tets(g, phys)
+        kz = int(np.searchsorted(zs, 0.0))
+        domains = [(AIR, sig_air, 1.0, 1.0), (EARTH, host, 1.0, 1.0)] + \
+                  [(EARTH + 1 + k, float(ell_sig[k]), 1.0, 1.0) for k in range(n_ell)]
+        loops0, rec, rec_rhs = [], [], []
+        for cy in centers:
+            for cx in centers:
+                loops0.append(staircase_loop(g, kz, lambda x, y, cx=cx, cy=cy:
+                                             (np.abs(x - cx) < a) & (np.abs(y - cy) < a)))
+                rec.append(_nudge((cx, cy, kw.get("rec_z", 2.5)), g))
+                rec_rhs.append(len(loops0) - 1)
     elif kind == "layered":
         nlay = int(kw.get("n_layers", rng.integers(3, 7)))
         sig_l = 10.0 ** rng.uniform(-4.0, -1.0, nlay)
