@@ -61,6 +61,8 @@ CONFIGS = {
     2: dict(kind="multiloop", kw=dict(BLOCK_GRID), label="block3d-1.48M-edges-64-loops-64rhs"),
     3: dict(kind="block", kw=dict(BLOCK_GRID),
             label="block3d-1.48M-edges-lognormal-32x32x16-cells-64rec-40gates-adjoint"),
+    4: dict(kind="ellipsoids", kw=dict(h_core=20.0, h_z=12.0, ratio=1.4),
+            label="ellipsoids-0.005Spm-4.37M-tets-5.17M-edges-256-loops-64rhs-blocks"),
 }
 # config 3: the inversion grid (32 x 32 x 16 cells of 25 x 25 x 12.5 m under the
 # loop), log-normal cell conductivities around 0.01 S/m with 0.5 decades, and
@@ -292,6 +294,47 @@ def adjoint_measure(local: int, fd_cells: int = 0):
             scale = float(np.abs(grad).max())
             out["fd"] = {"cells": [int(k) for k in pick], "max_rel_err": float(max(rel)),
                          "median_rel_err": float(np.median(rel)), "step": h, "grad_max": scale}
+    return out
+
+
+def config4_measure(local: int, max_steps: int):
+    """Config 4: the ~5M-edge ellipsoid model with 256 small-loop sources in
+    blocks of 64 columns.  Reports the analysis (nnz(L), factor flops), the
+    device memory of the plan (one factor slot, relative indices, vectors)
+    against the GPU's, and runs the first `max_steps` time steps of the
+    adaptive loop for all 256 columns (each block of 64 one block sweep per
+    step), timed with CUDA events inside the library."""
+    import torch
+    from temf3dt_b200 import fetd
+    m = model_for(4)
+    c = m.ctl
+    free0, total = torch.cuda.mem_get_info(local)
+    out = {"workload": CONFIGS[4]["label"], "tets": int(len(m.mesh.tet_vex)), "rhs": len(m.loops)}
+    with fetd.FetdGPU(local) as g:
+        t0 = time.perf_counter()
+        info = fetd.load_case(g, m.mesh, m.ctl)
+        out["setup_s"] = time.perf_counter() - t0
+        st = g.stats()
+        cols = m.source_columns(info["edg_vex"])
+        rec_tet = g.locate(m.receivers, c.rec_charac)
+        runs = []
+        free1 = free0
+        for b0 in range(0, len(cols), 64):   # the sources in blocks of 64 columns, one run each
+            sel = [i for i in range(len(m.receivers)) if b0 <= m.rec_rhs[i] < b0 + 64]
+            g.set_sources(cols[b0:b0 + 64], 1, c.pulse_type, c.t0, 1.0)
+            g.set_receivers(rec_tet[sel], m.receivers[sel], rec_rhs=m.rec_rhs[sel] - b0)
+            runs.append(g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum, max_steps=max_steps))
+            free1 = min(free1, torch.cuda.mem_get_info(local)[0])
+    ms = sum(o.ms_total for o in runs)
+    steps_rhs = sum((len(o.steps) - 1) * 64 for o in runs)
+    o = runs[0]
+    out.update({"n_edges": int(st["n"]), "nnz_L": st["nnz_L"], "stored_doubles": st["stored"],
+                "factor_slot_GB": 8 * st["stored"] / 1e9, "factor_tflop": st["flops"] / 1e12,
+                "device_GB_in_use": (free0 - free1) / 1e9, "device_GB_total": total / 1e9,
+                "steps_per_block": len(o.steps) - 1, "blocks": len(runs), "factorisations_per_block": o.n_factor,
+                "ms_factor_each": o.ms_factor / max(o.n_factor, 1),
+                "ms_per_step_64rhs": o.ms_steps / max(o.n_solve, 1),
+                "steps_rhs_per_s": steps_rhs / (ms / 1e3), "ms_total": ms})
     return out
 
 
@@ -682,8 +725,10 @@ def main():
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3],
-                    help="3: the adjoint measurement of config 3 alone (one JSON object, not a bench line)")
+    ap.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3, 4],
+                    help="3: the adjoint measurement of config 3 alone; 4: the 5M-edge 256-source run "
+                         "(one JSON object each, not a bench line)")
+    ap.add_argument("--c4-steps", type=int, default=100, help="config 4: time steps to run")
     ap.add_argument("--sample-steps", type=int, default=0, help="CPU arm: time steps per sample (0: 10)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--adjoint", type=int, default=1, help="config 1: also time one config-3 adjoint gradient")
@@ -705,6 +750,11 @@ def main():
         return profile_run(args)
     if args.impl == "reference":
         return reference_arm(args)
+    if args.config == 4:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps({"config4": config4_measure(int(os.environ.get("LOCAL_RANK", "0")), args.c4_steps)}))
+        return 0
     if args.config == 3:
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
