@@ -140,12 +140,15 @@ module temf_b200
     integer(c_int) function temf_solve_schedule(ctx, nrhs, split, tuned) bind(C, name="temf_solve_schedule")
       import; type(c_ptr), value :: ctx; integer(c_int), value :: nrhs; integer(c_int) :: split; integer(c_int) :: tuned
     end function
-    integer(c_int) function temf_set_solve_plan(ctx, tree_level, split) bind(C, name="temf_set_solve_plan")
+    integer(c_int) function temf_set_solve_plan(ctx, tree_level, split, run_leaders) &
+        bind(C, name="temf_set_solve_plan")
       import; type(c_ptr), value :: ctx; integer(c_int), value :: tree_level; integer(c_int), value :: split
+      integer(c_int), value :: run_leaders
     end function
-    integer(c_int) function temf_solve_plan(ctx, tree_level, split, n_trees, tuned) bind(C, name="temf_solve_plan")
+    integer(c_int) function temf_solve_plan(ctx, tree_level, split, run_leaders, n_trees, tuned) &
+        bind(C, name="temf_solve_plan")
       import; type(c_ptr), value :: ctx; integer(c_int) :: tree_level; integer(c_int) :: split
-      integer(c_int) :: n_trees; integer(c_int) :: tuned
+      integer(c_int) :: run_leaders; integer(c_int) :: n_trees; integer(c_int) :: tuned
     end function
     integer(c_int) function temf_set_wait_limit(ctx, spins, inject_unmet_wait) bind(C, name="temf_set_wait_limit")
       import; type(c_ptr), value :: ctx; integer(c_int), value :: spins; integer(c_int), value :: inject_unmet_wait

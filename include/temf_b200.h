@@ -221,13 +221,17 @@ int temf_solve_schedule(temf_ctx* ctx, int nrhs, int* split, int* tuned);
 /* The single-column sweeps (temf_solve, temf_run) first sweep the bottom of
  * the supernodal tree as whole subtrees, one warp each: the supernodes below
  * a subtree level, with no waits; the persistent task sweeps cover the rest.
- * For nrhs = 1, temf_tune_solve also picks the subtree level (0 = none, or
- * levels that leave at least one subtree per SM) before the queue split, and
- * reports the split candidates at the chosen level.  temf_set_solve_plan sets
- * both explicitly (checked on the host, marked tuned); temf_solve_plan
- * reports the plan in use and its number of subtrees.  No reference
- * counterpart. */
-int temf_set_solve_plan(temf_ctx* ctx, int tree_level, int split);
+ * Above the queue split, the column blocks of a wide supernode (one per
+ * level) are swept by one leader task that forwards the rows inside the run
+ * through shared memory instead of handing each block to another CTA
+ * (run_leaders = 1).  For nrhs = 1, temf_tune_solve also picks the subtree
+ * level (0 = none, or levels that leave at least one subtree per SM) before
+ * the queue split, then whether to use run leaders, and reports the split
+ * candidates at the chosen level.  temf_set_solve_plan sets the plan
+ * explicitly (checked on the host, marked tuned); temf_solve_plan reports the
+ * plan in use and its number of subtrees.  No reference counterpart. */
+int temf_set_solve_plan(temf_ctx* ctx, int tree_level, int split, int run_leaders);
+int temf_solve_plan(temf_ctx* ctx, int* tree_level, int* split, int* run_leaders, int* n_trees, int* tuned);
 /* Failure detection of the device waits.  No reference counterpart.  Every
  * wait of the persistent sweeps on a flag another CTA sets is bounded: after
  * `spins` polls (0: the default, about a second) it gives up, records which
@@ -238,7 +242,6 @@ int temf_set_solve_plan(temf_ctx* ctx, int tree_level, int split);
  * than any task provides for the last supernode, so that one wait cannot be
  * met (a test of this path; it is consumed by that solve). */
 int temf_set_wait_limit(temf_ctx* ctx, int spins, int inject_unmet_wait);
-int temf_solve_plan(temf_ctx* ctx, int* tree_level, int* split, int* n_trees, int* tuned);
 
 /* ---- profiling aid -------------------------------------------------------------
  * No reference counterpart.  One single-column solve (right-hand side all

@@ -56,8 +56,8 @@ SIGNATURES = {
     "temf_set_analysis_options": (_i, [_p, _i, _i]),
     "temf_tune_solve": (_i, [_p, _i, _i, _ip, _ip, _ip, _dp]),
     "temf_solve_schedule": (_i, [_p, _i, _ip, _ip]),
-    "temf_set_solve_plan": (_i, [_p, _i, _i]),
-    "temf_solve_plan": (_i, [_p, _ip, _ip, _ip, _ip]),
+    "temf_set_solve_plan": (_i, [_p, _i, _i, _i]),
+    "temf_solve_plan": (_i, [_p, _ip, _ip, _ip, _ip, _ip]),
     "temf_set_wait_limit": (_i, [_p, _i, _i]),
     "temf_schedule_check": (_i, [_i, C.POINTER(C.c_longlong), _ip, _dp, C.c_char_p, _i]),
     "temf_solve_timeline": (_i, [_p, _i, C.c_longlong, C.POINTER(C.c_ulonglong), _ip, _ip]),

@@ -1150,20 +1150,21 @@ int temf_set_wait_limit(temf_ctx* c, int spins, int inject_unmet_wait) {
   });
 }
 
-int temf_set_solve_plan(temf_ctx* c, int tree_level, int split) {
+int temf_set_solve_plan(temf_ctx* c, int tree_level, int split, int run_leaders) {
   return guarded(c, [&] {
     need(c->analysed, "temf_set_solve_plan: call temf_analyse first");
-    set_tree_plan(*c, tree_level, split);
+    set_tree_plan(*c, tree_level, split, run_leaders != 0);
     return TEMF_OK;
   });
 }
 
-int temf_solve_plan(temf_ctx* c, int* tree_level, int* split, int* n_trees, int* tuned) {
+int temf_solve_plan(temf_ctx* c, int* tree_level, int* split, int* run_leaders, int* n_trees, int* tuned) {
   return guarded(c, [&] {
     need(c->analysed, "temf_solve_plan: call temf_analyse first");
     const TreePlan& T = c->splan.tree;
     if (tree_level) *tree_level = T.level;
     if (split) *split = T.q.split;
+    if (run_leaders) *run_leaders = T.leaders ? 1 : 0;
     if (n_trees) *n_trees = T.ntree;
     if (tuned) *tuned = T.tuned ? 1 : 0;
     return TEMF_OK;

@@ -91,6 +91,7 @@ struct QueuePlan {
 // above `level` only.  level 0: no subtrees (the full schedules).
 struct TreePlan {
   int level = 0;
+  bool leaders = true;         // runs of column blocks above the queue split swept by one leader task
   int ntree = 0;
   DBuf<int2> trees;            // (first, root) per subtree, most stored panel values first
   DBuf<SolveTask> ftask, btask;

@@ -532,11 +532,187 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_persistent(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Runs of column blocks swept by one CTA (single right-hand side).
+// A wide supernode is split into blocks of at most 64 columns, one per level,
+// each block's rows being the next block's columns followed by the next
+// block's rows.  Handed from CTA to CTA, every block costs a publish, a fence
+// and a poll on the critical path.  A leader task instead walks the blocks of
+// a run itself: the first 128 rows of each block's panel (which, inside the
+// run, are the next blocks' columns) are applied locally through a ring of
+// run columns in shared memory, and only the other row chunks (ordinary chunk
+// tasks of other CTAs) and the rows beyond the run go through global memory
+// with atomics and counts, two blocks or more ahead of their use.  The task
+// entry of every block (the leader's own, or an absorbed entry past the
+// claimable tasks) keeps the owners of its first chunk beyond the run.
+//   forward: block q waits for its expected inputs, subtracts the ring, solves,
+//            publishes y_q, accumulates its first chunk into the ring or x;
+//   backward: block q waits for its other chunks and for the owners beyond
+//            the run, takes the run rows' x from the ring, solves, publishes.
+// ---------------------------------------------------------------------------
+constexpr int kRing = 256;  // run columns held in shared memory (>= 64 + 128 live)
+
+__device__ __forceinline__ int leader_blocks(const SolveTask& T) { return T.kind >> 4; }
+
+__device__ void fwd_leader(const SweepView& V, int t, const double* Lb, int* err, double (*D)[kSnCols + 1],
+                           double* rinv, double* ys, double* ring) {
+  int* ready = V.sync;
+  int* ydone = V.sync + V.nsn;
+  double* x = V.x;
+  const int tid = threadIdx.x;
+  const SolveTask T0 = V.tasks[t];
+  const int a = T0.s, e = a + leader_blocks(T0) - 1;
+  const int f_run = V.sn_first[a], f_end = V.sn_first[e + 1];
+  for (int k = tid; k < kRing; k += blockDim.x) ring[k] = 0.0;
+  FwdRegs R;
+  {
+    const int c = V.sn_first[a + 1] - f_run;
+    const int64_t r = V.rows_ptr[a + 1] - V.rows_ptr[a], ld = c + r;
+    const double* P = Lb + V.Lptr[a];
+    pre_fwd(R, P + c, c, ld, tid, tid < (r < kChunkRows ? r : (int64_t)kChunkRows));
+    load_diag_start(D, P, c, ld);
+  }
+  for (int q = a; q <= e; ++q) {
+    const int f = V.sn_first[q], c = V.sn_first[q + 1] - f;
+    const int64_t rp = V.rows_ptr[q], r = V.rows_ptr[q + 1] - rp;
+    const int r1 = (int)(r < kChunkRows ? r : (int64_t)kChunkRows);
+    const int dq = V.diag_task[q];
+    if (tid == 0) wait_geq(ready + q, V.expect[q], err, 1, spin_limit(V));
+    __syncthreads();
+    for (int j = tid; j < c; j += blockDim.x) {
+      const int slot = (f + j - f_run) & (kRing - 1);
+      ys[j] = __ldcg(x + f + j) - ring[slot];
+      ring[slot] = 0.0;
+    }
+    load_diag_finish(D, rinv, c);
+    diag_solve(D, rinv, ys, c, 1, true);
+    for (int j = tid; j < c; j += blockDim.x) x[f + j] = ys[j];
+    if (tid < r1) {
+      const double v = fin_fwd(R, ys, c);
+      const int row = V.sn_rows[rp + tid];
+      if (row < f_end) ring[(row - f_run) & (kRing - 1)] -= v;  // inside the run: one writer per row
+      else atomicAdd(x + row, -v);
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) atomicExch(ydone + q, 1);
+    if (V.queue) {
+      for (int k = V.tgt_ptr[dq] + tid; k < V.tgt_ptr[dq + 1]; k += blockDim.x) {
+        const int o = V.tgt[k];
+        const int d = V.diag_task[o];
+        if (!in_queue(V, d)) atomicAdd(ready + o, 1);
+        else if (atomicAdd(ready + o, 1) == V.expect[o] - 1) q_push(V, d);
+      }
+    } else if (tid == 0) {
+      for (int k = V.tgt_ptr[dq]; k < V.tgt_ptr[dq + 1]; ++k) atomicAdd(ready + V.tgt[k], 1);
+    }
+    if (q < e) {  // the next block's panel: first chunk into registers, diagonal block into shared memory
+      const int fn = V.sn_first[q + 1], cn = V.sn_first[q + 2] - fn;
+      const int64_t rn = V.rows_ptr[q + 2] - V.rows_ptr[q + 1], ldn = cn + rn;
+      const double* Pn = Lb + V.Lptr[q + 1];
+      pre_fwd(R, Pn + cn, cn, ldn, tid, tid < (rn < kChunkRows ? rn : (int64_t)kChunkRows));
+      load_diag_start(D, Pn, cn, ldn);
+    }
+  }
+}
+
+__device__ void bwd_leader(const SweepView& V, int t, const double* Lb, int* err, double (*D)[kSnCols + 1],
+                           double* rinv, double (*seg)[kSnCols], double* zs, double* ring) {
+  int* cdone = V.sync + 2 * V.nsn;
+  int* xdone = V.sync + 3 * V.nsn;
+  double* x = V.x;
+  const int tid = threadIdx.x;
+  const SolveTask T0 = V.tasks[t];
+  const int e = T0.s, a = e - leader_blocks(T0) + 1;
+  const int f_run = V.sn_first[a], f_end = V.sn_first[e + 1];
+  BwdRegs R;
+  {
+    const int c = V.sn_first[e + 1] - V.sn_first[e];
+    const int64_t r = V.rows_ptr[e + 1] - V.rows_ptr[e], ld = c + r;
+    const double* P = Lb + V.Lptr[e];
+    const int r1 = (int)(r < kChunkRows ? r : (int64_t)kChunkRows);
+    if (r1 > 0) pre_bwd(R, P, c, ld, 0, r1);
+    load_diag_start(D, P, c, ld);
+  }
+  for (int q = e; q >= a; --q) {
+    const int f = V.sn_first[q], c = V.sn_first[q + 1] - f;
+    const int64_t rp = V.rows_ptr[q], r = V.rows_ptr[q + 1] - rp;
+    const int r1 = (int)(r < kChunkRows ? r : (int64_t)kChunkRows);
+    const int dq = V.diag_task[q];
+    // the owners of the first chunk's rows beyond the run, and the block's other chunks
+    {
+      const int q0 = V.tgt_ptr[dq], nq = V.tgt_ptr[dq + 1] - q0;
+      for (int k = tid; k < nq; k += blockDim.x) wait_geq(xdone + V.tgt[q0 + k], 1, err, 3, spin_limit(V));
+      if (tid == blockDim.x - 1) wait_geq(cdone + q, V.nchunk[q] - (r1 > 0 ? 1 : 0), err, 4, spin_limit(V));
+    }
+    __syncthreads();
+    double* zx = zs + kSnCols;
+    if (r1 > 0) {
+      for (int ii = tid; ii < r1; ii += blockDim.x) {
+        const int row = V.sn_rows[rp + ii];
+        zx[ii] = row < f_end ? ring[(row - f_run) & (kRing - 1)] : __ldcg(x + row);
+      }
+      __syncthreads();
+      fin_bwd(R, zx, c, r1, seg);
+      __syncthreads();
+    }
+    // z = y_q - (first chunk) - (other chunks, fixed order)
+    const int nch = V.nchunk[q];
+    const double* pp = V.part + V.part_off[q];
+    double* psum = zx;  // the chunk rows are consumed: reuse as [2][64]
+    if (nch > 1) {
+      const int j = tid & (kSnCols - 1), h = tid / kSnCols;
+      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (j < c && h < 2) {
+        int k = 1 + h;
+        for (; k + 14 < nch; k += 16) {
+#pragma unroll
+          for (int u = 0; u < 8; ++u) acc[u] += __ldcg(pp + (int64_t)(k + 2 * u) * c + j);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (k + 2 * u < nch) acc[u] += __ldcg(pp + (int64_t)(k + 2 * u) * c + j);
+      }
+      if (h < 2) psum[h * kSnCols + j] = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+      __syncthreads();
+    }
+    for (int j = tid; j < c; j += blockDim.x) {
+      double v = __ldcg(x + f + j);
+      if (r1 > 0) v -= (seg[0][j] + seg[1][j]) + (seg[2][j] + seg[3][j]);
+      if (nch > 1) v -= psum[j] + psum[kSnCols + j];
+      zs[j] = v;
+    }
+    load_diag_finish(D, rinv, c);
+    diag_solve(D, rinv, zs, c, 1, false);
+    for (int j = tid; j < c; j += blockDim.x) {
+      x[f + j] = zs[j];
+      ring[(f + j - f_run) & (kRing - 1)] = zs[j];
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) atomicExch(xdone + q, 1);
+    if (V.queue)  // x_q is out: count it for every queued task whose rows q owns
+      for (int k = V.dep_ptr[q] + tid; k < V.dep_ptr[q + 1]; k += blockDim.x) {
+        const int d = V.dep[k];
+        if (in_queue(V, d) && atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
+      }
+    if (q > a) {  // the next block (one lower): first chunk into registers, diagonal block into shared memory
+      const int fn = V.sn_first[q - 1], cn = f - fn;
+      const int64_t rn = V.rows_ptr[q] - V.rows_ptr[q - 1], ldn = cn + rn;
+      const double* Pn = Lb + V.Lptr[q - 1];
+      const int r1n = (int)(rn < kChunkRows ? rn : (int64_t)kChunkRows);
+      if (r1n > 0) pre_bwd(R, Pn, cn, ldn, 0, r1n);
+      load_diag_start(D, Pn, cn, ldn);
+    }
+  }
+}
+
 // The same sweeps scheduled through the ready queue (single right-hand side).
 __global__ void __launch_bounds__(kSolveThreads) k_fwd_queued(const SweepView V, int* err) {
   __shared__ double D[kSnCols][kSnCols + 1];
   __shared__ double rinv[kSnCols];
   __shared__ double ys[kSnCols];
+  __shared__ double ring[kRing];
   __shared__ int task_id;
   const double* Lb = *V.Lbase;
   int phase = 0;
@@ -545,7 +721,12 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_queued(const SweepView V,
     if (t < 0) break;
     unsigned long long* rec = g_timeline_f ? g_timeline_f + 4 * (size_t)t : nullptr;
     if (rec && threadIdx.x == 0) rec[0] = gtime();
-    fwd_task(V, t, Lb, 1, err, D, rinv, ys, rec ? rec + 1 : nullptr);
+    if ((V.tasks[t].kind & 15) == 3) {
+      if (rec && threadIdx.x == 0) rec[1] = gtime();
+      fwd_leader(V, t, Lb, err, D, rinv, ys, ring);
+    } else {
+      fwd_task(V, t, Lb, 1, err, D, rinv, ys, rec ? rec + 1 : nullptr);
+    }
     if (rec && threadIdx.x == 0) { rec[2] = gtime(); rec[3] = smid(); }
   }
 }
@@ -555,6 +736,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_queued(const SweepView V,
   __shared__ double rinv[kSnCols];
   __shared__ double seg[4][kSnCols];
   __shared__ double zs[kSnCols + kChunkRows];
+  __shared__ double ring[kRing];
   __shared__ int task_id;
   const double* Lb = *V.Lbase;
   int phase = 0;
@@ -563,7 +745,12 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_queued(const SweepView V,
     if (t < 0) break;
     unsigned long long* rec = g_timeline_b ? g_timeline_b + 4 * (size_t)t : nullptr;
     if (rec && threadIdx.x == 0) rec[0] = gtime();
-    bwd_task(V, t, Lb, 1, err, D, rinv, seg, zs, rec ? rec + 1 : nullptr);
+    if ((V.tasks[t].kind & 15) == 3) {
+      if (rec && threadIdx.x == 0) rec[1] = gtime();
+      bwd_leader(V, t, Lb, err, D, rinv, seg, zs, ring);
+    } else {
+      bwd_task(V, t, Lb, 1, err, D, rinv, seg, zs, rec ? rec + 1 : nullptr);
+    }
     if (rec && threadIdx.x == 0) { rec[2] = gtime(); rec[3] = smid(); }
   }
 }
@@ -1311,22 +1498,30 @@ namespace {
 // kernels): per task its owner/target supernodes, per supernode the forward
 // chunk count it waits for, its row-chunk count and partial-sum offset.
 struct Sched {
-  std::vector<SolveTask> ft, bt;
+  std::vector<SolveTask> ft, bt;  // the claimable tasks (nf, nb of them), then the absorbed entries
   std::vector<int> ftp{0}, ftg, btp{0}, btg, expect, nch;
   std::vector<int64_t> poff;
+  int nf = 0, nb = 0;
 };
 
 // min_level > 0: supernodes below that level (swept by the subtree kernels)
-// get no tasks and feed no counts.
-void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0) {
+// get no tasks and feed no counts.  lead_level: runs of column blocks (at
+// least two, the first at or above that level) are swept by one leader task
+// (kind 3 | blocks << 4: forward at the run's first block, backward at its
+// last); the diagonal entries of the other blocks become absorbed entries
+// (kind 4) after the claimable tasks.  The targets / owners of a run block's
+// first chunk exclude the run's own blocks (applied through the leader's
+// ring).  Single right-hand side only (128-row first chunks).
+void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lead_level = INT_MAX) {
   const int nsn = S.nsn;
-  // distinct owner supernodes of rows [r0, r1) of s (rows ascending -> owners ascending)
+  // distinct owner supernodes of rows [r0, r1) of s above `skip_to` (rows ascending -> owners ascending)
   std::vector<int> tmp;
-  auto owners = [&](int s, int r0, int r1) {
+  auto owners = [&](int s, int r0, int r1, int skip_to = -1) {
     tmp.clear();
     const int* rows = S.sn_rows.data() + S.sn_rows_ptr[s];
     for (int i = r0; i < r1; ++i) {
       const int ow = S.col2sn[rows[i]];
+      if (ow <= skip_to) continue;
       if (tmp.empty() || tmp.back() != ow) tmp.push_back(ow);
     }
   };
@@ -1338,6 +1533,20 @@ void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0) {
     o.nch[s] = ceil_div(r, CH);
     o.poff[s + 1] = o.poff[s] + (int64_t)o.nch[s] * (S.sn_first[s + 1] - S.sn_first[s]);
   }
+  // runs with a leader: run_a[s] = first block, run_e[s] = last block (-1: none)
+  std::vector<int> run_a(nsn, -1), run_e(nsn, -1);
+  if (lead_level < INT_MAX && CH == kChunkRows) {
+    const std::vector<int> rf = block_run_first(S);
+    for (int s0 = 0; s0 < nsn;) {
+      int e = s0;
+      while (e + 1 < nsn && rf[e + 1] == s0) ++e;
+      if (e > s0 && S.sn_level[s0] >= std::max(lead_level, min_level))
+        for (int q = s0; q <= e; ++q) { run_a[q] = s0; run_e[q] = e; }
+      s0 = e + 1;
+    }
+  }
+  std::vector<SolveTask> abs_t;
+  std::vector<std::vector<int>> abs_g;
   // forward: bottom-up levels; per supernode its diagonal task (with the first
   // row chunk), then the other chunks
   for (int l = std::max(0, min_level); l < S.nlevels; ++l)
@@ -1346,12 +1555,33 @@ void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0) {
       const int r = (int)(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]);
       for (int r0 = 0; r0 < std::max(r, 1); r0 += CH) {
         const int r1 = std::min(r, r0 + CH);
+        if (r0 == 0 && run_a[s] >= 0) {
+          owners(s, 0, r1, run_e[s]);
+          for (int ow : tmp) o.expect[ow]++;
+          if (s == run_a[s]) {
+            o.ft.push_back({s, 3 | ((run_e[s] - s + 1) << 4), 0, r1});
+            o.ftg.insert(o.ftg.end(), tmp.begin(), tmp.end());
+            o.ftp.push_back((int)o.ftg.size());
+          } else {
+            abs_t.push_back({s, 4, 0, r1});
+            abs_g.push_back(tmp);
+          }
+          continue;
+        }
         o.ft.push_back({s, r0 == 0 ? 0 : 1, r0, r1});
         owners(s, r0, r1);
         for (int ow : tmp) { o.ftg.push_back(ow); o.expect[ow]++; }
         o.ftp.push_back((int)o.ftg.size());
       }
     }
+  o.nf = (int)o.ft.size();
+  for (size_t k = 0; k < abs_t.size(); ++k) {
+    o.ft.push_back(abs_t[k]);
+    o.ftg.insert(o.ftg.end(), abs_g[k].begin(), abs_g[k].end());
+    o.ftp.push_back((int)o.ftg.size());
+  }
+  abs_t.clear();
+  abs_g.clear();
   // backward: top-down levels; per supernode its other chunks, then the
   // diagonal task with the first chunk
   for (int l = S.nlevels - 1; l >= std::max(0, min_level); --l)
@@ -1366,11 +1596,29 @@ void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0) {
         o.btp.push_back((int)o.btg.size());
       }
       const int r1 = std::min(r, CH);
+      if (run_a[s] >= 0) {
+        owners(s, 0, r1, run_e[s]);
+        if (s == run_e[s]) {
+          o.bt.push_back({s, 3 | ((run_e[s] - run_a[s] + 1) << 4), 0, r1});
+          o.btg.insert(o.btg.end(), tmp.begin(), tmp.end());
+          o.btp.push_back((int)o.btg.size());
+        } else {
+          abs_t.push_back({s, 4, 0, r1});
+          abs_g.push_back(tmp);
+        }
+        continue;
+      }
       o.bt.push_back({s, 0, 0, r1});
       owners(s, 0, r1);
       o.btg.insert(o.btg.end(), tmp.begin(), tmp.end());
       o.btp.push_back((int)o.btg.size());
     }
+  o.nb = (int)o.bt.size();
+  for (size_t k = 0; k < abs_t.size(); ++k) {
+    o.bt.push_back(abs_t[k]);
+    o.btg.insert(o.btg.end(), abs_g[k].begin(), abs_g[k].end());
+    o.btp.push_back((int)o.btg.size());
+  }
 }
 // Ready-queue data of a schedule: diagonal task per supernode (forward,
 // backward), backward completion counts and dependants, initially ready
@@ -1383,10 +1631,12 @@ void build_queue_data(const Sched& a, int nsn, QueueData& q, int f_hi, int b_lo)
   q.fdiag.assign(nsn, -1);
   q.bdiag.assign(nsn, -1);
   q.bneed.assign(a.bt.size(), 0);
+  // diagonal entry per supernode: its diagonal task, its run's leader, or its absorbed entry
+  auto diag_kind = [](int k) { k &= 15; return k == 0 || k == 3 || k == 4; };
   for (size_t i = 0; i < a.ft.size(); ++i)
-    if (a.ft[i].kind == 0) q.fdiag[a.ft[i].s] = (int)i;
+    if (diag_kind(a.ft[i].kind)) q.fdiag[a.ft[i].s] = (int)i;
   for (size_t i = 0; i < a.bt.size(); ++i)
-    if (a.bt[i].kind == 0) q.bdiag[a.bt[i].s] = (int)i;
+    if (diag_kind(a.bt[i].kind)) q.bdiag[a.bt[i].s] = (int)i;
   q.dptr.assign(nsn + 1, 0);
   for (size_t i = 0; i < a.bt.size(); ++i) {
     const SolveTask& T = a.bt[i];
@@ -1403,7 +1653,7 @@ void build_queue_data(const Sched& a, int nsn, QueueData& q, int f_hi, int b_lo)
   q.binit.clear();
   for (int i = 0; i < f_hi; ++i)
     if (a.ft[i].kind == 0 && a.expect[a.ft[i].s] == 0) q.finit.push_back(i);
-  for (int i = b_lo; i < (int)a.bt.size(); ++i)
+  for (int i = b_lo; i < a.nb; ++i)
     if (q.bneed[i] == 0) q.binit.push_back(i);
 }
 
@@ -1411,8 +1661,8 @@ void build_queue_data(const Sched& a, int nsn, QueueData& q, int f_hi, int b_lo)
 // bottom-up schedule), backward tasks below it (a suffix of the top-down one)
 void split_ranges(const Sched& a, const Symbolic& S, int split, int& f_hi, int& b_lo) {
   f_hi = 0;
-  while (f_hi < (int)a.ft.size() && S.sn_level[a.ft[f_hi].s] < split) ++f_hi;
-  b_lo = (int)a.bt.size();
+  while (f_hi < a.nf && S.sn_level[a.ft[f_hi].s] < split) ++f_hi;
+  b_lo = a.nb;
   while (b_lo > 0 && S.sn_level[a.bt[b_lo - 1].s] < split) --b_lo;
 }
 
@@ -1463,20 +1713,48 @@ void upload_queue_plan(const Sched& a, const Symbolic& S, int split, QueuePlan& 
 // Forward: queue phase, then the ordered phase; backward: the other way
 // round, the ordered tasks' completions feeding the queue.  Returns an empty
 // string or the first violation.
-std::string check_schedule(const Symbolic& S, int CH, int split, int min_level = 0) {
+std::string check_schedule(const Symbolic& S, int CH, int split, int min_level = 0, int lead_level = INT_MAX) {
   Sched a;
-  build_sched(S, CH, a, min_level);
+  build_sched(S, CH, a, min_level, lead_level);
   int f_hi = 0, b_lo = 0;
   split_ranges(a, S, split, f_hi, b_lo);
   QueueData q;
   build_queue_data(a, S.nsn, q, f_hi, b_lo);
-  const int nsn = S.nsn, nf = (int)a.ft.size(), nb = (int)a.bt.size();
+  const int nsn = S.nsn, nf = a.nf, nb = a.nb;
+  auto first_rows = [&](int s) { return (int)std::min<int64_t>(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s], CH); };
   {
     std::vector<int> ready(nsn, 0), ydone(nsn, 0), seen(nf, 0);
     std::vector<int> queue(q.finit);
+    // run leaders in progress: (next block, last block)
+    std::vector<std::pair<int, int>> leaders;
+    auto feed = [&](int t) {  // the targets of entry t count one input more
+      for (int k = a.ftp[t]; k < a.ftp[t + 1]; ++k) {
+        const int o = a.ftg[k];
+        if (++ready[o] == a.expect[o] && q.fdiag[o] < f_hi) queue.push_back(q.fdiag[o]);
+      }
+    };
+    auto advance = [&]() {  // every leader as far as its inputs allow
+      for (bool moved = true; moved;) {
+        moved = false;
+        for (auto& L : leaders)
+          while (L.first <= L.second && ready[L.first] == a.expect[L.first]) {
+            ydone[L.first] = 1;
+            feed(q.fdiag[L.first]);
+            ++L.first;
+            moved = true;
+          }
+      }
+    };
     auto run = [&](int t, bool queued) -> std::string {
       if (seen[t]++) return "forward: task handed out twice";
       const SolveTask& T = a.ft[t];
+      if ((T.kind & 15) == 3) {
+        if (queued) return "forward queue: a run leader in the queue";
+        leaders.push_back({T.s, T.s + (T.kind >> 4) - 1});
+        advance();
+        return std::string();
+      }
+      advance();
       if (T.kind == 0) {
         if (ready[T.s] != a.expect[T.s]) return queued ? "forward queue: diagonal task before its inputs"
                                                        : "forward: diagonal task claimed before its inputs";
@@ -1485,13 +1763,12 @@ std::string check_schedule(const Symbolic& S, int CH, int split, int min_level =
         const int nx = std::max(1, (r + CH - 1) / CH) - 1;
         for (int k = 0; k < nx; ++k)
           if (t + 1 + k < f_hi) queue.push_back(t + 1 + k);
-      } else if (!ydone[T.s]) {
-        return "forward: chunk before its diagonal task";
+      } else if (T.kind == 1) {
+        if (!ydone[T.s]) return "forward: chunk before its diagonal block is solved";
+      } else {
+        return "forward: an absorbed entry among the claimable tasks";
       }
-      for (int k = a.ftp[t]; k < a.ftp[t + 1]; ++k) {
-        const int o = a.ftg[k];
-        if (++ready[o] == a.expect[o] && q.fdiag[o] < f_hi) queue.push_back(q.fdiag[o]);
-      }
+      feed(t);
       return std::string();
     };
     for (size_t h = 0; h < queue.size(); ++h) {
@@ -1504,13 +1781,49 @@ std::string check_schedule(const Symbolic& S, int CH, int split, int min_level =
       const std::string w = run(t, false);
       if (!w.empty()) return w;
     }
+    advance();
+    for (const auto& L : leaders)
+      if (L.first <= L.second) return "forward: a run leader cannot finish";
+    for (int s = 0; s < nsn; ++s)
+      if (S.sn_level[s] >= min_level && !ydone[s]) return "forward: a supernode never solved";
   }
   {
     std::vector<int> xdone(nsn, 0), cdone(nsn, 0), cnt(nb, 0), seen(nb, 0);
     std::vector<int> queue(q.binit);
+    std::vector<std::pair<int, int>> leaders;  // (next block, first block), top-down
+    auto count = [&](int d) {
+      if (d < nb && ++cnt[d] == q.bneed[d] && d >= b_lo) queue.push_back(d);
+    };
+    auto solved = [&](int s) {
+      xdone[s] = 1;
+      for (int k = q.dptr[s]; k < q.dptr[s + 1]; ++k) count(q.dep[k]);
+    };
+    auto inputs_done = [&](int t, int s) {
+      for (int k = a.btp[t]; k < a.btp[t + 1]; ++k)
+        if (!xdone[a.btg[k]]) return false;
+      return cdone[s] == std::max(a.nch[s], 1) - 1 || (first_rows(s) == 0 && cdone[s] == 0);
+    };
+    auto advance = [&]() {
+      for (bool moved = true; moved;) {
+        moved = false;
+        for (auto& L : leaders)
+          while (L.first >= L.second && inputs_done(q.bdiag[L.first], L.first)) {
+            solved(L.first);
+            --L.first;
+            moved = true;
+          }
+      }
+    };
     auto run = [&](int t, bool queued) -> std::string {
       if (seen[t]++) return "backward: task handed out twice";
       const SolveTask& T = a.bt[t];
+      if ((T.kind & 15) == 3) {
+        if (queued) return "backward queue: a run leader in the queue";
+        leaders.push_back({T.s, T.s - (T.kind >> 4) + 1});
+        advance();
+        return std::string();
+      }
+      advance();
       if (queued) {
         if (cnt[t] != q.bneed[t]) return "backward queue: task before its inputs";
       } else {
@@ -1520,14 +1833,11 @@ std::string check_schedule(const Symbolic& S, int CH, int split, int min_level =
       }
       if (T.kind == 1) {
         cdone[T.s]++;
-        const int d = q.bdiag[T.s];
-        if (++cnt[d] == q.bneed[d] && d >= b_lo) queue.push_back(d);
+        count(q.bdiag[T.s]);
+      } else if (T.kind == 0) {
+        solved(T.s);
       } else {
-        xdone[T.s] = 1;
-        for (int k = q.dptr[T.s]; k < q.dptr[T.s + 1]; ++k) {
-          const int d = q.dep[k];
-          if (++cnt[d] == q.bneed[d] && d >= b_lo) queue.push_back(d);
-        }
+        return "backward: an absorbed entry among the claimable tasks";
       }
       return std::string();
     };
@@ -1535,12 +1845,17 @@ std::string check_schedule(const Symbolic& S, int CH, int split, int min_level =
       const std::string w = run(t, false);
       if (!w.empty()) return w;
     }
+    advance();
+    for (const auto& L : leaders)
+      if (L.first >= L.second) return "backward: a run leader cannot finish";
     for (size_t h = 0; h < queue.size(); ++h) {
       if (queue[h] < b_lo) return "backward queue: task outside the queue range";
       const std::string w = run(queue[h], true);
       if (!w.empty()) return w;
     }
     if ((int)queue.size() != nb - b_lo) return "backward queue: not every queued task handed out";
+    for (int s = 0; s < nsn; ++s)
+      if (S.sn_level[s] >= min_level && !xdone[s]) return "backward: a supernode never solved";
   }
   return std::string();
 }
@@ -1611,19 +1926,20 @@ std::string check_trees(const Symbolic& S, int level) {
 }
 
 // The single-column plan at a subtree level and queue split.
-void upload_tree_plan(temf_ctx& c, int level, int split) {
+void upload_tree_plan(temf_ctx& c, int level, int split, bool leaders) {
   const Symbolic& S = c.sym;
   TreePlan& T = c.splan.tree;
   cudaStream_t st = c.stream;
   const std::vector<int2> trees = build_trees(S, level);
   Sched a;
-  build_sched(S, kChunkRows, a, level);
+  build_sched(S, kChunkRows, a, level, leaders ? std::max(level, split) : INT_MAX);
   T.level = level;
+  T.leaders = leaders;
   T.ntree = (int)trees.size();
   if (trees.empty()) T.trees.alloc(1);
   else T.trees.upload(trees.data(), trees.size(), st);
-  T.n_ftask = (int)a.ft.size();
-  T.n_btask = (int)a.bt.size();
+  T.n_ftask = a.nf;
+  T.n_btask = a.nb;
   auto up_tasks = [&](DBuf<SolveTask>& d, const std::vector<SolveTask>& v) {
     if (v.empty()) d.alloc(1);
     else d.upload(v.data(), v.size(), st);
@@ -1695,7 +2011,7 @@ void build_solve_plan(temf_ctx& c) {
   P.macc_off.upload(aoff.data(), aoff.size(), st);
   upload_queue_plan(b, S, default_split(S), P.qm, st);
   P.sync.alloc(4 * (size_t)nsn + 8);  // + 2 claim counters of the task kernels, 2 of the subtree kernels
-  upload_tree_plan(c, default_tree_level(S), default_split(S));
+  upload_tree_plan(c, default_tree_level(S), default_split(S), true);
   P.tree.tuned = false;
   TEMF_CUDA(cudaStreamSynchronize(st));
 }
@@ -2116,7 +2432,7 @@ void solve_timeline(temf_ctx& c, int slot, const double* b_perm, int64_t cap, un
     unsigned long long* o = out + 8 * i;
     for (int q = 0; q < 4; ++q) o[q] = h[4 * i + q];
     o[4] = (unsigned long long)t.s;
-    o[5] = (unsigned long long)t.kind;
+    o[5] = (unsigned long long)(t.kind & 15);
     o[6] = (unsigned long long)t.r0;
     o[7] = (unsigned long long)c.sym.sn_level[t.s];
   }
@@ -2170,6 +2486,8 @@ std::string check_schedules(const Symbolic& S) {
   for (int sp : splits) {
     std::string w = check_schedule(S, kChunkRows, sp);
     if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ": " + w;
+    w = check_schedule(S, kChunkRows, sp, 0, sp);
+    if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ", run leaders: " + w;
     w = check_schedule(S, kChunkRowsMulti, sp);
     if (!w.empty()) return "64-row chunks, split " + std::to_string(sp) + ": " + w;
   }
@@ -2181,6 +2499,9 @@ std::string check_schedules(const Symbolic& S) {
     for (int sp : split_candidates(S, l)) {
       w = check_schedule(S, kChunkRows, sp, l);
       if (!w.empty()) return "subtree level " + std::to_string(l) + ", split " + std::to_string(sp) + ": " + w;
+      w = check_schedule(S, kChunkRows, sp, l, std::max(l, sp));
+      if (!w.empty())
+        return "subtree level " + std::to_string(l) + ", split " + std::to_string(sp) + ", run leaders: " + w;
     }
   }
   return std::string();
@@ -2281,8 +2602,8 @@ static int tune_tree(temf_ctx& c, int slot) {
   TEMF_CUDA(cudaEventCreate(&e1));
   std::vector<int> lv_c, sp_c;
   std::vector<double> ms_c;
-  auto time_plan = [&](int level, int split) {
-    upload_tree_plan(c, level, split);
+  auto time_plan = [&](int level, int split, bool leaders = true) {
+    upload_tree_plan(c, level, split, leaders);
     double tot = 0.0;
     for (int rep = 0; rep < 4; ++rep) {
       TEMF_CUDA(cudaMemcpyAsync(x.p, ones.p, vec * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -2320,9 +2641,15 @@ static int tune_tree(temf_ctx& c, int slot) {
     sms.push_back(ms);
     if (ms < best) { best = ms; best_split = sp; }
   }
+  // and the chosen plan without run leaders (every block handed from CTA to CTA)
+  bool best_leaders = true;
+  {
+    const double ms = time_plan(best_level, best_split, false);
+    if (ms < best) { best = ms; best_leaders = false; }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  upload_tree_plan(c, best_level, best_split);
+  upload_tree_plan(c, best_level, best_split, best_leaders);
   T.q.tune_ms = sms;
   T.q.tune_split = sps;
   T.tune_level = lv_c;
@@ -2331,7 +2658,7 @@ static int tune_tree(temf_ctx& c, int slot) {
   return best_split;
 }
 
-void set_tree_plan(temf_ctx& c, int level, int split) {
+void set_tree_plan(temf_ctx& c, int level, int split, bool leaders) {
   const Symbolic& S = c.sym;
   if (level < 0 || level > S.nlevels) throw ArgError("subtree level out of range");
   if (split < 0 || split > S.nlevels) throw ArgError("queue split level out of range");
@@ -2339,7 +2666,7 @@ void set_tree_plan(temf_ctx& c, int level, int split) {
     const std::string w = check_trees(S, level);
     if (!w.empty()) throw StateError("subtrees below level " + std::to_string(level) + ": " + w);
   }
-  upload_tree_plan(c, level, split);
+  upload_tree_plan(c, level, split, leaders);
   c.splan.tree.q.tuned = true;
   c.splan.tree.tuned = true;
 }

@@ -96,7 +96,7 @@ int models_grid(bool forward);
 int tune_solve(temf_ctx& c, int slot, int nrhs);
 // The single-column plan set explicitly: subtree level (0: none) and queue
 // split level; checked on the host first.
-void set_tree_plan(temf_ctx& c, int level, int split);
+void set_tree_plan(temf_ctx& c, int level, int split, bool leaders);
 // Profiling aid: one single-column solve of b (permuted order) in `slot` with
 // a per-task timeline (8 words per task; see solve.cu).
 void solve_timeline(temf_ctx& c, int slot, const double* b_perm, int64_t cap, unsigned long long* out,

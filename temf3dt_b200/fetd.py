@@ -312,9 +312,12 @@ class FetdGPU:
         self._ck(self._L.temf_solve_schedule(self._h, nrhs, C.byref(sp), C.byref(tu)), "temf_solve_schedule")
         return sp.value, bool(tu.value)
 
-    def set_solve_plan(self, tree_level: int, split: int) -> None:
-        """Single-column sweep plan: subtree level (0 = no subtrees) and queue split level."""
-        self._ck(self._L.temf_set_solve_plan(self._h, int(tree_level), int(split)), "temf_set_solve_plan")
+    def set_solve_plan(self, tree_level: int, split: int, run_leaders: bool = True) -> None:
+        """Single-column sweep plan: subtree level (0 = no subtrees), queue
+        split level, and whether runs of column blocks above the split are
+        swept by one leader task."""
+        self._ck(self._L.temf_set_solve_plan(self._h, int(tree_level), int(split), 1 if run_leaders else 0),
+                 "temf_set_solve_plan")
 
     def set_wait_limit(self, spins: int = 0, inject_unmet_wait: bool = False) -> None:
         """Polls a device wait may spin before it gives up (0: the default);
@@ -324,11 +327,12 @@ class FetdGPU:
                  "temf_set_wait_limit")
 
     def solve_plan(self) -> Dict[str, int]:
-        """The single-column sweep plan in use: subtree level, queue split, subtrees, tuned."""
-        lv, sp, nt, tu = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
-        self._ck(self._L.temf_solve_plan(self._h, C.byref(lv), C.byref(sp), C.byref(nt), C.byref(tu)),
-                 "temf_solve_plan")
-        return {"tree_level": lv.value, "split": sp.value, "n_trees": nt.value, "tuned": bool(tu.value)}
+        """The single-column sweep plan in use: subtree level, queue split, run leaders, subtrees, tuned."""
+        lv, sp, ld, nt, tu = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
+        self._ck(self._L.temf_solve_plan(self._h, C.byref(lv), C.byref(sp), C.byref(ld), C.byref(nt),
+                                         C.byref(tu)), "temf_solve_plan")
+        return {"tree_level": lv.value, "split": sp.value, "run_leaders": bool(ld.value), "n_trees": nt.value,
+                "tuned": bool(tu.value)}
 
     def solve_timeline(self, slot: int):
         """Per-task timeline of one single-column solve (profiling aid):

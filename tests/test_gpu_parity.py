@@ -100,8 +100,10 @@ def test_tuned_sweep_schedules_solve_to_backward_error(small, nrhs):
 def test_subtree_sweeps_solve_to_backward_error(small, level):
     """Single-column solves with the supernodes below `level` swept as whole
     subtrees (one warp each, no waits) before and after the persistent task
-    sweeps, with and without the ready queue above them: backward error 1e-12,
-    and the same solution as the plan without subtrees to that tolerance."""
+    sweeps, with and without the ready queue above them, and with and without
+    run leaders (one CTA walking the column blocks of a wide supernode):
+    backward error 1e-12, and the same solution as the plan without subtrees
+    to that tolerance."""
     m, om, g, info = small
     dt = 1e-6
     A = 3 * O.full_from_upper(om.B) + 2 * dt * O.full_from_upper(om.C)
@@ -110,15 +112,17 @@ def test_subtree_sweeps_solve_to_backward_error(small, level):
     b = A @ np.random.default_rng(level).standard_normal(om.n)
     nb = np.linalg.norm(b)
     try:
-        g.set_solve_plan(0, 0)
+        g.set_solve_plan(0, 0, run_leaders=False)
         x0 = g.solve(1, b)
         for split in (L, L + 3):
-            g.set_solve_plan(L, split)
-            plan = g.solve_plan()
-            assert plan["tree_level"] == L and plan["split"] == split and plan["n_trees"] > 0
-            x = g.solve(1, b)
-            assert np.linalg.norm(A @ x - b) <= 1e-12 * nb
-            assert np.linalg.norm(A @ (x - x0)) <= 2e-12 * nb
+            for leaders in (True, False):
+                g.set_solve_plan(L, split, run_leaders=leaders)
+                plan = g.solve_plan()
+                assert plan["tree_level"] == L and plan["split"] == split and plan["n_trees"] > 0
+                assert plan["run_leaders"] == leaders
+                x = g.solve(1, b)
+                assert np.linalg.norm(A @ x - b) <= 1e-12 * nb
+                assert np.linalg.norm(A @ (x - x0)) <= 2e-12 * nb
     finally:
         g.tune_solve(1, 1)
 
