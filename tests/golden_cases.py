@@ -197,3 +197,29 @@ def oracle_model_with(model, oc):
     mesh = dict(nod_cor=model.mesh.nod_cor, tet_vex=model.mesh.tet_vex, tet_phy=model.mesh.tet_phy,
                 src_vex=model.mesh.src_vex, src_phy=model.mesh.src_phy)
     return O.build_model(mesh, oc)
+
+
+def golden_field_report(steps, times, dbz, trial_errors, gold, sp_double, rtol=6e-4):
+    """Row-by-row comparison of a run with a shipped .field (step, time, dB_z/dt
+    printed to 4 digits).  Returns (first row whose time differs, or the row
+    count when none does; the trial error that decided that row, or None;
+    largest relative dB_z/dt difference over the agreeing rows, away from the
+    sign change).  Trial k runs at step (k+1) * sp_double
+    (src/FETD_FWD.f90:1312), so the first row after a differing decision is
+    decided by the last trial at or before it."""
+    n = min(len(times), len(gold))
+    same = np.isclose(np.asarray(times[:n]), gold[:n, 1], rtol=rtol, atol=0) | (gold[:n, 1] == 0)
+    first = int(np.argmin(same)) if not same.all() else n
+    if first == n and len(times) != len(gold):
+        first = n            # one run ends earlier: the rows after n differ
+    decided = None
+    if first < max(len(times), len(gold)) and len(trial_errors):
+        step = int(steps[min(first, len(steps) - 1)])
+        k = step // sp_double - 1
+        if 0 <= k < len(trial_errors):
+            decided = float(trial_errors[k])
+    gd = gold[:first, 2]
+    v = np.asarray(dbz[:first])
+    big = np.abs(gd) >= 1e-3 * np.abs(gd).max()
+    rel = float((np.abs(v[big] - gd[big]) / np.abs(gd[big])).max()) if big.any() else 0.0
+    return first, decided, rel

@@ -227,23 +227,26 @@ def test_src_small_example_matches_reference_field():
 def test_linux_examples_match_reference_field(name):
     """The reference's LINUX examples (108k edges, 918/922 rows to t = 0.1 s)
     on the GPU, replaying the schedule of the build that wrote them, vs the
-    shipped .field (4 printed digits)."""
+    shipped .field (4 printed digits), row by row: every row's time (the
+    accept/reject schedule) and dB_z/dt to the print.  A schedule may only
+    part from the file at a trial whose error estimate sits at the 1e-4
+    threshold within rounding (then either decision is the reference's own
+    behaviour); the rows up to it must match."""
+    from tests.golden_cases import golden_field_report
     fx = load_fixture(name)
     mesh, ctl, _ = host_model_from_fixture(fx)
     gold = fx["field"]
     with fetd.FetdGPU(0) as g:
         fetd.load_case(g, mesh, ctl)
         out = g.run(ctl.sp_division, ctl.sp_double, ctl.sp_dblesize, ctl.time_maximum, legacy_linux=True)
-    # compare up to the first trial whose accept/reject differs (error near 1e-4)
-    n = min(len(out.steps), len(gold))
-    same = np.isclose(out.times[:n], gold[:n, 1], rtol=6e-4, atol=0) | (gold[:n, 1] == 0)
-    first_diff = int(np.argmin(same)) if not same.all() else n
-    assert first_diff >= 400, first_diff
-    v = out.fields[:first_diff, 0, 5]
-    gd = gold[:first_diff, 2]
-    big = np.abs(gd) >= 1e-3 * np.abs(gd).max()     # away from the sign change (4 digits)
-    rel = np.abs(v[big] - gd[big]) / np.abs(gd[big])
-    assert rel.max() < 6e-4, rel.max()
+    first, decided, rel = golden_field_report(out.steps, out.times, out.fields[:, 0, 5], out.trial_errors, gold,
+                                              ctl.sp_double)
+    near = sorted(np.abs(out.trial_errors / 1e-4 - 1.0))[:3]
+    print("%s: rows %d / %d, first differing row %d, its trial error %s, dBz/dt rel %.2e, closest trials %s"
+          % (name, len(out.steps), len(gold), first, decided, rel, near))
+    assert rel < 6e-4, rel
+    if first < len(gold) or len(out.steps) != len(gold):
+        assert decided is not None and abs(decided / 1e-4 - 1.0) <= 1e-3, (first, decided)
 
 
 def test_multi_rhs_columns_match_single_runs():
