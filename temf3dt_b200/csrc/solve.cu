@@ -581,7 +581,7 @@ __device__ void fwd_leader(const SweepView& V, int t, const double* Lb, int* err
     __syncthreads();
     for (int j = tid; j < c; j += blockDim.x) {
       const int slot = (f + j - f_run) & (kRing - 1);
-      ys[j] = __ldcg(x + f + j) - ring[slot];
+      ys[j] = __ldcg(x + f + j) + ring[slot];  // the ring holds the negated in-run contributions
       ring[slot] = 0.0;
     }
     load_diag_finish(D, rinv, c);
