@@ -37,10 +37,11 @@ struct CtxExtra {
   bool adj_valid = false;
   // PARDISO shim: user upper-CSR position -> CSR position of the permuted full pattern
   std::vector<int> shim_map;  // nnz_user (index into pattern) or -1
+  std::vector<int> shim_map_up;  // the mirrored (upper) position of each off-diagonal entry, -1 on the diagonal
   int shim_n = 0, shim_nnz = 0;
   int shim_max = 0;
   DBuf<double> shim_vals;     // user values on device
-  DBuf<int> shim_map_d;
+  DBuf<int> shim_map_d, shim_map_up_d;
   DBuf<double> vec;           // scratch vectors for host-facing solves
   DBuf<double*> lb;           // device word holding the factor base for host solves
   DBuf<double> shim_full[2];  // PARDISO shim: the user's matrix of each slot on the permuted pattern
@@ -1405,6 +1406,7 @@ int temf_pardiso_direct_1(temf_ctx* c, int num_m, int symm, int n, int nnz, cons
       // map each user entry (upper, 1-based) onto the permuted lower pattern
       const Pattern& P = c->pat;
       X.shim_map.assign(nnz, -1);
+      X.shim_map_up.assign(nnz, -1);
       for (int i = 0; i < n; ++i) {
         for (int q = ia[i] - 1; q < ia[i + 1] - 1; ++q) {
           const int j = ja[q] - 1;
@@ -1415,11 +1417,19 @@ int temf_pardiso_direct_1(temf_ctx* c, int num_m, int symm, int n, int nnz, cons
           const int* f = std::lower_bound(b, e, pj);
           if (f == e || *f != pj) throw ArgError("matrix error: entry outside the mesh's step-matrix pattern");
           X.shim_map[q] = (int)(f - P.col.data());
+          if (pi != pj) {  // the same value at (pj, pi): the full symmetric matrix for the refinement
+            const int* b2 = P.col.data() + P.rowptr[pj];
+            const int* e2 = P.col.data() + P.rowptr[pj + 1];
+            const int* f2 = std::lower_bound(b2, e2, pi);
+            if (f2 == e2 || *f2 != pi) throw ArgError("matrix error: pattern not symmetric");
+            X.shim_map_up[q] = (int)(f2 - P.col.data());
+          }
         }
       }
       X.shim_n = n;
       X.shim_nnz = nnz;
       X.shim_map_d.upload(X.shim_map.data(), X.shim_map.size(), c->stream);
+      X.shim_map_up_d.upload(X.shim_map_up.data(), X.shim_map_up.size(), c->stream);
     }
     // place the user's values on the permuted full pattern (kept with the
     // slot: the refinement of an indefinite factor applies them)
@@ -1429,6 +1439,8 @@ int temf_pardiso_direct_1(temf_ctx* c, int num_m, int symm, int n, int nnz, cons
     if (full.n < (size_t)c->pat.nnz) full.alloc(c->pat.nnz);
     TEMF_CUDA(cudaMemsetAsync(full.p, 0, c->pat.nnz * sizeof(double), c->stream));
     k_scatter_user<<<ceil_div(nnz, 256), 256, 0, c->stream>>>(nnz, X.shim_map_d.p, uv.p, full.p);
+    TEMF_CHECK_LAUNCH();
+    k_scatter_user<<<ceil_div(nnz, 256), 256, 0, c->stream>>>(nnz, X.shim_map_up_d.p, uv.p, full.p);
     TEMF_CHECK_LAUNCH();
     // not positive definite: the indefinite mode, as the reference retries with
     // mtype -2 (src/FETD_UTILITY.f90:923-935); the positive return is its warning
