@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(kFacThreads) k_potrf(
     int* __restrict__ status, double* __restrict__ sgn) {
   constexpr int CB = kSnCols;
   __shared__ double D[CB][CB + 1];
-  __shared__ double sk[CB];
+  __shared__ double diag[CB];  // L_kk, written into D after the loop
   __shared__ double d0[CB];
   const int s = level_sn[blockIdx.x];
   const int f = sn_first[s];
@@ -75,38 +75,44 @@ __global__ void __launch_bounds__(kFacThreads) k_potrf(
   __syncthreads();
   if (tid < c) d0[tid] = fabs(D[tid][tid]);
   __syncthreads();
+  // Right-looking, two barriers per column: every thread derives the pivot
+  // from the same shared value (the diagonal itself is written at the end),
+  // the column is scaled, then the trailing triangle is updated on a 8 x 16
+  // thread grid.
+  const int tx = tid & 15, ty = tid >> 4;
   for (int k = 0; k < c; ++k) {
-    if (tid == 0) {
-      double d = D[k][k];
-      double s = 1.0;
-      if (!(d > 0.0)) atomicMin(status, f + k + 1);  // non-positive or NaN pivot: record
-      if (sgn) {
-        s = d < 0.0 ? -1.0 : 1.0;
-        d = fabs(d);
-        const double tau = kPivotTol * (d0[k] > 0.0 ? d0[k] : 1.0);
-        if (!(d >= tau) || !(d <= 1e300)) {  // cancelled, NaN or infinite pivot: perturb
-          d = tau;
-          atomicAdd(status + 2, 1);
-        }
-        sgn[f + k] = s;
-      } else if (!(d > 0.0)) {
-        d = 1.0;  // continue with 1; the factor is reported invalid
+    const double a = D[k][k];
+    double d = a, s = 1.0;
+    bool perturbed = false;
+    if (sgn) {
+      s = d < 0.0 ? -1.0 : 1.0;
+      d = fabs(d);
+      const double tau = kPivotTol * (d0[k] > 0.0 ? d0[k] : 1.0);
+      if (!(d >= tau) || !(d <= 1e300)) {  // cancelled, NaN or infinite pivot: perturb
+        d = tau;
+        perturbed = true;
       }
-      D[k][k] = sqrt(d);
-      sk[k] = s;
+    } else if (!(d > 0.0)) {
+      d = 1.0;  // continue with 1; the factor is reported invalid
     }
+    const double lkk = sqrt(d);
+    if (tid == 0) {
+      if (!(a > 0.0)) atomicMin(status, f + k + 1);  // non-positive or NaN pivot: record
+      if (perturbed) atomicAdd(status + 2, 1);
+      if (sgn) sgn[f + k] = s;
+      diag[k] = lkk;
+    }
+    const double inv = 1.0 / (lkk * s);
+    for (int i = k + 1 + tid; i < c; i += blockDim.x) D[i][k] *= inv;
     __syncthreads();
-    const double piv = D[k][k] * sk[k];
-    for (int i = k + 1 + tid; i < c; i += blockDim.x) D[i][k] /= piv;
-    __syncthreads();
-    const int m = c - k - 1;
-    const double s = sk[k];
-    for (int idx = tid; idx < m * m; idx += blockDim.x) {
-      const int jj = k + 1 + idx / m, ii = k + 1 + idx % m;
-      if (ii >= jj) D[ii][jj] -= D[ii][k] * s * D[jj][k];
+    for (int ii = k + 1 + ty; ii < c; ii += 8) {
+      const double lik = D[ii][k] * s;
+      for (int jj = k + 1 + tx; jj <= ii; jj += 16) D[ii][jj] -= lik * D[jj][k];
     }
     __syncthreads();
   }
+  if (tid < c) D[tid][tid] = diag[tid];
+  __syncthreads();
   for (int idx = tid; idx < c * c; idx += blockDim.x) {
     const int j = idx / c, i = idx % c;
     if (i >= j) P[(int64_t)j * ld + i] = D[i][j];
