@@ -551,6 +551,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_persistent(
 //            the run, takes the run rows' x from the ring, solves, publishes.
 // ---------------------------------------------------------------------------
 constexpr int kRing = 256;  // run columns held in shared memory (>= 64 + 128 live)
+// Most run leaders spanning any one level (a leader holds a CTA while it waits
+// for chunk tasks claimed after it; the persistent kernels keep hundreds of
+// CTAs resident, so the chunk tasks always find CTAs).
+constexpr int kMaxLeaders = 24;
 
 __device__ __forceinline__ int leader_blocks(const SolveTask& T) { return T.kind >> 4; }
 
@@ -1533,16 +1537,32 @@ void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lea
     o.nch[s] = ceil_div(r, CH);
     o.poff[s + 1] = o.poff[s] + (int64_t)o.nch[s] * (S.sn_first[s + 1] - S.sn_first[s]);
   }
-  // runs with a leader: run_a[s] = first block, run_e[s] = last block (-1: none)
+  // runs with a leader: run_a[s] = first block, run_e[s] = last block (-1: none).
+  // A leader holds its CTA while it waits for chunk tasks claimed after it, so
+  // the leaders that may be active at once must stay well below the resident
+  // CTAs of the kernel: runs are taken from the top of the tree down while no
+  // level is spanned by more than kMaxLeaders of them.
   std::vector<int> run_a(nsn, -1), run_e(nsn, -1);
   if (lead_level < INT_MAX && CH == kChunkRows) {
     const std::vector<int> rf = block_run_first(S);
+    std::vector<std::pair<int, int>> cand;  // (first, last block)
     for (int s0 = 0; s0 < nsn;) {
       int e = s0;
       while (e + 1 < nsn && rf[e + 1] == s0) ++e;
-      if (e > s0 && S.sn_level[s0] >= std::max(lead_level, min_level))
-        for (int q = s0; q <= e; ++q) { run_a[q] = s0; run_e[q] = e; }
+      if (e > s0 && S.sn_level[s0] >= std::max(lead_level, min_level)) cand.push_back({s0, e});
       s0 = e + 1;
+    }
+    std::stable_sort(cand.begin(), cand.end(), [&](const std::pair<int, int>& x, const std::pair<int, int>& y) {
+      return S.sn_level[x.second] > S.sn_level[y.second];
+    });
+    std::vector<int> span(S.nlevels + 1, 0);  // runs spanning each level
+    for (const auto& rn : cand) {
+      const int lo = S.sn_level[rn.first], hi = S.sn_level[rn.second];
+      bool room = true;
+      for (int l = lo; l <= hi && room; ++l) room = span[l] < kMaxLeaders;
+      if (!room) continue;
+      for (int l = lo; l <= hi; ++l) ++span[l];
+      for (int q = rn.first; q <= rn.second; ++q) { run_a[q] = rn.first; run_e[q] = rn.second; }
     }
   }
   std::vector<SolveTask> abs_t;
