@@ -698,18 +698,28 @@ def profile_run(args):
             g.factor(1, c.t0 / c.sp_division)
             split, cand = g.tune_solve(1, 1)
             f, b = g.solve_timeline(1)
-            out = {"config": args.config, "stats": st, "split": split, "candidates_ms": cand}
+            out = {"config": args.config, "stats": st, "plan": g.solve_plan(), "split_candidates_ms": cand}
+            names = {0: "diagonal", 1: "chunk", 2: "subtree", 3: "leader"}
             for name, T in (("forward", f), ("backward", b)):
                 t0 = T[:, 0].min()
-                lev = T[:, 7]
-                ends = np.array([T[lev == l, 2].max() - t0 for l in range(lev.max() + 1)]) / 1e3
                 span = (T[:, 2].max() - t0) / 1e3
-                done = np.maximum.accumulate(ends if name == "forward" else ends[::-1])
-                q = {p: float(done[int(p / 100 * (len(done) - 1))]) for p in (10, 25, 50, 75, 100)}
-                out[name] = {"tasks": int(len(T)), "span_us": float(span), "levels": int(len(ends)),
-                             "done_us_at_level_pct": q,
-                             "work_us_mean": float(np.mean(T[:, 2] - T[:, 1]) / 1e3),
-                             "to_ready_us_mean": float(np.mean(T[:, 1] - T[:, 0]) / 1e3)}
+                kinds = {}
+                for k in np.unique(T[:, 5]):
+                    R = T[T[:, 5] == k]
+                    kinds[names.get(int(k), str(k))] = {
+                        "tasks": int(len(R)), "first_start_us": float((R[:, 0].min() - t0) / 1e3),
+                        "last_end_us": float((R[:, 2].max() - t0) / 1e3),
+                        "work_us_mean": float(np.mean(R[:, 2] - R[:, 1]) / 1e3),
+                        "to_ready_us_mean": float(np.mean(R[:, 1] - R[:, 0]) / 1e3)}
+                # time by which each level's tasks (not the subtrees) have all ended
+                tk = T[T[:, 5] != 2]
+                lev = tk[:, 7]
+                levels = np.unique(lev)
+                ends = np.array([tk[lev == l, 2].max() - t0 for l in levels]) / 1e3
+                done = np.maximum.accumulate(ends if name == "forward" else ends[::-1]) if len(ends) else ends
+                q = {p_: float(done[int(p_ / 100 * (len(done) - 1))]) for p_ in (10, 25, 50, 75, 100)} if len(done) else {}
+                out[name] = {"tasks": int(len(T)), "span_us": float(span), "task_levels": int(len(levels)),
+                             "levels_done_us_at_pct": q, "by_kind": kinds}
             print(json.dumps(out))
             return 0
         o = g.run(c.sp_division, c.sp_double, c.sp_dblesize, c.time_maximum, max_steps=args.profile_steps)
