@@ -98,6 +98,7 @@ struct TreePlan {
   int n_ftask = 0, n_btask = 0;
   DBuf<int> ftgt_ptr, ftgt, fexpect, btgt_ptr, btgt;
   QueuePlan q;
+  DBuf<double> bacc;           // backward: per column, the sum of its supernode's chunk partials
   bool tuned = false;
   std::vector<int> tune_level;  // per candidate (level, split) when tuned; splits and times in q
 };

@@ -424,7 +424,10 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
   if (T.kind == 1) {
     const int chunk = T.r0 / kChunkRows;
     double* pp = V.part + (V.part_off[s] + (int64_t)chunk * c) * nrhs;
-    if (nrhs == 1) {
+    if (nrhs == 1 && V.bacc) {  // one accumulator per column: the diagonal task reads c values
+      for (int j = tid; j < c; j += blockDim.x)
+        atomicAdd(V.bacc + f + j, (seg[0][j] + seg[1][j]) + (seg[2][j] + seg[3][j]));
+    } else if (nrhs == 1) {
       for (int j = tid; j < c; j += blockDim.x) pp[j] = (seg[0][j] + seg[1][j]) + (seg[2][j] + seg[3][j]);
     } else {
       for (int j = warp; j < c; j += nw) {
@@ -455,7 +458,13 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
       // the other chunks' partials: thread (j, h) sums chunks q = 1 + h, 3 + h, ...
       // with eight loads in flight; fixed order, so still deterministic
       double* psum = zx;  // the chunk rows are consumed: reuse as [2][64]
-      if (nch > 1) {
+      if (nch > 1 && V.bacc) {
+        for (int j = tid; j < c; j += blockDim.x) {
+          psum[j] = __ldcg(V.bacc + f + j);
+          psum[kSnCols + j] = 0.0;
+        }
+        __syncthreads();
+      } else if (nch > 1) {
         const int j = tid & (kSnCols - 1), h = tid / kSnCols;
         double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         if (j < c && h < 2) {
@@ -664,7 +673,13 @@ __device__ void bwd_leader(const SweepView& V, int t, const double* Lb, int* err
     const int nch = V.nchunk[q];
     const double* pp = V.part + V.part_off[q];
     double* psum = zx;  // the chunk rows are consumed: reuse as [2][64]
-    if (nch > 1) {
+    if (nch > 1 && V.bacc) {
+      for (int j = tid; j < c; j += blockDim.x) {
+        psum[j] = __ldcg(V.bacc + f + j);
+        psum[kSnCols + j] = 0.0;
+      }
+      __syncthreads();
+    } else if (nch > 1) {
       const int j = tid & (kSnCols - 1), h = tid / kSnCols;
       double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       if (j < c && h < 2) {
@@ -1955,6 +1970,7 @@ void upload_tree_plan(temf_ctx& c, int level, int split, bool leaders) {
   build_sched(S, kChunkRows, a, level, leaders ? std::max(level, split) : INT_MAX);
   T.level = level;
   T.leaders = leaders;
+  if (T.bacc.n < (size_t)S.n) T.bacc.alloc(S.n);
   T.ntree = (int)trees.size();
   if (trees.empty()) T.trees.alloc(1);
   else T.trees.upload(trees.data(), trees.size(), st);
@@ -2142,6 +2158,7 @@ static void tree_views(temf_ctx& c, double* const* Lbase, double* x, SweepView& 
                  T.btgt.p, nullptr, P.nchunk.p, P.part_off.p, c.d_part.p, P.sync.p, P.nsn, nb,
                  q + nf, words + 1, words + 3, Q.bdiag.p, Q.bdep_ptr.p, Q.bdep.p, Q.bneed.p, q + nf + nb,
                  Q.b_lo, nb, 0, c.spin_limit};
+  vb.bacc = T.bacc.p;  // allocated with the plan
 }
 
 static void reset_tree_queues(temf_ctx& c, cudaStream_t st) {
@@ -2251,6 +2268,7 @@ void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaSt
     TEMF_CHECK_LAUNCH();
   }
   if (sgn) scale_rows(c, sgn, x, 1, 1, st);  // indefinite factor: L S L^T
+  TEMF_CUDA(cudaMemsetAsync(T.bacc.p, 0, (size_t)c.n_edges * sizeof(double), st));
   if (T.n_btask) {
     const int gridb = std::min(persistent_grid(k_bwd_queued, 0), T.n_btask);
     k_bwd_queued<<<gridb, kSolveThreads, 0, st>>>(vb, c.d_status.p + 1);

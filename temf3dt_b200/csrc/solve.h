@@ -37,6 +37,7 @@ struct SweepView {
   int q_lo, q_hi;          // tasks [q_lo, q_hi) go through the queue, the rest are claimed in order
   int tag;                 // model id << 24 when several models share one queue (0 otherwise)
   int spin = 0;            // iterations a device wait may spin before it gives up (0: the default)
+  double* bacc = nullptr;  // backward, one column: chunk partial sums accumulated per column (FP64 atomics)
 };
 
 void build_solve_plan(temf_ctx& c);
