@@ -698,6 +698,8 @@ def profile_run(args):
             g.factor(1, c.t0 / c.sp_division)
             split, cand = g.tune_solve(1, 1)
             f, b = g.solve_timeline(1)
+            if args.timeline_out:
+                np.savez_compressed(args.timeline_out, forward=f, backward=b)
             out = {"config": args.config, "stats": st, "plan": g.solve_plan(), "split_candidates_ms": cand}
             names = {0: "diagonal", 1: "chunk", 2: "subtree", 3: "leader"}
             for name, T in (("forward", f), ("backward", b)):
@@ -751,6 +753,7 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="profiling: run only the first N time steps of the config's model and print phase timings")
     ap.add_argument("--timeline", action="store_true", help="profiling: one solve with per-task GPU timestamps")
+    ap.add_argument("--timeline-out", default="", help="profiling: also save the raw timeline rows (.npz)")
     ap.add_argument("--rhs", type=int, default=0, help="profiling, config 2: the first RHS loops only (0 = all)")
     ap.add_argument("--h-core", type=float, default=0.0, help="profiling: core cell size override (m)")
     ap.add_argument("--replicate", type=int, default=1,
