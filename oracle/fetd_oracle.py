@@ -871,7 +871,7 @@ class _Output:
 def adap_euler(model: OracleModel, slots: SuperLUSlots, out: Optional[_Output],
                pulse_sign: float = 1.0, res_e: Optional[np.ndarray] = None,
                max_steps: Optional[int] = None, time_maximum: Optional[float] = None,
-               legacy_linux: bool = False):
+               legacy_linux: bool = False, forced: Optional[List[bool]] = None):
     """Adaptive BDF2 time loop, src/FETD_FWD.f90:1229-1464.
 
     ``pulse_sign`` = -1 reproduces the ``r_h = -r_h`` of the DC pass of pulse
@@ -880,6 +880,8 @@ def adap_euler(model: OracleModel, slots: SuperLUSlots, out: Optional[_Output],
     restarted from ``e3 = all_e(idx - sp_dblesize)`` instead of
     ``all_e(idx)`` (:1405) and advanced the time by one more old step than
     ``tmp_time_cur = time_cur - step_cur + tmp_step_cur`` (:1350).
+    ``forced``: accept/reject decisions replayed for the first trials in place
+    of the 1e-4 test (the trial errors are still computed and returned).
     """
     ctl = model.ctl
     n = model.n
@@ -942,7 +944,10 @@ def adap_euler(model: OracleModel, slots: SuperLUSlots, out: Optional[_Output],
             e_veri_2 = slots.solve(other, rh)
             error = two_error(e_veri_2, e_veri_1)
             errors.append(error)
-            if error > 1.0e-4 and not_changed < 2:         # :1382
+            reject = error > 1.0e-4 and not_changed < 2      # :1382
+            if forced is not None and len(errors) - 1 < len(forced):
+                reject = not forced[len(errors) - 1]
+            if reject:
                 accepted.append(False)
                 slots.release(other)
                 e1 = e_record_1
@@ -975,7 +980,7 @@ def adap_euler(model: OracleModel, slots: SuperLUSlots, out: Optional[_Output],
 
 
 def run_fetd(model: OracleModel, max_steps: Optional[int] = None, time_maximum: Optional[float] = None,
-             legacy_linux: bool = False, slots=None) -> FetdResult:
+             legacy_linux: bool = False, slots=None, forced: Optional[List[bool]] = None) -> FetdResult:
     """``time_solver`` (src/FETD_FWD.f90:1174-1227) with MKL replaced by SuperLU
     (or by other factor slots with the SuperLUSlots interface)."""
     if slots is None:
@@ -989,10 +994,10 @@ def run_fetd(model: OracleModel, max_steps: Optional[int] = None, time_maximum: 
         res_e, _, _ = adap_euler(model, slots, None, pulse_sign=-1.0, max_steps=None,
                                  time_maximum=time_maximum)
         e_last, errs, acc = adap_euler(model, slots, out, res_e=res_e, max_steps=max_steps,
-                                       time_maximum=time_maximum, legacy_linux=legacy_linux)
+                                       time_maximum=time_maximum, legacy_linux=legacy_linux, forced=forced)
     else:
         e_last, errs, acc = adap_euler(model, slots, out, max_steps=max_steps, time_maximum=time_maximum,
-                                       legacy_linux=legacy_linux)
+                                       legacy_linux=legacy_linux, forced=forced)
     return FetdResult(out.steps, out.times, out.dts, np.array(out.rows), out.chan_val, errs, acc, e_last,
                       out.mesh_fields)
 

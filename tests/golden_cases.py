@@ -223,3 +223,18 @@ def golden_field_report(steps, times, dbz, trial_errors, gold, sp_double, rtol=6
     big = np.abs(gd) >= 1e-3 * np.abs(gd).max()
     rel = float((np.abs(v[big] - gd[big]) / np.abs(gd[big])).max()) if big.any() else 0.0
     return first, decided, rel
+
+
+def golden_decisions(gold, sp_double):
+    """The accept/reject decisions of the run that wrote a .field, read off its
+    time column: trial k runs at step (k+1) * sp_double and was accepted iff the
+    time step after it is about twice the one before it (src/FETD_FWD.f90:1404-1418)."""
+    t = gold[:, 1]
+    out = []
+    s = sp_double
+    while s + 1 < len(t):
+        before = t[s - 1] - t[s - 2]
+        after = t[s + 1] - t[s]
+        out.append(bool(after > 1.5 * before))
+        s += sp_double
+    return out
