@@ -697,6 +697,21 @@ def profile_run(args):
         if args.timeline:
             g.factor(1, c.t0 / c.sp_division)
             split, cand = g.tune_solve(1, 1)
+            if args.plans:
+                # forced plans "level,split,options;...": sweep spans of each (median of 3)
+                tuned = g.solve_plan()
+                spans = {}
+                for spec in args.plans.split(";"):
+                    lv, sp, op = (int(v) for v in spec.split(","))  # op: run leaders 0/1
+                    g.set_solve_plan(lv, min(sp, int(st["levels"])), bool(op & 1))
+                    rs = []
+                    for _ in range(3):
+                        f, b = g.solve_timeline(1)
+                        rs.append(((f[:, 2].max() - f[:, 0].min()) / 1e3, (b[:, 2].max() - b[:, 0].min()) / 1e3))
+                    rs.sort(key=lambda v: v[0] + v[1])
+                    spans[spec] = {"fwd_us": rs[1][0], "bwd_us": rs[1][1]}
+                print(json.dumps({"config": args.config, "tuned": tuned, "cand": cand, "plans": spans}))
+                g.set_solve_plan(tuned["tree_level"], tuned["split"], tuned["run_leaders"])
             f, b = g.solve_timeline(1)
             if args.timeline_out:
                 np.savez_compressed(args.timeline_out, forward=f, backward=b)
@@ -754,6 +769,8 @@ def main():
                     help="profiling: run only the first N time steps of the config's model and print phase timings")
     ap.add_argument("--timeline", action="store_true", help="profiling: one solve with per-task GPU timestamps")
     ap.add_argument("--timeline-out", default="", help="profiling: also save the raw timeline rows (.npz)")
+    ap.add_argument("--plans", default="", help="profiling, with --timeline: sweep spans of forced plans "
+                    "'level,split,leaders;...' (leaders 0/1)")
     ap.add_argument("--rhs", type=int, default=0, help="profiling, config 2: the first RHS loops only (0 = all)")
     ap.add_argument("--h-core", type=float, default=0.0, help="profiling: core cell size override (m)")
     ap.add_argument("--replicate", type=int, default=1,

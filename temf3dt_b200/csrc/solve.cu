@@ -73,9 +73,96 @@ __device__ __forceinline__ void wait_geq(const int* flag, int target, int* err, 
   __threadfence();
 }
 
+// One warp solves the c x c diagonal block for one right-hand side; lane l
+// holds rows l (v0) and 32 + l (v1).  Columns are taken eight at a time:
+// their eight current values are broadcast, every lane solves the 8 x 8
+// block redundantly, the owners take their rows' results and every lane
+// updates its rows beyond the block.  Each row receives exactly the updates
+// of column-by-column substitution, one FMA each, in the same column order,
+// so the result is the same to the bit; the dependent chain per column is one
+// FMA and one multiply instead of a shuffle round trip.
+__device__ __forceinline__ void diag_solve_fwd_warp(const double (*D)[kSnCols + 1], const double* rinv, double& v0,
+                                                    double& v1, int c) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k0 = 0; k0 < kSnCols; k0 += 8) {
+    if (k0 < c) {  // warp-uniform
+      double y[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) y[i] = __shfl_sync(0xffffffffu, k0 < 32 ? v0 : v1, (k0 + i) & 31);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        if (k0 + i < c) {
+          double t = y[i];
+#pragma unroll
+          for (int j = 0; j < i; ++j) t -= D[k0 + i][k0 + j] * y[j];
+          y[i] = t * rinv[k0 + i];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        if (lane == ((k0 + i) & 31) && k0 + i < c) {
+          if (k0 < 32) v0 = y[i];
+          else v1 = y[i];
+        }
+      }
+      if (k0 < 32 && lane >= k0 + 8 && lane < c) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v0 -= D[lane][k0 + j] * y[j];
+      }
+      if (lane + 32 >= k0 + 8 && lane + 32 < c) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v1 -= D[lane + 32][k0 + j] * y[j];
+      }
+    }
+  }
+}
+// L^T x = z, columns from the last: the same blocking, eight at a time from
+// the top, every row updated in descending column order as in the
+// column-by-column substitution.
+__device__ __forceinline__ void diag_solve_bwd_warp(const double (*D)[kSnCols + 1], const double* rinv, double& v0,
+                                                    double& v1, int c) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k0 = kSnCols - 8; k0 >= 0; k0 -= 8) {
+    if (k0 < c) {  // warp-uniform
+      double x[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) x[i] = __shfl_sync(0xffffffffu, k0 < 32 ? v0 : v1, (k0 + i) & 31);
+#pragma unroll
+      for (int i = 7; i >= 0; --i) {
+        if (k0 + i < c) {
+          double t = x[i];
+#pragma unroll
+          for (int j = 7; j > i; --j)
+            if (k0 + j < c) t -= D[k0 + j][k0 + i] * x[j];
+          x[i] = t * rinv[k0 + i];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        if (lane == ((k0 + i) & 31) && k0 + i < c) {
+          if (k0 < 32) v0 = x[i];
+          else v1 = x[i];
+        }
+      }
+      if (lane < k0 && lane < c) {
+#pragma unroll
+        for (int j = 7; j >= 0; --j)
+          if (k0 + j < c) v0 -= D[k0 + j][lane] * x[j];
+      }
+      if (k0 >= 32 && lane + 32 < k0 && lane + 32 < c) {
+#pragma unroll
+        for (int j = 7; j >= 0; --j)
+          if (k0 + j < c) v1 -= D[k0 + j][lane + 32] * x[j];
+      }
+    }
+  }
+}
+
 // Dense lower-triangular solve of the c x c diagonal block held in D (shared)
 // for nrhs columns of ys (row-major c x nrhs), forward (L y = b) or backward
-// (L^T x = z).  nrhs == 1 runs in one warp with shuffles.
+// (L^T x = z).  nrhs == 1 runs in one warp (the blocked substitution above).
 __device__ void diag_solve(const double (*D)[kSnCols + 1], const double* rinv, double* ys, int c, int nrhs,
                            bool forward) {
   const int tid = threadIdx.x;
@@ -84,23 +171,8 @@ __device__ void diag_solve(const double (*D)[kSnCols + 1], const double* rinv, d
       const int lane = tid;
       double v0 = lane < c ? ys[lane] : 0.0;
       double v1 = lane + 32 < c ? ys[lane + 32] : 0.0;
-      if (forward) {
-        for (int j = 0; j < c; ++j) {
-          const double v = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-          const double yj = v * rinv[j];
-          if (lane == (j & 31)) { if (j < 32) v0 = yj; else v1 = yj; }
-          if (lane > j && lane < c) v0 -= D[lane][j] * yj;
-          if (lane + 32 > j && lane + 32 < c) v1 -= D[lane + 32][j] * yj;
-        }
-      } else {
-        for (int j = c - 1; j >= 0; --j) {
-          const double v = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
-          const double xj = v * rinv[j];
-          if (lane == (j & 31)) { if (j < 32) v0 = xj; else v1 = xj; }
-          if (lane < j) v0 -= D[j][lane] * xj;
-          if (lane + 32 < j) v1 -= D[j][lane + 32] * xj;
-        }
-      }
+      if (forward) diag_solve_fwd_warp(D, rinv, v0, v1, c);
+      else diag_solve_bwd_warp(D, rinv, v0, v1, c);
       if (lane < c) ys[lane] = v0;
       if (lane + 32 < c) ys[lane + 32] = v1;
     }
@@ -215,6 +287,49 @@ __device__ __forceinline__ void q_push(const SweepView& V, int task) {
   const int pos = atomicAdd(V.qtail, 1);
   atomicExch(V.queue + pos, (V.tag | task) + 1);
 }
+// Forward: one more input for each supernode in tgt[k0, k1); the queued
+// diagonal tasks whose inputs are then complete are pushed.  Four entries
+// per thread at a time, so the round trips of their atomics overlap.
+__device__ __forceinline__ void count_inputs(const SweepView& V, int k0, int k1) {
+  int* ready = V.sync;
+  const int nt = blockDim.x;
+  for (int k = k0 + (int)threadIdx.x; k < k1; k += 4 * nt) {
+    int o[4], d[4], ex[4], old[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) o[u] = k + u * nt < k1 ? V.tgt[k + u * nt] : -1;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      d[u] = o[u] >= 0 ? V.diag_task[o[u]] : -1;
+      ex[u] = o[u] >= 0 ? V.expect[o[u]] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) old[u] = o[u] >= 0 ? atomicAdd(ready + o[u], 1) : -1;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (o[u] >= 0 && in_queue(V, d[u]) && old[u] == ex[u] - 1) q_push(V, d[u]);
+  }
+}
+// Backward: one completion for each task in dep[k0, k1) (an owner of its
+// rows is solved); the queued tasks whose count is then complete are pushed.
+__device__ __forceinline__ void count_owner_done(const SweepView& V, int k0, int k1) {
+  const int nt = blockDim.x;
+  for (int k = k0 + (int)threadIdx.x; k < k1; k += 4 * nt) {
+    int d[4], nd[4], old[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      d[u] = k + u * nt < k1 ? V.dep[k + u * nt] : -1;
+      if (d[u] >= 0 && !in_queue(V, d[u])) d[u] = -1;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) nd[u] = d[u] >= 0 ? V.need[d[u]] : 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) old[u] = d[u] >= 0 ? atomicAdd(V.cnt + d[u], 1) : -1;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (d[u] >= 0 && old[u] == nd[u] - 1) q_push(V, d[u]);
+  }
+}
+
 // thread 0 only: next ready task, or -1 when all ntask tasks are handed out
 // (or a wait timed out: error word set)
 __device__ __forceinline__ int q_pop(int* qhead, const int* queue, int limit, int* err, int spin) {
@@ -293,6 +408,7 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
   const bool row_on = i < T.r1;
   FwdRegs R;
   if (nrhs == 1) pre_fwd(R, Pc, c, ld, i, row_on);
+  const int row_i = row_on ? V.sn_rows[rp + i] : 0;  // the row this thread pushes to (read before the wait)
   const bool queued = in_queue(V, t);
   if (T.kind == 0) {
     load_diag_start(D, P, c, ld);
@@ -313,9 +429,9 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
   }
   if (T.r1 > T.r0) {
     if (nrhs == 1) {
-      if (row_on) atomicAdd(x + V.sn_rows[rp + i], -fin_fwd(R, ys, c));
+      if (row_on) atomicAdd(x + row_i, -fin_fwd(R, ys, c));
     } else if (row_on) {
-      double* dst = x + (int64_t)V.sn_rows[rp + i] * nrhs;
+      double* dst = x + (int64_t)row_i * nrhs;
       for (int col = 0; col < nrhs; ++col) {
         double a = 0.0;
         for (int j = 0; j < c; ++j) a += __ldg(Pc + (int64_t)j * ld + i) * ys[j * nrhs + col];
@@ -334,12 +450,7 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
   }
   if (T.r1 > T.r0) {
     if (V.queue) {
-      for (int q = V.tgt_ptr[t] + tid; q < V.tgt_ptr[t + 1]; q += blockDim.x) {
-        const int o = V.tgt[q];
-        const int d = V.diag_task[o];
-        if (!in_queue(V, d)) atomicAdd(ready + o, 1);  // claimed in order: only its count matters
-        else if (atomicAdd(ready + o, 1) == V.expect[o] - 1) q_push(V, d);
-      }
+      count_inputs(V, V.tgt_ptr[t], V.tgt_ptr[t + 1]);
     } else if (tid == 0) {
       for (int q = V.tgt_ptr[t]; q < V.tgt_ptr[t + 1]; ++q) atomicAdd(ready + V.tgt[q], 1);
     }
@@ -399,6 +510,8 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
   const int nr = T.r1 - T.r0;
   BwdRegs R;
   if (nrhs == 1 && nr > 0) pre_bwd(R, P, c, ld, T.r0, nr);
+  // one chunk row per thread for a single column: its index read before the wait
+  const int row_t = (nrhs == 1 && tid < nr) ? V.sn_rows[rp + T.r0 + tid] : 0;
   if (T.kind == 0) load_diag_start(D, P, c, ld);
   const bool queued = in_queue(V, t);
   // the chunk's rows need their owners' x; the diagonal task also its other chunks
@@ -411,9 +524,13 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
   if (stamp && tid == 0) *stamp = gtime();
   double* zx = zs + (T.kind == 0 ? kSnCols * nrhs : 0);  // chunk rows live after the diagonal block
   if (nr > 0) {
-    for (int idx = tid; idx < nr * nrhs; idx += blockDim.x) {
-      const int ii = idx / nrhs, col = idx % nrhs;
-      zx[idx] = __ldcg(x + (int64_t)V.sn_rows[rp + T.r0 + ii] * nrhs + col);
+    if (nrhs == 1) {  // nr <= blockDim.x
+      if (tid < nr) zx[tid] = __ldcg(x + row_t);
+    } else {
+      for (int idx = tid; idx < nr * nrhs; idx += blockDim.x) {
+        const int ii = idx / nrhs, col = idx % nrhs;
+        zx[idx] = __ldcg(x + (int64_t)V.sn_rows[rp + T.r0 + ii] * nrhs + col);
+      }
     }
     __syncthreads();
     if (nrhs == 1) {
@@ -505,11 +622,7 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
     __threadfence();
     __syncthreads();
     if (tid == 0) atomicExch(xdone + s, 1);
-    if (V.queue)  // x_s is out: count it for every queued task whose rows s owns
-      for (int q = V.dep_ptr[s] + tid; q < V.dep_ptr[s + 1]; q += blockDim.x) {
-        const int d = V.dep[q];
-        if (in_queue(V, d) && atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
-      }
+    if (V.queue) count_owner_done(V, V.dep_ptr[s], V.dep_ptr[s + 1]);  // x_s is out: every queued task whose rows s owns
   }
 }
 
@@ -610,12 +723,7 @@ __device__ void fwd_leader(const SweepView& V, int t, const double* Lb, int* err
     __syncthreads();
     if (tid == 0) atomicExch(ydone + q, 1);
     if (V.queue) {
-      for (int k = V.tgt_ptr[dq] + tid; k < V.tgt_ptr[dq + 1]; k += blockDim.x) {
-        const int o = V.tgt[k];
-        const int d = V.diag_task[o];
-        if (!in_queue(V, d)) atomicAdd(ready + o, 1);
-        else if (atomicAdd(ready + o, 1) == V.expect[o] - 1) q_push(V, d);
-      }
+      count_inputs(V, V.tgt_ptr[dq], V.tgt_ptr[dq + 1]);
     } else if (tid == 0) {
       for (int k = V.tgt_ptr[dq]; k < V.tgt_ptr[dq + 1]; ++k) atomicAdd(ready + V.tgt[k], 1);
     }
@@ -710,11 +818,7 @@ __device__ void bwd_leader(const SweepView& V, int t, const double* Lb, int* err
     __threadfence();
     __syncthreads();
     if (tid == 0) atomicExch(xdone + q, 1);
-    if (V.queue)  // x_q is out: count it for every queued task whose rows q owns
-      for (int k = V.dep_ptr[q] + tid; k < V.dep_ptr[q + 1]; k += blockDim.x) {
-        const int d = V.dep[k];
-        if (in_queue(V, d) && atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
-      }
+    if (V.queue) count_owner_done(V, V.dep_ptr[q], V.dep_ptr[q + 1]);  // x_q is out: every queued task whose rows q owns
     if (q > a) {  // the next block (one lower): first chunk into registers, diagonal block into shared memory
       const int fn = V.sn_first[q - 1], cn = f - fn;
       const int64_t rn = V.rows_ptr[q] - V.rows_ptr[q - 1], ldn = cn + rn;
@@ -727,7 +831,7 @@ __device__ void bwd_leader(const SweepView& V, int t, const double* Lb, int* err
 }
 
 // The same sweeps scheduled through the ready queue (single right-hand side).
-__global__ void __launch_bounds__(kSolveThreads) k_fwd_queued(const SweepView V, int* err) {
+__global__ void __launch_bounds__(kSolveThreads, 3) k_fwd_queued(const SweepView V, int* err) {
   __shared__ double D[kSnCols][kSnCols + 1];
   __shared__ double rinv[kSnCols];
   __shared__ double ys[kSnCols];
@@ -907,8 +1011,10 @@ __device__ __forceinline__ void fwd_sn_warp(const TreeView& V, const double* Lb,
   __syncwarp();
 }
 
-// backward L^T x = y for supernode s by one warp
-__device__ __forceinline__ void bwd_sn_warp(const TreeView& V, const double* Lb, int s) {
+// backward L^T x = y for supernode s by one warp; xs: this warp's kTreeXs
+// doubles of shared memory (x at the first rows, kept from the first pass)
+constexpr int kTreeXs = 256;
+__device__ __forceinline__ void bwd_sn_warp(const TreeView& V, const double* Lb, int s, double* xs) {
   const int lane = threadIdx.x & 31;
   const int f = V.sn_first[s];
   const int c = V.sn_first[s + 1] - f;
@@ -920,15 +1026,26 @@ __device__ __forceinline__ void bwd_sn_warp(const TreeView& V, const double* Lb,
   const int* rows = V.sn_rows + rp;
   double v0 = lane < c ? __ldcg(x + f + lane) : 0.0;
   double v1 = 32 + lane < c ? __ldcg(x + f + 32 + lane) : 0.0;
-  // z_j = y_j - sum_i L21[i][j] x[rows_i], 32 columns at a time
+  // z_j = y_j - sum_i L21[i][j] x[rows_i], 32 columns at a time.  The first
+  // pass gathers x at the rows one 32-row block ahead (the gather overlaps
+  // the block in flight) and keeps the first kTreeXs in shared memory for
+  // the second pass.
   double acc[32];
   for (int h = 0; h * 32 < c; ++h) {
 #pragma unroll
     for (int k = 0; k < 32; ++k) acc[k] = 0.0;
+    double xn = (h == 0 && lane < r) ? __ldcg(x + rows[lane]) : 0.0;
     for (int q0 = 0; q0 < r; q0 += 32) {
       const int i = q0 + lane;
       const bool on = i < r;
-      const double xi = on ? __ldcg(x + rows[i]) : 0.0;
+      double xi;
+      if (h == 0) {
+        xi = xn;
+        if (on && i < kTreeXs) xs[i] = xi;
+        xn = i + 32 < r ? __ldcg(x + rows[i + 32]) : 0.0;
+      } else {
+        xi = !on ? 0.0 : (i < kTreeXs ? xs[i] : __ldcg(x + rows[i]));
+      }
       const double* col = P + c + i;
 #pragma unroll
       for (int k = 0; k < 32; ++k) {
@@ -1000,7 +1117,8 @@ __global__ void __launch_bounds__(kTreeThreads, 3) k_fwd_subtrees(const TreeView
 }
 
 __global__ void __launch_bounds__(kTreeThreads, 3) k_bwd_subtrees(const TreeView V) {
-  const int lane = threadIdx.x & 31;
+  __shared__ double xsm[kTreeThreads / 32][kTreeXs];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double* Lb = *V.Lbase;
   for (;;) {
     int t = 0;
@@ -1010,7 +1128,7 @@ __global__ void __launch_bounds__(kTreeThreads, 3) k_bwd_subtrees(const TreeView
     unsigned long long* rec = g_timeline_tb ? g_timeline_tb + 4 * (size_t)t : nullptr;
     if (rec && lane == 0) rec[0] = gtime();
     const int2 tr = V.trees[t];
-    for (int s = tr.y; s >= tr.x; --s) bwd_sn_warp(V, Lb, s);
+    for (int s = tr.y; s >= tr.x; --s) bwd_sn_warp(V, Lb, s, xsm[warp]);
     if (rec && lane == 0) { rec[1] = rec[0]; rec[2] = gtime(); rec[3] = smid(); }
   }
 }
@@ -1299,12 +1417,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_fwd_multi(const SweepView V, 
       }
       __threadfence();
       __syncthreads();
-      for (int q = V.tgt_ptr[t] + tid; q < V.tgt_ptr[t + 1]; q += blockDim.x) {
-        const int o = V.tgt[q];
-        const int d = V.diag_task[o];
-        if (!in_queue(V, d)) atomicAdd(ready + o, 1);
-        else if (atomicAdd(ready + o, 1) == V.expect[o] - 1) q_push(V, d);
-      }
+      count_inputs(V, V.tgt_ptr[t], V.tgt_ptr[t + 1]);
     }
   }
 }
@@ -1388,11 +1501,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_multi(const SweepView V, 
       __threadfence();
       __syncthreads();
       if (tid == 0) atomicExch(xdone + s, 1);
-      // x_s is out: count it for every queued task whose rows s owns
-      for (int q = V.dep_ptr[s] + tid; q < V.dep_ptr[s + 1]; q += blockDim.x) {
-        const int d = V.dep[q];
-        if (in_queue(V, d) && atomicAdd(V.cnt + d, 1) == V.need[d] - 1) q_push(V, d);
-      }
+      count_owner_done(V, V.dep_ptr[s], V.dep_ptr[s + 1]);  // x_s is out: every queued task whose rows s owns
     }
   }
 }
@@ -1618,7 +1727,16 @@ void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lea
   abs_t.clear();
   abs_g.clear();
   // backward: top-down levels; per supernode its other chunks, then the
-  // diagonal task with the first chunk
+  // diagonal task with the first chunk.  A backward task waits for one owner
+  // only: the owner A of its lowest row.  Its rows R' lie in R(s) above A's
+  // first column; following the supernodal tree from s up to A, each step
+  // keeps R' inside the next supernode's rows (R(child) minus the parent's
+  // columns lies in R(parent)), so R' lies in cols(A) and R(A), and A is
+  // solved only after every owner of R(A) (check_schedule replays the real
+  // row dependencies).  So each task has one dependency, not one per owner.
+  auto lowest = [&]() {
+    if (tmp.size() > 1) tmp.resize(1);
+  };
   for (int l = S.nlevels - 1; l >= std::max(0, min_level); --l)
     for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
       const int s = S.level_sn[q];
@@ -1627,12 +1745,14 @@ void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lea
         const int r1 = std::min(r, r0 + CH);
         o.bt.push_back({s, 1, r0, r1});
         owners(s, r0, r1);
+        lowest();
         o.btg.insert(o.btg.end(), tmp.begin(), tmp.end());
         o.btp.push_back((int)o.btg.size());
       }
       const int r1 = std::min(r, CH);
       if (run_a[s] >= 0) {
         owners(s, 0, r1, run_e[s]);
+        lowest();
         if (s == run_e[s]) {
           o.bt.push_back({s, 3 | ((run_e[s] - run_a[s] + 1) << 4), 0, r1});
           o.btg.insert(o.btg.end(), tmp.begin(), tmp.end());
@@ -1645,6 +1765,7 @@ void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lea
       }
       o.bt.push_back({s, 0, 0, r1});
       owners(s, 0, r1);
+      lowest();
       o.btg.insert(o.btg.end(), tmp.begin(), tmp.end());
       o.btp.push_back((int)o.btg.size());
     }
@@ -1826,6 +1947,17 @@ std::string check_schedule(const Symbolic& S, int CH, int split, int min_level =
     std::vector<int> xdone(nsn, 0), cdone(nsn, 0), cnt(nb, 0), seen(nb, 0);
     std::vector<int> queue(q.binit);
     std::vector<std::pair<int, int>> leaders;  // (next block, first block), top-down
+    // the real inputs: every row [r0, r1) of s owned above `skip_to` is solved
+    auto rows_final = [&](int s, int r0, int r1, int skip_to) {
+      const int* rows = S.sn_rows.data() + S.sn_rows_ptr[s];
+      for (int i = r0; i < r1; ++i) {
+        const int ow = S.col2sn[rows[i]];
+        if (ow > skip_to && !xdone[ow]) return false;
+      }
+      return true;
+    };
+    std::string real_err;
+    std::vector<int> run_last(nsn, -1);  // per first block of a leader's run: its last block
     auto count = [&](int d) {
       if (d < nb && ++cnt[d] == q.bneed[d] && d >= b_lo) queue.push_back(d);
     };
@@ -1843,6 +1975,9 @@ std::string check_schedule(const Symbolic& S, int CH, int split, int min_level =
         moved = false;
         for (auto& L : leaders)
           while (L.first >= L.second && inputs_done(q.bdiag[L.first], L.first)) {
+            const SolveTask& E = a.bt[q.bdiag[L.first]];
+            if (real_err.empty() && !rows_final(E.s, E.r0, E.r1, run_last[L.second]))
+              real_err = "backward: a run block solved before an owner of its rows";
             solved(L.first);
             --L.first;
             moved = true;
@@ -1855,6 +1990,7 @@ std::string check_schedule(const Symbolic& S, int CH, int split, int min_level =
       if ((T.kind & 15) == 3) {
         if (queued) return "backward queue: a run leader in the queue";
         leaders.push_back({T.s, T.s - (T.kind >> 4) + 1});
+        run_last[T.s - (T.kind >> 4) + 1] = T.s;
         advance();
         return std::string();
       }
@@ -1866,6 +2002,7 @@ std::string check_schedule(const Symbolic& S, int CH, int split, int min_level =
           if (!xdone[a.btg[k]]) return "backward: task claimed before an owner of its rows";
         if (T.kind == 0 && cdone[T.s] != std::max(a.nch[T.s], 1) - 1) return "backward: diagonal task before its chunks";
       }
+      if (!rows_final(T.s, T.r0, T.r1, -1)) return "backward: task run before an owner of its rows";
       if (T.kind == 1) {
         cdone[T.s]++;
         count(q.bdiag[T.s]);
@@ -1889,6 +2026,7 @@ std::string check_schedule(const Symbolic& S, int CH, int split, int min_level =
       if (!w.empty()) return w;
     }
     if ((int)queue.size() != nb - b_lo) return "backward queue: not every queued task handed out";
+    if (!real_err.empty()) return real_err;
     for (int s = 0; s < nsn; ++s)
       if (S.sn_level[s] >= min_level && !xdone[s]) return "backward: a supernode never solved";
   }
