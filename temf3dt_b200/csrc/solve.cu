@@ -240,39 +240,35 @@ __device__ __forceinline__ double fin_fwd(const FwdRegs& R, const double* ys, in
   return (a0 + a1) + (a2 + a3);
 }
 
-// backward work items of a 128-row chunk: (column j, 32-row segment q),
-// two per thread, 32 contiguous panel values each.
-struct BwdRegs {
-  double v[2][32];
-};
-__device__ __forceinline__ void pre_bwd(BwdRegs& R, const double* P, int c, int64_t ld, int r0, int nr) {
-  const int nseg = (nr + 31) / 32;
+// Sum over the 32 lanes of each of the 32 per-lane values a[0..31]: lane l
+// ends with the sum of a[l] (31 shuffles: each step halves the live values).
+__device__ __forceinline__ double lane_transpose_sum(double a[32]) {
+  const int lane = threadIdx.x & 31;
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int w = threadIdx.x + h * kSolveThreads;
-    const int j = w % kSnCols, q = w / kSnCols;
-    const bool on = j < c && q < nseg;
-    const double* colp = P + (int64_t)j * ld + c + r0 + q * 32;
-    const int m = on ? min(32, nr - q * 32) : 0;
+  for (int o = 16; o >= 1; o >>= 1) {
+    const bool up = (lane & o) != 0;
 #pragma unroll
-    for (int k = 0; k < 32; ++k) R.v[h][k] = (k < m) ? __ldg(colp + k) : 0.0;
-  }
-}
-// partial sums of the chunk (one value per column), fixed reduction order
-__device__ __forceinline__ void fin_bwd(const BwdRegs& R, const double* zs, int c, int nr, double (*seg)[kSnCols]) {
-  const int nseg = (nr + 31) / 32;
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int w = threadIdx.x + h * kSolveThreads;
-    const int j = w % kSnCols, q = w / kSnCols;
-    double acc = 0.0;
-    if (j < c && q < nseg) {
-      const int m = min(32, nr - q * 32);
-#pragma unroll
-      for (int k = 0; k < 32; ++k) acc += R.v[h][k] * (k < m ? zs[q * 32 + k] : 0.0);
+    for (int k = 0; k < o; ++k) {
+      const double send = up ? a[k] : a[k + o];
+      const double keep = up ? a[k + o] : a[k];
+      a[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
     }
-    if (j < c) seg[q][j] = acc;
   }
+  return a[0];
+}
+
+// Backward chunk products, single right-hand side: the chunk is loaded as in
+// the forward sweep (thread = row, its c panel values in registers, loads
+// coalesced along each column); each thread scales its row by z_row and the
+// per-column sums over the warp's 32 rows come out of two transposing
+// shuffle reductions, one value per lane and column: seg[warp][j].  The
+// consumers add the four warps' sums in a fixed order.
+__device__ __forceinline__ void bwd_row_sums(FwdRegs& R, double zi, double (*seg)[kSnCols]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < kSnCols; ++j) R.v[j] *= zi;
+  seg[warp][lane] = lane_transpose_sum(R.v);
+  seg[warp][32 + lane] = lane_transpose_sum(R.v + 32);
 }
 
 // Ready queue: a task is appended once every task it depends on has finished
@@ -410,6 +406,18 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
   if (nrhs == 1) pre_fwd(R, Pc, c, ld, i, row_on);
   const int row_i = row_on ? V.sn_rows[rp + i] : 0;  // the row this thread pushes to (read before the wait)
   const bool queued = in_queue(V, t);
+  // this thread's target supernode with its diagonal task and input count,
+  // read before the wait (a chunk of at most blockDim rows feeds at most
+  // blockDim supernodes: one entry per thread)
+  int tg_o = -1, tg_d = -1, tg_ex = 0;
+  if (V.queue && T.r1 > T.r0) {
+    const int k = V.tgt_ptr[t] + tid;
+    if (k < V.tgt_ptr[t + 1]) {
+      tg_o = V.tgt[k];
+      tg_d = V.diag_task[tg_o];
+      tg_ex = V.expect[tg_o];
+    }
+  }
   if (T.kind == 0) {
     load_diag_start(D, P, c, ld);
     if (tid == 0 && !queued) wait_geq(ready + s, V.expect[s], err, 1, spin_limit(V));
@@ -450,7 +458,11 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
   }
   if (T.r1 > T.r0) {
     if (V.queue) {
-      count_inputs(V, V.tgt_ptr[t], V.tgt_ptr[t + 1]);
+      if (tg_o >= 0) {
+        const int old = atomicAdd(ready + tg_o, 1);
+        if (in_queue(V, tg_d) && old == tg_ex - 1) q_push(V, tg_d);
+      }
+      count_inputs(V, V.tgt_ptr[t] + (int)blockDim.x, V.tgt_ptr[t + 1]);  // longer lists (none expected)
     } else if (tid == 0) {
       for (int q = V.tgt_ptr[t]; q < V.tgt_ptr[t + 1]; ++q) atomicAdd(ready + V.tgt[q], 1);
     }
@@ -508,8 +520,8 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
   const int64_t ld = c + r;
   const double* P = Lb + V.Lptr[s];
   const int nr = T.r1 - T.r0;
-  BwdRegs R;
-  if (nrhs == 1 && nr > 0) pre_bwd(R, P, c, ld, T.r0, nr);
+  FwdRegs R;
+  if (nrhs == 1 && nr > 0) pre_fwd(R, P + c, c, ld, T.r0 + tid, tid < nr);
   // one chunk row per thread for a single column: its index read before the wait
   const int row_t = (nrhs == 1 && tid < nr) ? V.sn_rows[rp + T.r0 + tid] : 0;
   if (T.kind == 0) load_diag_start(D, P, c, ld);
@@ -524,8 +536,8 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
   if (stamp && tid == 0) *stamp = gtime();
   double* zx = zs + (T.kind == 0 ? kSnCols * nrhs : 0);  // chunk rows live after the diagonal block
   if (nr > 0) {
-    if (nrhs == 1) {  // nr <= blockDim.x
-      if (tid < nr) zx[tid] = __ldcg(x + row_t);
+    if (nrhs == 1) {  // nr <= blockDim.x: one row per thread
+      bwd_row_sums(R, tid < nr ? __ldcg(x + row_t) : 0.0, seg);
     } else {
       for (int idx = tid; idx < nr * nrhs; idx += blockDim.x) {
         const int ii = idx / nrhs, col = idx % nrhs;
@@ -533,10 +545,6 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
       }
     }
     __syncthreads();
-    if (nrhs == 1) {
-      fin_bwd(R, zx, c, nr, seg);
-      __syncthreads();
-    }
   }
   if (T.kind == 1) {
     const int chunk = T.r0 / kChunkRows;
@@ -746,13 +754,13 @@ __device__ void bwd_leader(const SweepView& V, int t, const double* Lb, int* err
   const SolveTask T0 = V.tasks[t];
   const int e = T0.s, a = e - leader_blocks(T0) + 1;
   const int f_run = V.sn_first[a], f_end = V.sn_first[e + 1];
-  BwdRegs R;
+  FwdRegs R;
   {
     const int c = V.sn_first[e + 1] - V.sn_first[e];
     const int64_t r = V.rows_ptr[e + 1] - V.rows_ptr[e], ld = c + r;
     const double* P = Lb + V.Lptr[e];
     const int r1 = (int)(r < kChunkRows ? r : (int64_t)kChunkRows);
-    if (r1 > 0) pre_bwd(R, P, c, ld, 0, r1);
+    if (r1 > 0) pre_fwd(R, P + c, c, ld, tid, tid < r1);
     load_diag_start(D, P, c, ld);
   }
   for (int q = e; q >= a; --q) {
@@ -769,12 +777,12 @@ __device__ void bwd_leader(const SweepView& V, int t, const double* Lb, int* err
     __syncthreads();
     double* zx = zs + kSnCols;
     if (r1 > 0) {
-      for (int ii = tid; ii < r1; ii += blockDim.x) {
-        const int row = V.sn_rows[rp + ii];
-        zx[ii] = row < f_end ? ring[(row - f_run) & (kRing - 1)] : __ldcg(x + row);
+      double zi = 0.0;
+      if (tid < r1) {
+        const int row = V.sn_rows[rp + tid];
+        zi = row < f_end ? ring[(row - f_run) & (kRing - 1)] : __ldcg(x + row);
       }
-      __syncthreads();
-      fin_bwd(R, zx, c, r1, seg);
+      bwd_row_sums(R, zi, seg);
       __syncthreads();
     }
     // z = y_q - (first chunk) - (other chunks, fixed order)
@@ -824,13 +832,17 @@ __device__ void bwd_leader(const SweepView& V, int t, const double* Lb, int* err
       const int64_t rn = V.rows_ptr[q] - V.rows_ptr[q - 1], ldn = cn + rn;
       const double* Pn = Lb + V.Lptr[q - 1];
       const int r1n = (int)(rn < kChunkRows ? rn : (int64_t)kChunkRows);
-      if (r1n > 0) pre_bwd(R, Pn, cn, ldn, 0, r1n);
+      if (r1n > 0) pre_fwd(R, Pn + cn, cn, ldn, tid, tid < r1n);
       load_diag_start(D, Pn, cn, ldn);
     }
   }
 }
 
 // The same sweeps scheduled through the ready queue (single right-hand side).
+// Instantiated with and without run leaders: the leader code needs many more
+// registers, so the plans without leaders get three resident CTAs per SM
+// (168 registers) for both sweeps; the backward with leaders two.
+template <bool kLeaders>
 __global__ void __launch_bounds__(kSolveThreads, 3) k_fwd_queued(const SweepView V, int* err) {
   __shared__ double D[kSnCols][kSnCols + 1];
   __shared__ double rinv[kSnCols];
@@ -844,7 +856,7 @@ __global__ void __launch_bounds__(kSolveThreads, 3) k_fwd_queued(const SweepView
     if (t < 0) break;
     unsigned long long* rec = g_timeline_f ? g_timeline_f + 4 * (size_t)t : nullptr;
     if (rec && threadIdx.x == 0) rec[0] = gtime();
-    if ((V.tasks[t].kind & 15) == 3) {
+    if (kLeaders && (V.tasks[t].kind & 15) == 3) {
       if (rec && threadIdx.x == 0) rec[1] = gtime();
       fwd_leader(V, t, Lb, err, D, rinv, ys, ring);
     } else {
@@ -854,7 +866,8 @@ __global__ void __launch_bounds__(kSolveThreads, 3) k_fwd_queued(const SweepView
   }
 }
 
-__global__ void __launch_bounds__(kSolveThreads) k_bwd_queued(const SweepView V, int* err) {
+template <bool kLeaders>
+__global__ void __launch_bounds__(kSolveThreads, kLeaders ? 2 : 3) k_bwd_queued(const SweepView V, int* err) {
   __shared__ double D[kSnCols][kSnCols + 1];
   __shared__ double rinv[kSnCols];
   __shared__ double seg[4][kSnCols];
@@ -868,7 +881,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_bwd_queued(const SweepView V,
     if (t < 0) break;
     unsigned long long* rec = g_timeline_b ? g_timeline_b + 4 * (size_t)t : nullptr;
     if (rec && threadIdx.x == 0) rec[0] = gtime();
-    if ((V.tasks[t].kind & 15) == 3) {
+    if (kLeaders && (V.tasks[t].kind & 15) == 3) {
       if (rec && threadIdx.x == 0) rec[1] = gtime();
       bwd_leader(V, t, Lb, err, D, rinv, seg, zs, ring);
     } else {
@@ -916,22 +929,6 @@ struct TreeView {
   int* counter;
 };
 
-// Sum over the 32 lanes of each of the 32 per-lane values a[0..31]: lane l
-// ends with the sum of a[l] (31 shuffles: each step halves the live values).
-__device__ __forceinline__ double lane_transpose_sum(double a[32]) {
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) {
-    const bool up = (lane & o) != 0;
-#pragma unroll
-    for (int k = 0; k < o; ++k) {
-      const double send = up ? a[k] : a[k + o];
-      const double keep = up ? a[k + o] : a[k];
-      a[k] = keep + __shfl_xor_sync(kFull, send, o);
-    }
-  }
-  return a[0];
-}
 
 // forward L y = b for supernode s by one warp; ys: this warp's 64 doubles of shared memory
 __device__ __forceinline__ void fwd_sn_warp(const TreeView& V, const double* Lb, int s, int inside_end, double* ys) {
@@ -2397,8 +2394,13 @@ void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaSt
     TEMF_CHECK_LAUNCH();
   }
   if (T.n_ftask) {
-    const int grid = std::min(persistent_grid(k_fwd_queued, 0), T.n_ftask);
-    k_fwd_queued<<<grid, kSolveThreads, 0, st>>>(vf, c.d_status.p + 1);
+    if (T.leaders) {
+      const int grid = std::min(persistent_grid(k_fwd_queued<true>, 0), T.n_ftask);
+      k_fwd_queued<true><<<grid, kSolveThreads, 0, st>>>(vf, c.d_status.p + 1);
+    } else {
+      const int grid = std::min(persistent_grid(k_fwd_queued<false>, 0), T.n_ftask);
+      k_fwd_queued<false><<<grid, kSolveThreads, 0, st>>>(vf, c.d_status.p + 1);
+    }
     TEMF_CHECK_LAUNCH();
   }
   if (inject) {
@@ -2408,8 +2410,13 @@ void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaSt
   if (sgn) scale_rows(c, sgn, x, 1, 1, st);  // indefinite factor: L S L^T
   TEMF_CUDA(cudaMemsetAsync(T.bacc.p, 0, (size_t)c.n_edges * sizeof(double), st));
   if (T.n_btask) {
-    const int gridb = std::min(persistent_grid(k_bwd_queued, 0), T.n_btask);
-    k_bwd_queued<<<gridb, kSolveThreads, 0, st>>>(vb, c.d_status.p + 1);
+    if (T.leaders) {
+      const int gridb = std::min(persistent_grid(k_bwd_queued<true>, 0), T.n_btask);
+      k_bwd_queued<true><<<gridb, kSolveThreads, 0, st>>>(vb, c.d_status.p + 1);
+    } else {
+      const int gridb = std::min(persistent_grid(k_bwd_queued<false>, 0), T.n_btask);
+      k_bwd_queued<false><<<gridb, kSolveThreads, 0, st>>>(vb, c.d_status.p + 1);
+    }
     TEMF_CHECK_LAUNCH();
   }
   if (T.ntree) {
