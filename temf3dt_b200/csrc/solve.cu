@@ -1637,7 +1637,15 @@ struct Sched {
 // (kind 4) after the claimable tasks.  The targets / owners of a run block's
 // first chunk exclude the run's own blocks (applied through the leader's
 // ring).  Single right-hand side only (128-row first chunks).
-void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lead_level = INT_MAX) {
+// group_from: at levels from this one up, the tasks of a level are ordered
+// by kind instead of by supernode (forward: every diagonal task of the level,
+// then the other chunks; backward: every other chunk, then the diagonal
+// tasks), so a task claimed in schedule order finds the tasks it waits for
+// claimed a whole level's worth earlier.  Only above the queue split: the
+// queued forward tasks rely on a supernode's chunks following its diagonal
+// task.
+void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lead_level = INT_MAX,
+                 int group_from = INT_MAX) {
   const int nsn = S.nsn;
   // distinct owner supernodes of rows [r0, r1) of s above `skip_to` (rows ascending -> owners ascending)
   std::vector<int> tmp;
@@ -1691,10 +1699,12 @@ void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lea
   // forward: bottom-up levels; per supernode its diagonal task (with the first
   // row chunk), then the other chunks
   for (int l = std::max(0, min_level); l < S.nlevels; ++l)
+    for (int pass = 0; pass < (l >= group_from ? 2 : 1); ++pass)
     for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
       const int s = S.level_sn[q];
       const int r = (int)(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]);
       for (int r0 = 0; r0 < std::max(r, 1); r0 += CH) {
+        if (l >= group_from && (pass == 0) != (r0 == 0)) continue;
         const int r1 = std::min(r, r0 + CH);
         if (r0 == 0 && run_a[s] >= 0) {
           owners(s, 0, r1, run_e[s]);
@@ -1735,17 +1745,21 @@ void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lea
     if (tmp.size() > 1) tmp.resize(1);
   };
   for (int l = S.nlevels - 1; l >= std::max(0, min_level); --l)
+    for (int pass = 0; pass < (l >= group_from ? 2 : 1); ++pass)
     for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
       const int s = S.level_sn[q];
       const int r = (int)(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]);
-      for (int r0 = CH; r0 < r; r0 += CH) {
-        const int r1 = std::min(r, r0 + CH);
-        o.bt.push_back({s, 1, r0, r1});
-        owners(s, r0, r1);
-        lowest();
-        o.btg.insert(o.btg.end(), tmp.begin(), tmp.end());
-        o.btp.push_back((int)o.btg.size());
+      if (l < group_from || pass == 0) {
+        for (int r0 = CH; r0 < r; r0 += CH) {
+          const int r1 = std::min(r, r0 + CH);
+          o.bt.push_back({s, 1, r0, r1});
+          owners(s, r0, r1);
+          lowest();
+          o.btg.insert(o.btg.end(), tmp.begin(), tmp.end());
+          o.btp.push_back((int)o.btg.size());
+        }
       }
+      if (l >= group_from && pass == 0) continue;
       const int r1 = std::min(r, CH);
       if (run_a[s] >= 0) {
         owners(s, 0, r1, run_e[s]);
@@ -1866,9 +1880,10 @@ void upload_queue_plan(const Sched& a, const Symbolic& S, int split, QueuePlan& 
 // Forward: queue phase, then the ordered phase; backward: the other way
 // round, the ordered tasks' completions feeding the queue.  Returns an empty
 // string or the first violation.
-std::string check_schedule(const Symbolic& S, int CH, int split, int min_level = 0, int lead_level = INT_MAX) {
+std::string check_schedule(const Symbolic& S, int CH, int split, int min_level = 0, int lead_level = INT_MAX,
+                           bool grouped = false) {
   Sched a;
-  build_sched(S, CH, a, min_level, lead_level);
+  build_sched(S, CH, a, min_level, lead_level, grouped ? std::max(split, min_level) : INT_MAX);
   int f_hi = 0, b_lo = 0;
   split_ranges(a, S, split, f_hi, b_lo);
   QueueData q;
@@ -2102,7 +2117,7 @@ void upload_tree_plan(temf_ctx& c, int level, int split, bool leaders) {
   cudaStream_t st = c.stream;
   const std::vector<int2> trees = build_trees(S, level);
   Sched a;
-  build_sched(S, kChunkRows, a, level, leaders ? std::max(level, split) : INT_MAX);
+  build_sched(S, kChunkRows, a, level, leaders ? std::max(level, split) : INT_MAX, std::max(level, split));
   T.level = level;
   T.leaders = leaders;
   if (T.bacc.n < (size_t)S.n) T.bacc.alloc(S.n);
@@ -2669,7 +2684,9 @@ std::string check_schedules(const Symbolic& S) {
   for (int sp : splits) {
     std::string w = check_schedule(S, kChunkRows, sp);
     if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ": " + w;
-    w = check_schedule(S, kChunkRows, sp, 0, sp);
+    w = check_schedule(S, kChunkRows, sp, 0, INT_MAX, true);
+    if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ", grouped levels: " + w;
+    w = check_schedule(S, kChunkRows, sp, 0, sp, true);
     if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ", run leaders: " + w;
     w = check_schedule(S, kChunkRowsMulti, sp);
     if (!w.empty()) return "64-row chunks, split " + std::to_string(sp) + ": " + w;
@@ -2680,9 +2697,9 @@ std::string check_schedules(const Symbolic& S) {
     std::string w = check_trees(S, l);
     if (!w.empty()) return "subtrees below level " + std::to_string(l) + ": " + w;
     for (int sp : split_candidates(S, l)) {
-      w = check_schedule(S, kChunkRows, sp, l);
+      w = check_schedule(S, kChunkRows, sp, l, INT_MAX, true);
       if (!w.empty()) return "subtree level " + std::to_string(l) + ", split " + std::to_string(sp) + ": " + w;
-      w = check_schedule(S, kChunkRows, sp, l, std::max(l, sp));
+      w = check_schedule(S, kChunkRows, sp, l, std::max(l, sp), true);
       if (!w.empty())
         return "subtree level " + std::to_string(l) + ", split " + std::to_string(sp) + ", run leaders: " + w;
     }
