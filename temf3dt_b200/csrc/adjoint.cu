@@ -191,7 +191,7 @@ void run_adjoint(temf_ctx& c, const double* dJ, int rows, const int* tet_cell, i
   DBuf<double*> lp;
   lp.alloc(1);
   ensure_update_buffer(c, 1);
-  if (c.slots[0].L.n < (size_t)c.sym.stored) c.slots[0].L.alloc(c.sym.stored);
+  if (c.slots[0].L.n < (size_t)slot_len(c)) c.slots[0].L.alloc(slot_len(c));
   k_set_ptr_adj<<<1, 1, 0, st>>>(lp.p, c.slots[0].L.p);
   TEMF_CHECK_LAUNCH();
   clear_solve_error_flag(c);

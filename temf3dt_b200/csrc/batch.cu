@@ -151,7 +151,7 @@ struct BatchEngine {
       TEMF_CUDA(cudaMallocHost((void**)&R->coef_h, (std::max(dbl, 8) + 8) * sizeof(double)));
       TEMF_CUDA(cudaMallocHost((void**)&R->err_h, 2 * sizeof(double)));
       for (int s = 0; s < 2; ++s)
-        if (c.slots[s].L.n < (size_t)c.sym.stored) c.slots[s].L.alloc(c.sym.stored);
+        if (c.slots[s].L.n < (size_t)slot_len(c)) c.slots[s].L.alloc(slot_len(c));
       ensure_update_buffer(c, 1);
       k_set_ptr_b<<<1, 1, 0, st>>>(R->lptr.p + 0, c.slots[0].L.p);
       k_set_ptr_b<<<1, 1, 0, st>>>(R->lptr.p + 1, c.slots[1].L.p);

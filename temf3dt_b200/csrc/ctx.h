@@ -54,6 +54,11 @@ struct FactorPlan {
   int64_t n_relind = 0;
   int64_t n_tiles = 0;
   int n_runs = 0;              // runs of column blocks whose updates are summed
+  // The single-column sweeps' copy of each diagonal block, after the panels in
+  // the same slot allocation: c x c column-major, row i scaled by 1/L_ii
+  // (unit lower triangle below the diagonal) and 1/L_ii on the diagonal.
+  DBuf<int64_t> sn_Dptr;       // per supernode: offset of its copy (from the panel base)
+  int64_t dsc_len = 0;         // doubles of all copies
 };
 
 // A task of the persistent triangular-solve kernels: the diagonal block of

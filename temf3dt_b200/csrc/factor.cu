@@ -56,7 +56,7 @@ constexpr double kPivotTol = 1e-13;
 __global__ void __launch_bounds__(kFacThreads) k_potrf(
     const int* __restrict__ level_sn, const int* __restrict__ sn_first,
     const int64_t* __restrict__ rows_ptr, const int64_t* __restrict__ Lptr, double* __restrict__ L,
-    int* __restrict__ status, double* __restrict__ sgn) {
+    int* __restrict__ status, double* __restrict__ sgn, const int64_t* __restrict__ Dptr) {
   constexpr int CB = kSnCols;
   __shared__ double D[CB][CB + 1];
   __shared__ double diag[CB];  // L_kk, written into D after the loop
@@ -111,11 +111,18 @@ __global__ void __launch_bounds__(kFacThreads) k_potrf(
     }
     __syncthreads();
   }
-  if (tid < c) D[tid][tid] = diag[tid];
+  if (tid < c) {
+    D[tid][tid] = diag[tid];
+    d0[tid] = 1.0 / diag[tid];
+  }
   __syncthreads();
+  // the panel's block, and the sweeps' copy: row i scaled by 1/L_ii, 1/L_ii on
+  // the diagonal, zeros above (c x c, column-major)
+  double* Q = L + Dptr[s];
   for (int idx = tid; idx < c * c; idx += blockDim.x) {
     const int j = idx / c, i = idx % c;
     if (i >= j) P[(int64_t)j * ld + i] = D[i][j];
+    Q[idx] = i > j ? D[i][j] * d0[i] : (i == j ? d0[i] : 0.0);
   }
 }
 
@@ -196,10 +203,12 @@ __device__ __forceinline__ void cp_async8_f(void* smem, const void* gmem) {
 // m = 1 otherwise.  jl > 0 restricts the tile to columns j < jl (inside a run,
 // a member updates the later members' columns only).  C is scattered into the
 // ancestors' panels through the relative indices of s.  The K loop runs over
-// 32-column chunks of the members, double-buffered: the next chunk's copies
-// are in flight while the DMMA tiles consume the current one.
-constexpr int kUpdChunk = 32;
-constexpr int kUpdMaxMembers = 4;
+// 16-column chunks of the members, double-buffered: the next chunk's copies
+// are in flight while the DMMA tiles consume the current one (37 KB of
+// shared memory: five CTAs per SM, by registers, where 32-column chunks
+// allowed three).
+constexpr int kUpdChunk = 16;
+constexpr int kUpdMaxMembers = 8;
 
 __global__ void __launch_bounds__(128) k_update(
     const UpdTile* __restrict__ tiles, const int* __restrict__ sn_first,
@@ -219,20 +228,25 @@ __global__ void __launch_bounds__(128) k_update(
   const int64_t rp = rows_ptr[s];
   const int r = (int)(rows_ptr[s + 1] - rp);
   const int tid = threadIdx.x;
-  // chunks of the members: (member, first column)
+  // K chunks of kUpdChunk columns over the members in order; a cursor
+  // (member, first column) for the chunk being copied and one for the chunk
+  // being multiplied
   int nch = 0;
-  int ch_q[2 * kUpdMaxMembers], ch_k0[2 * kUpdMaxMembers];
   for (int u = 0; u < m; ++u) {
     const int q = s - m + 1 + u;
-    const int cq = sn_first[q + 1] - sn_first[q];
-    for (int k0 = 0; k0 < cq; k0 += kUpdChunk) {
-      ch_q[nch] = q;
-      ch_k0[nch] = k0;
-      ++nch;
-    }
+    nch += (sn_first[q + 1] - sn_first[q] + kUpdChunk - 1) / kUpdChunk;
   }
-  auto issue = [&](int ch, int buf) {
-    const int q = ch_q[ch], k0 = ch_k0[ch];
+  int cp_q = s - m + 1, cp_k0 = 0, mm_q = s - m + 1, mm_k0 = 0;
+  auto advance = [&](int& q, int& k0) {
+    k0 += kUpdChunk;
+    if (k0 >= sn_first[q + 1] - sn_first[q]) {
+      ++q;
+      k0 = 0;
+    }
+  };
+  auto issue = [&](int buf) {
+    const int q = cp_q, k0 = cp_k0;
+    advance(cp_q, cp_k0);
     const int fq = sn_first[q];
     const int cq = sn_first[q + 1] - fq;
     const int rq = (int)(rows_ptr[q + 1] - rows_ptr[q]);
@@ -259,11 +273,11 @@ __global__ void __launch_bounds__(128) k_update(
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
-  issue(0, 0);
+  issue(0);
   for (int ch = 0; ch < nch; ++ch) {
     const int buf = ch & 1;
     if (ch + 1 < nch) {
-      issue(ch + 1, buf ^ 1);
+      issue(buf ^ 1);
       asm volatile("cp.async.wait_group 1;\n" ::: "memory");
     } else {
       asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -272,14 +286,15 @@ __global__ void __launch_bounds__(128) k_update(
     double* A = As(buf);
     const double* B = Bs(buf);
     if (sgn) {  // indefinite mode: A22 -= L21 S11 L21^T
-      const int fq = sn_first[ch_q[ch]];
-      const int cq = sn_first[ch_q[ch] + 1] - fq;
+      const int fq = sn_first[mm_q];
+      const int cq = sn_first[mm_q + 1] - fq;
       for (int idx = tid; idx < kUpdChunk * kUpdTile; idx += blockDim.x) {
         const int k = idx / kUpdTile, ii = idx % kUpdTile;
-        if (ch_k0[ch] + k < cq) A[k * kLdsU + ii] *= sgn[fq + ch_k0[ch] + k];
+        if (mm_k0 + k < cq) A[k * kLdsU + ii] *= sgn[fq + mm_k0 + k];
       }
       __syncthreads();
     }
+    advance(mm_q, mm_k0);
 #pragma unroll 2
     for (int k0 = 0; k0 < kUpdChunk; k0 += 4) {
       double fa[4], fb[4];
@@ -357,6 +372,17 @@ void build_factor_plan(temf_ctx& c) {
 
   auto width = [&](int s) { return S.sn_first[s + 1] - S.sn_first[s]; };
   auto nrows = [&](int s) { return (int64_t)(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]); };
+  {  // the sweeps' scaled copies of the diagonal blocks, after the panels
+    std::vector<int64_t> dp(S.nsn + 1);
+    int64_t o = S.stored;
+    for (int s = 0; s < S.nsn; ++s) {
+      dp[s] = o;
+      o += (int64_t)width(s) * width(s);
+    }
+    dp[S.nsn] = o;
+    F.dsc_len = o - S.stored;
+    F.sn_Dptr.upload(dp.data(), dp.size(), st);
+  }
   // position of global row i in the panel of supernode t (i >= first column of t)
   auto panel_row = [&](int t, int i) -> int64_t {
     const int ft = S.sn_first[t], ct = width(t);
@@ -497,7 +523,7 @@ void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
   FactorPlan& F = c.fplan;
   FactorSlot& fs = c.slots[slot];
   cudaStream_t st = c.stream;
-  if (fs.L.n < (size_t)S.stored) fs.L.alloc(S.stored);
+  if (fs.L.n < (size_t)slot_len(c)) fs.L.alloc(slot_len(c));
   TEMF_CUDA(cudaMemsetAsync(fs.L.p, 0, S.stored * sizeof(double), st));
   int init[3] = {INT_MAX, 0, 0};
   TEMF_CUDA(cudaMemcpyAsync(c.d_status.p, &init[0], sizeof(int), cudaMemcpyHostToDevice, st));
@@ -522,7 +548,7 @@ void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
     const int cnt = S.level_ptr[l + 1] - S.level_ptr[l];
     if (cnt > 0) {
       k_potrf<<<cnt, kFacThreads, 0, st>>>(F.level_sn.p + S.level_ptr[l], F.sn_first.p, F.sn_rows_ptr.p,
-                                           F.sn_Lptr.p, fs.L.p, c.d_status.p, sgn);
+                                           F.sn_Lptr.p, fs.L.p, c.d_status.p, sgn, F.sn_Dptr.p);
       TEMF_CHECK_LAUNCH();
     }
     const int64_t c0 = F.trsm_level_ptr[l], c1 = F.trsm_level_ptr[l + 1];

@@ -6,6 +6,8 @@ constexpr int kSnCols = 64;     // maximum supernode width (columns per panel)
 constexpr int kUpdTile = 64;    // update tile edge
 
 void build_factor_plan(temf_ctx& c);
+// Doubles of one factor slot: the panels, then the scaled diagonal blocks.
+inline int64_t slot_len(const temf_ctx& c) { return c.sym.stored + c.fplan.dsc_len; }
 // Numeric LL^T of A = 3 M + 2 dt K into `slot`.  Returns 0 or the 1-based
 // (original numbering) column of the first non-positive pivot.
 int numeric_factor(temf_ctx& c, int slot, double dt);

@@ -155,7 +155,7 @@ struct Engine {
     TEMF_CUDA(cudaEventCreate(&ev1));
     ensure_update_buffer(c, nrhs);
     for (int s = 0; s < 2; ++s)
-      if (c.slots[s].L.n < (size_t)c.sym.stored) c.slots[s].L.alloc(c.sym.stored);
+      if (c.slots[s].L.n < (size_t)slot_len(c)) c.slots[s].L.alloc(slot_len(c));
     k_set_ptr<<<1, 1, 0, st>>>(lptr.p + 0, c.slots[0].L.p);
     k_set_ptr<<<1, 1, 0, st>>>(lptr.p + 1, c.slots[1].L.p);
     TEMF_CHECK_LAUNCH();

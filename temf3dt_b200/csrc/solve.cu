@@ -160,12 +160,109 @@ __device__ __forceinline__ void diag_solve_bwd_warp(const double (*D)[kSnCols + 
   }
 }
 
+// The same blocking on the factor's scaled copy of the block: D holds the
+// unit lower triangle L_ij / L_ii below its diagonal.  Forward: L y = b is
+// D y = b / L_ii, so each unknown is its scaled right-hand side minus the
+// scaled products of the unknowns before it -- one FMA per column on the
+// dependent chain (FP64 latency is about 23 cycles on sm_100a, a shuffle
+// about 26), against an FMA and a multiply with the unscaled block.
+// Backward: L^T x = z is D^T w = z with w_i = L_ii x_i; the caller scales w.
+__device__ __forceinline__ void unit_solve_fwd_warp(const double (*D)[kSnCols + 1], double& v0, double& v1, int c) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k0 = 0; k0 < kSnCols; k0 += 8) {
+    if (k0 < c) {  // warp-uniform
+      double y[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) y[i] = __shfl_sync(0xffffffffu, k0 < 32 ? v0 : v1, (k0 + i) & 31);
+#pragma unroll
+      for (int i = 1; i < 8; ++i) {
+        if (k0 + i < c) {
+#pragma unroll
+          for (int j = 0; j < i; ++j) y[i] -= D[k0 + i][k0 + j] * y[j];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        if (lane == ((k0 + i) & 31) && k0 + i < c) {
+          if (k0 < 32) v0 = y[i];
+          else v1 = y[i];
+        }
+      }
+      if (k0 < 32 && lane >= k0 + 8 && lane < c) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v0 -= D[lane][k0 + j] * y[j];
+      }
+      if (lane + 32 >= k0 + 8 && lane + 32 < c) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v1 -= D[lane + 32][k0 + j] * y[j];
+      }
+    }
+  }
+}
+__device__ __forceinline__ void unit_solve_bwd_warp(const double (*D)[kSnCols + 1], double& v0, double& v1, int c) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k0 = kSnCols - 8; k0 >= 0; k0 -= 8) {
+    if (k0 < c) {  // warp-uniform
+      double x[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) x[i] = __shfl_sync(0xffffffffu, k0 < 32 ? v0 : v1, (k0 + i) & 31);
+#pragma unroll
+      for (int i = 6; i >= 0; --i) {
+        if (k0 + i < c) {
+#pragma unroll
+          for (int j = 7; j > i; --j)
+            if (k0 + j < c) x[i] -= D[k0 + j][k0 + i] * x[j];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        if (lane == ((k0 + i) & 31) && k0 + i < c) {
+          if (k0 < 32) v0 = x[i];
+          else v1 = x[i];
+        }
+      }
+      if (lane < k0 && lane < c) {
+#pragma unroll
+        for (int j = 7; j >= 0; --j)
+          if (k0 + j < c) v0 -= D[k0 + j][lane] * x[j];
+      }
+      if (k0 >= 32 && lane + 32 < k0 && lane + 32 < c) {
+#pragma unroll
+        for (int j = 7; j >= 0; --j)
+          if (k0 + j < c) v1 -= D[k0 + j][lane + 32] * x[j];
+      }
+    }
+  }
+}
+
 // Dense lower-triangular solve of the c x c diagonal block held in D (shared)
 // for nrhs columns of ys (row-major c x nrhs), forward (L y = b) or backward
 // (L^T x = z).  nrhs == 1 runs in one warp (the blocked substitution above).
 __device__ void diag_solve(const double (*D)[kSnCols + 1], const double* rinv, double* ys, int c, int nrhs,
-                           bool forward) {
+                           bool forward, bool scaled = false) {
   const int tid = threadIdx.x;
+  if (nrhs == 1 && scaled) {  // D: the factor's scaled copy; rinv: 1 / L_ii
+    if (tid < 32) {
+      const int lane = tid;
+      double v0 = lane < c ? ys[lane] : 0.0;
+      double v1 = lane + 32 < c ? ys[lane + 32] : 0.0;
+      if (forward) {
+        v0 *= lane < c ? rinv[lane] : 0.0;
+        v1 *= lane + 32 < c ? rinv[lane + 32] : 0.0;
+        unit_solve_fwd_warp(D, v0, v1, c);
+      } else {
+        unit_solve_bwd_warp(D, v0, v1, c);
+        v0 *= lane < c ? rinv[lane] : 0.0;
+        v1 *= lane + 32 < c ? rinv[lane + 32] : 0.0;
+      }
+      if (lane < c) ys[lane] = v0;
+      if (lane + 32 < c) ys[lane + 32] = v1;
+    }
+    __syncthreads();
+    return;
+  }
   if (nrhs == 1) {
     if (tid < 32) {
       const int lane = tid;
@@ -211,11 +308,24 @@ __device__ __forceinline__ void load_diag_start(double (*D)[kSnCols + 1], const 
     if (i >= j) cp_async8(&D[i][j], P + (int64_t)j * ld + i);
   }
 }
-__device__ __forceinline__ void load_diag_finish(double (*D)[kSnCols + 1], double* rinv, int c) {
+__device__ __forceinline__ void load_diag_finish(double (*D)[kSnCols + 1], double* rinv, int c, bool scaled = false) {
   cp_async_wait_all();
   __syncthreads();
-  if ((int)threadIdx.x < c) rinv[threadIdx.x] = 1.0 / D[threadIdx.x][threadIdx.x];
+  if ((int)threadIdx.x < c) rinv[threadIdx.x] = scaled ? D[threadIdx.x][threadIdx.x] : 1.0 / D[threadIdx.x][threadIdx.x];
   __syncthreads();
+}
+// the factor's scaled copy of the block (c x c, column-major), lower triangle
+__device__ __forceinline__ void load_diag_start_scaled(double (*D)[kSnCols + 1], const double* Q, int c) {
+  for (int idx = threadIdx.x; idx < c * c; idx += blockDim.x) {
+    const int j = idx / c, i = idx - j * c;
+    if (i >= j) cp_async8(&D[i][j], Q + idx);
+  }
+}
+// single column: the scaled copy when the view has one, else the panel's block
+__device__ __forceinline__ void load_diag_start_1(double (*D)[kSnCols + 1], const SweepView& V, const double* Lb, int s,
+                                                  const double* P, int c, int64_t ld) {
+  if (V.Dptr) load_diag_start_scaled(D, Lb + V.Dptr[s], c);
+  else load_diag_start(D, P, c, ld);
 }
 
 // Row-chunk products, single right-hand side.  The panel values are loaded
@@ -418,14 +528,16 @@ __device__ __forceinline__ void fwd_task(const SweepView& V, int t, const double
       tg_ex = V.expect[tg_o];
     }
   }
+  const bool sc = nrhs == 1 && V.Dptr != nullptr;
   if (T.kind == 0) {
-    load_diag_start(D, P, c, ld);
+    if (sc) load_diag_start_scaled(D, Lb + V.Dptr[s], c);
+    else load_diag_start(D, P, c, ld);
     if (tid == 0 && !queued) wait_geq(ready + s, V.expect[s], err, 1, spin_limit(V));
     __syncthreads();
     if (stamp && tid == 0) *stamp = gtime();
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) ys[idx] = __ldcg(x + (int64_t)f * nrhs + idx);
-    load_diag_finish(D, rinv, c);
-    diag_solve(D, rinv, ys, c, nrhs, true);
+    load_diag_finish(D, rinv, c, sc);
+    diag_solve(D, rinv, ys, c, nrhs, true, sc);
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = ys[idx];
     // y_s is published together with the first chunk's pushes below: one fence for both
   } else {
@@ -524,7 +636,11 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
   if (nrhs == 1 && nr > 0) pre_fwd(R, P + c, c, ld, T.r0 + tid, tid < nr);
   // one chunk row per thread for a single column: its index read before the wait
   const int row_t = (nrhs == 1 && tid < nr) ? V.sn_rows[rp + T.r0 + tid] : 0;
-  if (T.kind == 0) load_diag_start(D, P, c, ld);
+  const bool sc = nrhs == 1 && V.Dptr != nullptr;
+  if (T.kind == 0) {
+    if (sc) load_diag_start_scaled(D, Lb + V.Dptr[s], c);
+    else load_diag_start(D, P, c, ld);
+  }
   const bool queued = in_queue(V, t);
   // the chunk's rows need their owners' x; the diagonal task also its other chunks
   if (!queued) {  // one polling thread per owner (and one for the chunk count)
@@ -624,8 +740,8 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
         zs[idx] = v;
       }
     }
-    load_diag_finish(D, rinv, c);
-    diag_solve(D, rinv, zs, c, nrhs, false);
+    load_diag_finish(D, rinv, c, sc);
+    diag_solve(D, rinv, zs, c, nrhs, false, sc);
     for (int idx = tid; idx < c * nrhs; idx += blockDim.x) x[(int64_t)f * nrhs + idx] = zs[idx];
     __threadfence();
     __syncthreads();
@@ -704,8 +820,9 @@ __device__ void fwd_leader(const SweepView& V, int t, const double* Lb, int* err
     const int64_t r = V.rows_ptr[a + 1] - V.rows_ptr[a], ld = c + r;
     const double* P = Lb + V.Lptr[a];
     pre_fwd(R, P + c, c, ld, tid, tid < (r < kChunkRows ? r : (int64_t)kChunkRows));
-    load_diag_start(D, P, c, ld);
+    load_diag_start_1(D, V, Lb, a, P, c, ld);
   }
+  const bool sc = V.Dptr != nullptr;
   for (int q = a; q <= e; ++q) {
     const int f = V.sn_first[q], c = V.sn_first[q + 1] - f;
     const int64_t rp = V.rows_ptr[q], r = V.rows_ptr[q + 1] - rp;
@@ -718,8 +835,8 @@ __device__ void fwd_leader(const SweepView& V, int t, const double* Lb, int* err
       ys[j] = __ldcg(x + f + j) + ring[slot];  // the ring holds the negated in-run contributions
       ring[slot] = 0.0;
     }
-    load_diag_finish(D, rinv, c);
-    diag_solve(D, rinv, ys, c, 1, true);
+    load_diag_finish(D, rinv, c, sc);
+    diag_solve(D, rinv, ys, c, 1, true, sc);
     for (int j = tid; j < c; j += blockDim.x) x[f + j] = ys[j];
     if (tid < r1) {
       const double v = fin_fwd(R, ys, c);
@@ -740,7 +857,7 @@ __device__ void fwd_leader(const SweepView& V, int t, const double* Lb, int* err
       const int64_t rn = V.rows_ptr[q + 2] - V.rows_ptr[q + 1], ldn = cn + rn;
       const double* Pn = Lb + V.Lptr[q + 1];
       pre_fwd(R, Pn + cn, cn, ldn, tid, tid < (rn < kChunkRows ? rn : (int64_t)kChunkRows));
-      load_diag_start(D, Pn, cn, ldn);
+      load_diag_start_1(D, V, Lb, q + 1, Pn, cn, ldn);
     }
   }
 }
@@ -761,8 +878,9 @@ __device__ void bwd_leader(const SweepView& V, int t, const double* Lb, int* err
     const double* P = Lb + V.Lptr[e];
     const int r1 = (int)(r < kChunkRows ? r : (int64_t)kChunkRows);
     if (r1 > 0) pre_fwd(R, P + c, c, ld, tid, tid < r1);
-    load_diag_start(D, P, c, ld);
+    load_diag_start_1(D, V, Lb, e, P, c, ld);
   }
+  const bool sc = V.Dptr != nullptr;
   for (int q = e; q >= a; --q) {
     const int f = V.sn_first[q], c = V.sn_first[q + 1] - f;
     const int64_t rp = V.rows_ptr[q], r = V.rows_ptr[q + 1] - rp;
@@ -817,8 +935,8 @@ __device__ void bwd_leader(const SweepView& V, int t, const double* Lb, int* err
       if (nch > 1) v -= psum[j] + psum[kSnCols + j];
       zs[j] = v;
     }
-    load_diag_finish(D, rinv, c);
-    diag_solve(D, rinv, zs, c, 1, false);
+    load_diag_finish(D, rinv, c, sc);
+    diag_solve(D, rinv, zs, c, 1, false, sc);
     for (int j = tid; j < c; j += blockDim.x) {
       x[f + j] = zs[j];
       ring[(f + j - f_run) & (kRing - 1)] = zs[j];
@@ -833,7 +951,7 @@ __device__ void bwd_leader(const SweepView& V, int t, const double* Lb, int* err
       const double* Pn = Lb + V.Lptr[q - 1];
       const int r1n = (int)(rn < kChunkRows ? rn : (int64_t)kChunkRows);
       if (r1n > 0) pre_fwd(R, Pn + cn, cn, ldn, tid, tid < r1n);
-      load_diag_start(D, Pn, cn, ldn);
+      load_diag_start_1(D, V, Lb, q - 1, Pn, cn, ldn);
     }
   }
 }
@@ -2309,6 +2427,7 @@ static void tree_views(temf_ctx& c, double* const* Lbase, double* x, SweepView& 
                  q + nf, words + 1, words + 3, Q.bdiag.p, Q.bdep_ptr.p, Q.bdep.p, Q.bneed.p, q + nf + nb,
                  Q.b_lo, nb, 0, c.spin_limit};
   vb.bacc = T.bacc.p;  // allocated with the plan
+  vf.Dptr = vb.Dptr = F.sn_Dptr.p;
 }
 
 static void reset_tree_queues(temf_ctx& c, cudaStream_t st) {

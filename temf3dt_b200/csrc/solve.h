@@ -38,6 +38,10 @@ struct SweepView {
   int tag;                 // model id << 24 when several models share one queue (0 otherwise)
   int spin = 0;            // iterations a device wait may spin before it gives up (0: the default)
   double* bacc = nullptr;  // backward, one column: chunk partial sums accumulated per column (FP64 atomics)
+  // single column: offsets (from the panel base) of the factor's scaled copies
+  // of the diagonal blocks (unit lower triangle, reciprocal diagonal); null:
+  // the tasks read the blocks from the panels
+  const int64_t* Dptr = nullptr;
 };
 
 void build_solve_plan(temf_ctx& c);
