@@ -1045,63 +1045,17 @@ struct TreeView {
   double* const* Lbase;
   double* x;
   int* counter;
+  const int64_t* Dptr;  // the factor's scaled diagonal copies
 };
 
 
-// forward L y = b for supernode s by one warp; ys: this warp's 64 doubles of shared memory
-__device__ __forceinline__ void fwd_sn_warp(const TreeView& V, const double* Lb, int s, int inside_end, double* ys) {
+// Rows below the diagonal block, 32 at a time: push -L21 y (ys: y in shared
+// memory), plain writes for rows inside the subtree, atomics above it.
+__device__ __forceinline__ void fwd_sn_rows(const TreeView& V, const double* P, int s, int c, int r, int64_t ld,
+                                            int inside_end, const double* ys) {
   const int lane = threadIdx.x & 31;
-  const int f = V.sn_first[s];
-  const int c = V.sn_first[s + 1] - f;
-  const int64_t rp = V.rows_ptr[s];
-  const int r = (int)(V.rows_ptr[s + 1] - rp);
-  const int64_t ld = c + r;
-  const double* P = Lb + V.Lptr[s];
   double* x = V.x;
-  const int c0 = min(c, 32);
-  // columns 0..31: lane i holds row i of the diagonal block
-  double a[32];
-#pragma unroll
-  for (int j = 0; j < 32; ++j) a[j] = (j < lane && lane < c) ? P[(int64_t)j * ld + lane] : 0.0;
-  const double rinv0 = lane < c ? 1.0 / P[(int64_t)lane * ld + lane] : 0.0;
-  double v0 = lane < c ? __ldcg(x + f + lane) : 0.0;
-#pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    if (j < c0) {
-      if (lane == j) v0 *= rinv0;
-      const double yj = __shfl_sync(kFull, v0, j);
-      if (lane > j) v0 -= a[j] * yj;
-    }
-  }
-  double v1 = 0.0;
-  if (c > 32) {  // warp-uniform: rows 32..c-1
-    const bool on = 32 + lane < c;
-    v1 = on ? __ldcg(x + f + 32 + lane) : 0.0;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) a[j] = on ? P[(int64_t)j * ld + 32 + lane] : 0.0;
-    double acc = 0.0;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) acc += a[j] * __shfl_sync(kFull, v0, j);
-    v1 -= acc;
-#pragma unroll
-    for (int m = 0; m < 32; ++m) a[m] = (m < lane && on) ? P[(int64_t)(32 + m) * ld + 32 + lane] : 0.0;
-    const double rinv1 = on ? 1.0 / P[(int64_t)(32 + lane) * ld + 32 + lane] : 0.0;
-#pragma unroll
-    for (int m = 0; m < 32; ++m) {
-      if (32 + m < c) {
-        if (lane == m) v1 *= rinv1;
-        const double ym = __shfl_sync(kFull, v1, m);
-        if (lane > m) v1 -= a[m] * ym;
-      }
-    }
-  }
-  if (lane < c) x[f + lane] = v0;
-  if (32 + lane < c) x[f + 32 + lane] = v1;
-  ys[lane] = lane < c ? v0 : 0.0;
-  ys[32 + lane] = 32 + lane < c ? v1 : 0.0;
-  __syncwarp();
-  // rows below the diagonal block, 32 at a time: push -L21 y
-  const int* rows = V.sn_rows + rp;
+  const int* rows = V.sn_rows + V.rows_ptr[s];
   for (int q0 = 0; q0 < r; q0 += 32) {
     const int i = q0 + lane;
     if (i < r) {
@@ -1124,6 +1078,60 @@ __device__ __forceinline__ void fwd_sn_warp(const TreeView& V, const double* Lb,
     }
   }
   __syncwarp();
+}
+
+// forward L y = b for supernode s by one warp (ys: this warp's 64 doubles of
+// shared memory).  The diagonal block comes from the factor's scaled copy Q
+// (c x c column-major: L_ij / L_ii below the diagonal, 1 / L_ii on it), so
+// y = D^-1 (b / L_ii) with one FMA per column on the dependent chain; lane i
+// holds row i of the block.
+__device__ __forceinline__ void fwd_sn_warp(const TreeView& V, const double* Lb, int s, int inside_end, double* ys) {
+  const int lane = threadIdx.x & 31;
+  const int f = V.sn_first[s];
+  const int c = V.sn_first[s + 1] - f;
+  const int r = (int)(V.rows_ptr[s + 1] - V.rows_ptr[s]);
+  const int64_t ld = c + r;
+  const double* P = Lb + V.Lptr[s];
+  const double* Q = Lb + V.Dptr[s];
+  double* x = V.x;
+  const int c0 = min(c, 32);
+  double a[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) a[j] = (j < lane && lane < c) ? Q[j * c + lane] : 0.0;
+  double v0 = lane < c ? __ldcg(x + f + lane) * Q[lane * c + lane] : 0.0;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j < c0) {
+      const double yj = __shfl_sync(kFull, v0, j);
+      if (lane > j) v0 -= a[j] * yj;
+    }
+  }
+  double v1 = 0.0;
+  if (c > 32) {  // warp-uniform: rows 32..c-1
+    const bool on = 32 + lane < c;
+    v1 = on ? __ldcg(x + f + 32 + lane) * Q[(32 + lane) * c + 32 + lane] : 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) a[j] = on ? Q[j * c + 32 + lane] : 0.0;
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) acc += a[j] * __shfl_sync(kFull, v0, j);
+    v1 -= acc;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) a[m] = (m < lane && on) ? Q[(32 + m) * c + 32 + lane] : 0.0;
+#pragma unroll
+    for (int m = 0; m < 32; ++m) {
+      if (32 + m < c) {
+        const double ym = __shfl_sync(kFull, v1, m);
+        if (lane > m) v1 -= a[m] * ym;
+      }
+    }
+  }
+  if (lane < c) x[f + lane] = v0;
+  if (32 + lane < c) x[f + 32 + lane] = v1;
+  ys[lane] = lane < c ? v0 : 0.0;
+  ys[32 + lane] = 32 + lane < c ? v1 : 0.0;
+  __syncwarp();
+  fwd_sn_rows(V, P, s, c, r, ld, inside_end, ys);
 }
 
 // backward L^T x = y for supernode s by one warp; xs: this warp's kTreeXs
@@ -1172,42 +1180,43 @@ __device__ __forceinline__ void bwd_sn_warp(const TreeView& V, const double* Lb,
     if (h == 0) v0 -= p;
     else v1 -= p;
   }
-  // diagonal block, columns c-1 .. 32 (lane m holds column 32 + m)
+  // diagonal block on the factor's scaled copy Q (c x c column-major,
+  // D_ij = L_ij / L_ii below the diagonal, 1 / L_ii on it): D^T w = z with
+  // w_i = L_ii x_i, one FMA per column on the dependent chain, then x = w / L_ii
+  const double* Q = Lb + V.Dptr[s];
   double b[32];
-  if (c > 32) {
+  if (c > 32) {  // columns c-1 .. 32 (lane m holds column 32 + m)
     const bool on = 32 + lane < c;
 #pragma unroll
-    for (int m = 0; m < 32; ++m) b[m] = (m > lane && 32 + m < c && on) ? P[(int64_t)(32 + lane) * ld + 32 + m] : 0.0;
-    const double rinv1 = on ? 1.0 / P[(int64_t)(32 + lane) * ld + 32 + lane] : 0.0;
+    for (int m = 0; m < 32; ++m) b[m] = (m > lane && 32 + m < c && on) ? Q[(32 + lane) * c + 32 + m] : 0.0;
 #pragma unroll
     for (int m = 31; m >= 0; --m) {
       if (32 + m < c) {
-        if (lane == m) v1 *= rinv1;
-        const double xm = __shfl_sync(kFull, v1, m);
-        if (lane < m) v1 -= b[m] * xm;
+        const double wm = __shfl_sync(kFull, v1, m);
+        if (lane < m) v1 -= b[m] * wm;
       }
     }
     // their contribution to columns 0..31 (lane l holds column l)
 #pragma unroll
-    for (int m = 0; m < 32; ++m) b[m] = (32 + m < c && lane < c) ? P[(int64_t)lane * ld + 32 + m] : 0.0;
+    for (int m = 0; m < 32; ++m) b[m] = (32 + m < c && lane < c) ? Q[lane * c + 32 + m] : 0.0;
     double acc2 = 0.0;
 #pragma unroll
     for (int m = 0; m < 32; ++m) acc2 += b[m] * __shfl_sync(kFull, v1, m);
     v0 -= acc2;
+    v1 *= on ? Q[(32 + lane) * c + 32 + lane] : 0.0;
   }
   // columns min(c,32)-1 .. 0
   const int c0 = min(c, 32);
 #pragma unroll
-  for (int m = 0; m < 32; ++m) b[m] = (m > lane && m < c0) ? P[(int64_t)lane * ld + m] : 0.0;
-  const double rinv0 = lane < c ? 1.0 / P[(int64_t)lane * ld + lane] : 0.0;
+  for (int m = 0; m < 32; ++m) b[m] = (m > lane && m < c0) ? Q[lane * c + m] : 0.0;
 #pragma unroll
   for (int m = 31; m >= 0; --m) {
     if (m < c0) {
-      if (lane == m) v0 *= rinv0;
-      const double xm = __shfl_sync(kFull, v0, m);
-      if (lane < m) v0 -= b[m] * xm;
+      const double wm = __shfl_sync(kFull, v0, m);
+      if (lane < m) v0 -= b[m] * wm;
     }
   }
+  v0 *= lane < c ? Q[lane * c + lane] : 0.0;
   if (lane < c) x[f + lane] = v0;
   if (32 + lane < c) x[f + 32 + lane] = v1;
   __syncwarp();
@@ -2524,7 +2533,8 @@ void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaSt
   if (T.ntree) {
     k_fwd_subtrees<<<tgrid, kTreeThreads, 0, st>>>(TreeView{T.trees.p, T.ntree, c.fplan.sn_first.p,
                                                             c.fplan.sn_rows_ptr.p, c.fplan.sn_rows.p,
-                                                            c.fplan.sn_Lptr.p, Lbase, x, tcount});
+                                                            c.fplan.sn_Lptr.p, Lbase, x, tcount,
+                                                            c.fplan.sn_Dptr.p});
     TEMF_CHECK_LAUNCH();
   }
   if (T.n_ftask) {
@@ -2556,7 +2566,8 @@ void launch_solve(temf_ctx& c, double* const* Lbase, double* x, int nrhs, cudaSt
   if (T.ntree) {
     k_bwd_subtrees<<<tgrid, kTreeThreads, 0, st>>>(TreeView{T.trees.p, T.ntree, c.fplan.sn_first.p,
                                                             c.fplan.sn_rows_ptr.p, c.fplan.sn_rows.p,
-                                                            c.fplan.sn_Lptr.p, Lbase, x, tcount + 1});
+                                                            c.fplan.sn_Lptr.p, Lbase, x, tcount + 1,
+                                                            c.fplan.sn_Dptr.p});
     TEMF_CHECK_LAUNCH();
   }
 }
