@@ -623,8 +623,9 @@ def ours(args):
         nbytes = 2 * 8 * st["nnz_L"] + 12 * st["nnz_A"] + 4 * st["n"] + 24 * st["n"]
         ach = nbytes / (ms_step / 1e3) / 1e9
         # DRAM bytes per step scaled from the ncu capture of the same sweep
-        # kernels on the config-0 model: 1.016 x stored panel bytes per sweep
-        traffic = 2 * 1.016 * 8 * st["stored"] + 12 * st["nnz_A"] + 28 * st["n"]
+        # kernels on the config-0 model (dram__bytes_read + write per launch):
+        # 1.047 (forward) and 1.077 (backward) x the stored panel bytes
+        traffic = (1.047 + 1.077) * 8 * st["stored"] + 12 * st["nnz_A"] + 28 * st["n"]
         roof = {"bound": "hbm", "achieved": ach / 1.0, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                 "traffic": traffic,
                 "kernel": "one time step: BDF2 SpMV + persistent forward/backward supernodal sweeps + receivers",
@@ -694,6 +695,16 @@ def profile_run(args):
             sel = [i for i in range(len(m.receivers)) if m.rec_rhs[i] < k]
             g.set_receivers(g.locate(m.receivers[sel], c.rec_charac), m.receivers[sel], rec_rhs=m.rec_rhs[sel])
         st = g.stats()
+        if args.solve_only > 0:
+            # one factorisation and K single-column solves with the analysis's
+            # default plan (no tuning): the sweep kernels launch 4 K times only
+            g.factor(1, c.t0 / c.sp_division)
+            b = np.random.default_rng(0).standard_normal(int(st["n"]))
+            for _ in range(args.solve_only):
+                x = g.solve(1, b)
+            print(json.dumps({"config": args.config, "plan": g.solve_plan(), "stored": st["stored"],
+                              "finite": bool(np.isfinite(x).all())}))
+            return 0
         if args.timeline:
             g.factor(1, c.t0 / c.sp_division)
             split, cand = g.tune_solve(1, 1)
@@ -771,12 +782,14 @@ def main():
     ap.add_argument("--timeline-out", default="", help="profiling: also save the raw timeline rows (.npz)")
     ap.add_argument("--plans", default="", help="profiling, with --timeline: sweep spans of forced plans "
                     "'level,split,leaders;...' (leaders 0/1)")
+    ap.add_argument("--solve-only", type=int, default=0,
+                    help="profiling: one factorisation and this many single-column solves (default plan)")
     ap.add_argument("--rhs", type=int, default=0, help="profiling, config 2: the first RHS loops only (0 = all)")
     ap.add_argument("--h-core", type=float, default=0.0, help="profiling: core cell size override (m)")
     ap.add_argument("--replicate", type=int, default=1,
                     help="profiling: solve the config's loop as this many identical RHS columns")
     args = ap.parse_args()
-    if args.profile_steps > 0 or args.timeline:
+    if args.profile_steps > 0 or args.timeline or args.solve_only > 0:
         return profile_run(args)
     if args.impl == "reference":
         return reference_arm(args)
