@@ -187,11 +187,50 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 
 constexpr int kLdsU = kUpdTile + 8;  // 72 doubles: two 128-byte wavefronts per fragment load
 
-// 8-byte asynchronous global -> shared copy (L1-allocating; only for panels
-// no CTA of the running kernel writes)
-__device__ __forceinline__ void cp_async8_f(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+// Bulk global -> shared copies on the TMA engine (cp.async.bulk, this GPU's
+// own memory, no multicast), completed on an mbarrier: one instruction per
+// panel column segment instead of one 8-byte copy per element.  Addresses
+// and sizes must be multiples of 16 bytes: a segment that starts at an odd
+// double is copied from one double earlier (its rows then start at offset 1
+// of the shared row), and the size is rounded up to 16 bytes -- at most one
+// double past the segment, which stays inside the slot allocation (the
+// panels are followed by the scaled diagonal copies).
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, unsigned bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const double* src, unsigned bytes, uint64_t* b) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_u32(b))
+               : "memory");
+}
+// Bounded wait for a phase of the copy barrier: gives up after ~seconds and
+// reports through the error word (the factor is then refused by the host).
+constexpr int kCopySpinLimit = 1 << 22;
+__device__ __forceinline__ void mbar_wait(uint64_t* b, unsigned parity, int* err) {
+  for (int it = 0; !mbar_try_wait(b, parity); ++it) {
+    if (it > kCopySpinLimit) {
+      atomicExch(err, 1);
+      return;
+    }
+    if (it > 64) __nanosleep(32);
+  }
 }
 
 // Schur update tiles.  A tile (s, i0, j0, members m, column limit jl) holds
@@ -203,21 +242,24 @@ __device__ __forceinline__ void cp_async8_f(void* smem, const void* gmem) {
 // m = 1 otherwise.  jl > 0 restricts the tile to columns j < jl (inside a run,
 // a member updates the later members' columns only).  C is scattered into the
 // ancestors' panels through the relative indices of s.  The K loop runs over
-// 16-column chunks of the members, double-buffered: the next chunk's copies
-// are in flight while the DMMA tiles consume the current one (37 KB of
+// 16-column chunks of the members, double-buffered: the next chunk's bulk
+// copies (one per column segment of A and of B: 32 per chunk, issued by warp
+// 0) are in flight while the DMMA tiles consume the current one (37 KB of
 // shared memory: five CTAs per SM, by registers, where 32-column chunks
 // allowed three).
 constexpr int kUpdChunk = 16;
 constexpr int kUpdMaxMembers = 8;
 
-__global__ void __launch_bounds__(128) k_update(
+__global__ void __launch_bounds__(128, 5) k_update(
     const UpdTile* __restrict__ tiles, const int* __restrict__ sn_first,
     const int64_t* __restrict__ rows_ptr, const int* __restrict__ sn_rows,
     const int64_t* __restrict__ Lptr, const int* __restrict__ row_grp,
     const int* __restrict__ grp_target, const int* __restrict__ grp_shift,
     const int64_t* __restrict__ grp_relind, const int* __restrict__ relind, double* __restrict__ L,
-    int use_atomics, const double* __restrict__ sgn) {
-  extern __shared__ double sm[];
+    int use_atomics, const double* __restrict__ sgn, int* __restrict__ err) {
+  extern __shared__ __align__(128) double sm[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ unsigned char shift[2][2][kUpdChunk];  // per buffer, operand, row: offset of the segment's first row
   // [buffer][A | B][kUpdChunk][kLdsU]
   auto As = [&](int buf) { return sm + (size_t)buf * 2 * kUpdChunk * kLdsU; };
   auto Bs = [&](int buf) { return sm + (size_t)buf * 2 * kUpdChunk * kLdsU + kUpdChunk * kLdsU; };
@@ -252,18 +294,26 @@ __global__ void __launch_bounds__(128) k_update(
     const int rq = (int)(rows_ptr[q + 1] - rows_ptr[q]);
     const int64_t ldq = cq + rq;
     const double* P = L + Lptr[q] + cq + (rq - r);  // row 0 of the rows beyond the run
-    double* A = As(buf);
-    double* B = Bs(buf);
-    for (int idx = tid; idx < kUpdChunk * kUpdTile; idx += blockDim.x) {
-      const int k = idx / kUpdTile, ii = idx % kUpdTile;
-      const int kk = k0 + k;
-      const int gi = tile.i0 + ii, gj = tile.j0 + ii;
-      if (kk < cq && gi < r) cp_async8_f(A + k * kLdsU + ii, P + (int64_t)kk * ldq + gi);
-      else A[k * kLdsU + ii] = 0.0;
-      if (kk < cq && gj < r) cp_async8_f(B + k * kLdsU + ii, P + (int64_t)kk * ldq + gj);
-      else B[k * kLdsU + ii] = 0.0;
+    if (tid < 2 * kUpdChunk) {  // warp 0: one segment each (operand A rows i0.., B rows j0..)
+      const int op = tid / kUpdChunk, k = tid % kUpdChunk, kk = k0 + k;
+      const int g0 = op == 0 ? tile.i0 : tile.j0;
+      double* row = (op == 0 ? As(buf) : Bs(buf)) + k * kLdsU;
+      if (kk < cq && g0 < r) {
+        const double* src = P + (int64_t)kk * ldq + g0;
+        const int n = min(kUpdTile, r - g0);  // rows past r only feed outputs that are not scattered
+        const int o = (__cvta_generic_to_global(src) & 15) ? 1 : 0;
+        const unsigned bytes = (unsigned)(((n + o) * 8 + 15) & ~15);
+        shift[buf][op][k] = (unsigned char)o;
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(&mbar[buf], bytes);
+        bulk_g2s(row, src - o, bytes, &mbar[buf]);
+      } else {  // past the member's columns: a zero row
+        shift[buf][op][k] = 0;
+        for (int ii = 0; ii < kUpdTile; ++ii) row[ii] = 0.0;
+      }
+      __syncwarp();
+      if (tid == 0) mbar_arrive(&mbar[buf]);
     }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
   const int warp = tid >> 5, lane = tid & 31;
   const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;
@@ -273,15 +323,19 @@ __global__ void __launch_bounds__(128) k_update(
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+  if (tid == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  unsigned phases = 0u;  // bit b: parity of buffer b's next phase
   issue(0);
   for (int ch = 0; ch < nch; ++ch) {
     const int buf = ch & 1;
-    if (ch + 1 < nch) {
-      issue(buf ^ 1);
-      asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-    } else {
-      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    }
+    if (ch + 1 < nch) issue(buf ^ 1);
+    mbar_wait(&mbar[buf], (phases >> buf) & 1u, err);
+    phases ^= 1u << buf;
     __syncthreads();
     double* A = As(buf);
     const double* B = Bs(buf);
@@ -290,7 +344,7 @@ __global__ void __launch_bounds__(128) k_update(
       const int cq = sn_first[mm_q + 1] - fq;
       for (int idx = tid; idx < kUpdChunk * kUpdTile; idx += blockDim.x) {
         const int k = idx / kUpdTile, ii = idx % kUpdTile;
-        if (mm_k0 + k < cq) A[k * kLdsU + ii] *= sgn[fq + mm_k0 + k];
+        if (mm_k0 + k < cq) A[k * kLdsU + shift[buf][0][k] + ii] *= sgn[fq + mm_k0 + k];
       }
       __syncthreads();
     }
@@ -298,10 +352,11 @@ __global__ void __launch_bounds__(128) k_update(
 #pragma unroll 2
     for (int k0 = 0; k0 < kUpdChunk; k0 += 4) {
       double fa[4], fb[4];
+      const int sa = shift[buf][0][k0 + qd], sb = shift[buf][1][k0 + qd];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) fa[a] = A[(k0 + qd) * kLdsU + wr + a * 8 + g];
+      for (int a = 0; a < 4; ++a) fa[a] = A[(k0 + qd) * kLdsU + sa + wr + a * 8 + g];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) fb[b] = B[(k0 + qd) * kLdsU + wc + b * 8 + g];
+      for (int b = 0; b < 4; ++b) fb[b] = B[(k0 + qd) * kLdsU + sb + wc + b * 8 + g];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -496,9 +551,13 @@ int numeric_factor_values_fallback(temf_ctx& c, int slot, const double* X, doubl
 
 int finish_factor(temf_ctx& c, int slot) {
   FactorSlot& fs = c.slots[slot];
-  int words[3] = {0, 0, 0};
-  TEMF_CUDA(cudaMemcpyAsync(words, c.d_status.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  int words[4] = {0, 0, 0, 0};
+  TEMF_CUDA(cudaMemcpyAsync(words, c.d_status.p, 4 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   TEMF_CUDA(cudaStreamSynchronize(c.stream));
+  if (words[3] != 0) {
+    fs.valid = false;
+    throw StateError("a factor update's panel copies did not complete (bounded wait timed out)");
+  }
   const int status = words[0];
   fs.perturbed = fs.indefinite ? words[2] : 0;
   if (status != INT_MAX) {
@@ -528,6 +587,7 @@ void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
   int init[3] = {INT_MAX, 0, 0};
   TEMF_CUDA(cudaMemcpyAsync(c.d_status.p, &init[0], sizeof(int), cudaMemcpyHostToDevice, st));
   TEMF_CUDA(cudaMemcpyAsync(c.d_status.p + 2, &init[2], sizeof(int), cudaMemcpyHostToDevice, st));
+  TEMF_CUDA(cudaMemcpyAsync(c.d_status.p + 3, &init[1], sizeof(int), cudaMemcpyHostToDevice, st));  // copy waits
   fs.X = X;
   fs.a = a;
   fs.Y = Y;
@@ -563,7 +623,7 @@ void launch_factor_values(temf_ctx& c, int slot, const double* X, double a, cons
       k_update<<<(unsigned)(t1 - t0), 128, upd_smem, st>>>(F.tiles.p + t0, F.sn_first.p, F.sn_rows_ptr.p,
                                                           F.sn_rows.p, F.sn_Lptr.p, F.row_grp.p, F.grp_target.p,
                                                           F.grp_shift.p, F.grp_relind.p, F.relind.p, fs.L.p,
-                                                          cnt > 1 ? 1 : 0, sgn);
+                                                          cnt > 1 ? 1 : 0, sgn, c.d_status.p + 3);
       TEMF_CHECK_LAUNCH();
     }
   }

@@ -1764,13 +1764,14 @@ struct Sched {
 // (kind 4) after the claimable tasks.  The targets / owners of a run block's
 // first chunk exclude the run's own blocks (applied through the leader's
 // ring).  Single right-hand side only (128-row first chunks).
-// group_from: at levels from this one up, the tasks of a level are ordered
-// by kind instead of by supernode (forward: every diagonal task of the level,
-// then the other chunks; backward: every other chunk, then the diagonal
-// tasks), so a task claimed in schedule order finds the tasks it waits for
-// claimed a whole level's worth earlier.  Only above the queue split: the
-// queued forward tasks rely on a supernode's chunks following its diagonal
-// task.
+// group_from: at levels from this one up, the tasks are ordered for in-order
+// claiming.  Forward: a level's diagonal tasks first; each other chunk is held
+// back until just before the diagonal tasks of the lowest level it feeds, so
+// chunks claimed in order find their own diagonal task long done and the
+// next level's diagonal tasks are not queued behind chunks that feed levels
+// far above.  Backward: every other chunk of a level, then its diagonal
+// tasks.  Only above the queue split: the queued forward tasks rely on a
+// supernode's chunks following its diagonal task.
 void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lead_level = INT_MAX,
                  int group_from = INT_MAX) {
   const int nsn = S.nsn;
@@ -1823,16 +1824,24 @@ void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lea
   }
   std::vector<SolveTask> abs_t;
   std::vector<std::vector<int>> abs_g;
+  // forward chunks above group_from, by the lowest level among their targets
+  std::vector<std::vector<std::pair<SolveTask, std::vector<int>>>> late(S.nlevels + 1);
   // forward: bottom-up levels; per supernode its diagonal task (with the first
   // row chunk), then the other chunks
-  for (int l = std::max(0, min_level); l < S.nlevels; ++l)
-    for (int pass = 0; pass < (l >= group_from ? 2 : 1); ++pass)
+  for (int l = std::max(0, min_level); l < S.nlevels; ++l) {
+    const bool grouped = l >= group_from;
     for (int q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
       const int s = S.level_sn[q];
       const int r = (int)(S.sn_rows_ptr[s + 1] - S.sn_rows_ptr[s]);
       for (int r0 = 0; r0 < std::max(r, 1); r0 += CH) {
-        if (l >= group_from && (pass == 0) != (r0 == 0)) continue;
         const int r1 = std::min(r, r0 + CH);
+        if (grouped && r0 > 0) {  // held back until just before its first consumer's level
+          owners(s, r0, r1);
+          int mlev = S.nlevels - 1;
+          for (int ow : tmp) mlev = std::min(mlev, S.sn_level[ow]);
+          late[mlev].push_back({SolveTask{s, 1, r0, r1}, tmp});
+          continue;
+        }
         if (r0 == 0 && run_a[s] >= 0) {
           owners(s, 0, r1, run_e[s]);
           for (int ow : tmp) o.expect[ow]++;
@@ -1852,6 +1861,16 @@ void build_sched(const Symbolic& S, int CH, Sched& o, int min_level = 0, int lea
         o.ftp.push_back((int)o.ftg.size());
       }
     }
+    // the chunks whose first consumer is at the next level, before its diagonal tasks
+    if (l + 1 < S.nlevels) {
+      for (auto& e : late[l + 1]) {
+        o.ft.push_back(e.first);
+        for (int ow : e.second) { o.ftg.push_back(ow); o.expect[ow]++; }
+        o.ftp.push_back((int)o.ftg.size());
+      }
+      late[l + 1].clear();
+    }
+  }
   o.nf = (int)o.ft.size();
   for (size_t k = 0; k < abs_t.size(); ++k) {
     o.ft.push_back(abs_t[k]);

@@ -238,3 +238,24 @@ def golden_decisions(gold, sp_double):
         out.append(bool(after > 1.5 * before))
         s += sp_double
     return out
+
+
+def free_divergence_explained(k, gpu_error, oracle_errors, file_decisions):
+    """Whether a free GPU run may part from a shipped .field at trial k.
+
+    The file's build decided trial k by its own estimate; the oracle's
+    estimates (the file's own decision history replayed) stand in for it.
+    Either the restated rule itself disagrees with the file at k (the oracle's
+    estimate, with the file's not_changed count, falls on the other side of
+    1e-4: the reference build's own rounding decided it), or the GPU's and
+    the oracle's estimates lie on both sides of 1e-4 or further apart than
+    the oracle's is from it (solver rounding in the air fields that dominate
+    the late estimates)."""
+    ora = float(oracle_errors[k])
+    not_changed = 0
+    for d in file_decisions[:k]:
+        not_changed = 0 if d else not_changed + 1
+    oracle_accepts = not (ora > 1e-4 and not_changed < 2)  # src/FETD_FWD.f90:1382
+    if oracle_accepts != file_decisions[k]:
+        return True
+    return (gpu_error - 1e-4) * (ora - 1e-4) < 0 or abs(gpu_error - ora) >= abs(ora - 1e-4)

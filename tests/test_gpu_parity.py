@@ -241,7 +241,10 @@ def test_linux_examples_match_reference_field(name):
        1e-12 S/m air leaves nearly undetermined (the receiver dB/dt agree to
        1e-14 while those estimates differ between solvers by tens of percent),
        so the GPU's and the oracle's estimates must lie on both sides of 1e-4,
-       or further apart than the oracle's estimate is from it."""
+       or further apart than the oracle's estimate is from it -- or the
+       restated rule on the oracle's estimate (file history) must itself
+       decide differently from the file there, as at trial 19 of
+       mod_small."""
     from tests.golden_cases import GOLDEN, golden_field_report
     fx = load_fixture(name)
     z = np.load(os.path.join(GOLDEN, "oracle_" + name + ".npz"))
@@ -265,10 +268,11 @@ def test_linux_examples_match_reference_field(name):
           % (name, len(out.steps), len(gold), first, decided, rel))
     assert rel < 6e-4, rel
     if first < len(gold) or len(out.steps) != len(gold):
+        from tests.golden_cases import free_divergence_explained, golden_decisions
         k = int(out.steps[min(first, len(out.steps) - 1)]) // ctl.sp_double - 1
-        ora = float(z["trial_errors"][k])
         assert decided is not None
-        assert (decided - 1e-4) * (ora - 1e-4) < 0 or abs(decided - ora) >= abs(ora - 1e-4), (k, decided, ora)
+        assert free_divergence_explained(k, decided, z["trial_errors"], golden_decisions(gold, ctl.sp_double)), \
+            (k, decided, float(z["trial_errors"][k]))
 
 
 def test_multi_rhs_columns_match_single_runs():
