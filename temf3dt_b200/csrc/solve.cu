@@ -642,11 +642,27 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
     else load_diag_start(D, P, c, ld);
   }
   const bool queued = in_queue(V, t);
+  // Diagonal task, one column: y_s (written by the forward sweep only) is read
+  // before any wait, and the column sums of the other chunks once their count
+  // is complete, while the owner of the first chunk's rows is still awaited
+  // (on the top chain that owner is the block just above, finished last).
+  const bool pre = T.kind == 0 && nrhs == 1 && V.bacc != nullptr;
+  const bool more = V.nchunk[s] > 1;
+  double y_pre = 0.0, acc_pre = 0.0;
+  if (pre && tid < c) y_pre = __ldcg(x + f + tid);
   // the chunk's rows need their owners' x; the diagonal task also its other chunks
   if (!queued) {  // one polling thread per owner (and one for the chunk count)
     const int q0 = V.tgt_ptr[t], nq = V.tgt_ptr[t + 1] - q0;
+    if (pre) {
+      if (tid == blockDim.x - 1) wait_geq(cdone + s, V.nchunk[s] - (nr > 0 ? 1 : 0), err, 4, spin_limit(V));
+      __syncthreads();
+      if (tid < c && more) acc_pre = __ldcg(V.bacc + f + tid);
+    }
     for (int q = tid; q < nq; q += blockDim.x) wait_geq(xdone + V.tgt[q0 + q], 1, err, 3, spin_limit(V));
-    if (T.kind == 0 && tid == blockDim.x - 1) wait_geq(cdone + s, V.nchunk[s] - (nr > 0 ? 1 : 0), err, 4, spin_limit(V));
+    if (!pre && T.kind == 0 && tid == blockDim.x - 1)
+      wait_geq(cdone + s, V.nchunk[s] - (nr > 0 ? 1 : 0), err, 4, spin_limit(V));
+  } else if (pre && tid < c && more) {
+    acc_pre = __ldcg(V.bacc + f + tid);
   }
   __syncthreads();
   if (stamp && tid == 0) *stamp = gtime();
@@ -699,12 +715,13 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
       // the other chunks' partials: thread (j, h) sums chunks q = 1 + h, 3 + h, ...
       // with eight loads in flight; fixed order, so still deterministic
       double* psum = zx;  // the chunk rows are consumed: reuse as [2][64]
-      if (nch > 1 && V.bacc) {
-        for (int j = tid; j < c; j += blockDim.x) {
-          psum[j] = __ldcg(V.bacc + f + j);
-          psum[kSnCols + j] = 0.0;
+      if (pre) {  // y_s and the column sums are in registers (c <= blockDim.x)
+        if (tid < c) {
+          double v = y_pre;
+          if (nr > 0) v -= (seg[0][tid] + seg[1][tid]) + (seg[2][tid] + seg[3][tid]);
+          if (more) v -= acc_pre;
+          zs[tid] = v;
         }
-        __syncthreads();
       } else if (nch > 1) {
         const int j = tid & (kSnCols - 1), h = tid / kSnCols;
         double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -721,11 +738,13 @@ __device__ __forceinline__ void bwd_task(const SweepView& V, int t, const double
         if (h < 2) psum[h * kSnCols + j] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
         __syncthreads();
       }
-      for (int j = tid; j < c; j += blockDim.x) {
-        double v = __ldcg(x + f + j);
-        if (nr > 0) v -= (seg[0][j] + seg[1][j]) + (seg[2][j] + seg[3][j]);
-        if (nch > 1) v -= psum[j] + psum[kSnCols + j];
-        zs[j] = v;
+      if (!pre) {
+        for (int j = tid; j < c; j += blockDim.x) {
+          double v = __ldcg(x + f + j);
+          if (nr > 0) v -= (seg[0][j] + seg[1][j]) + (seg[2][j] + seg[3][j]);
+          if (nch > 1) v -= psum[j] + psum[kSnCols + j];
+          zs[j] = v;
+        }
       }
     } else {
       for (int idx = tid; idx < c * nrhs; idx += blockDim.x) {
@@ -2931,7 +2950,8 @@ static std::vector<int> split_candidates(const Symbolic& S, int level) {
 
 // Autotuner of the single-column plan: first the subtree level (0 = none, and
 // the levels below which there are enough subtrees to fill the GPU twice),
-// each with the default queue split, then the queue split at the best level.
+// each with the default queue split, then the queue split at the best level,
+// both without run leaders, then the best plan with them.
 // Times one solve (right-hand side all ones) per candidate, keeps the fastest.
 static int tune_tree(temf_ctx& c, int slot) {
   const Symbolic& S = c.sym;
@@ -2951,7 +2971,7 @@ static int tune_tree(temf_ctx& c, int slot) {
   TEMF_CUDA(cudaEventCreate(&e1));
   std::vector<int> lv_c, sp_c;
   std::vector<double> ms_c;
-  auto time_plan = [&](int level, int split, bool leaders = true) {
+  auto time_plan = [&](int level, int split, bool leaders = false) {
     upload_tree_plan(c, level, split, leaders);
     double tot = 0.0;
     for (int rep = 0; rep < 4; ++rep) {
@@ -2990,11 +3010,12 @@ static int tune_tree(temf_ctx& c, int slot) {
     sms.push_back(ms);
     if (ms < best) { best = ms; best_split = sp; }
   }
-  // and the chosen plan without run leaders (every block handed from CTA to CTA)
-  bool best_leaders = true;
+  // and the chosen plan with run leaders (the level and split candidates are
+  // timed without: the leader instances carry more registers)
+  bool best_leaders = false;
   {
-    const double ms = time_plan(best_level, best_split, false);
-    if (ms < best) { best = ms; best_leaders = false; }
+    const double ms = time_plan(best_level, best_split, true);
+    if (ms < best) { best = ms; best_leaders = true; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
