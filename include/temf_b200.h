@@ -131,13 +131,15 @@ int temf_solve(temf_ctx* ctx, int slot, int nrhs, const double* b, double* x, in
  *   the library holds until the process exits.  A factor whose solve needs
  *   more returns TEMF_EARG with the byte count; use temf_solve then.
  * - The first call on a device looks the array's address up (set-up), so make
- *   that first call before any stream capture.
+ *   that first call before another thread starts a stream capture.
  * - Every call shares the array, so calls whose GPU work overlaps (two
  *   contexts, two threads, two devices' calls are separate arrays) race.
  *   Serialise them.
  * - The call runs on the context's stream and blocks: it synchronises that
  *   stream and returns after the solve finished, with the status of its
- *   waits. */
+ *   waits.  So it cannot itself be recorded into a CUDA graph (a stream
+ *   synchronise is not allowed during capture); what it avoids is allocating
+ *   while other work is being captured. */
 int temf_solve_noalloc(temf_ctx* ctx, int slot, const double* b_dev, double* x_dev);
 /* Forget the factor in `slot` (pardiso_direct_3, src/FETD_UTILITY.f90:959-975).
  * Device memory is kept for reuse until temf_destroy. */
