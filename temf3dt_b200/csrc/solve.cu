@@ -2321,6 +2321,8 @@ int default_tree_level(const Symbolic& S, int min_roots = 2 * 148 * 12) {
 }
 }  // namespace
 
+void upload_multi_plan(temf_ctx& c, int split);
+
 void build_solve_plan(temf_ctx& c) {
   const Symbolic& S = c.sym;
   SolvePlan& P = c.splan;
@@ -2344,8 +2346,22 @@ void build_solve_plan(temf_ctx& c) {
   P.part_off.upload(a.poff.data(), a.poff.size(), st);
   upload_queue_plan(a, S, default_split(S), P.q1, st);
   TEMF_CUDA(cudaStreamSynchronize(st));  // the host vectors of `a` go out of scope
+  upload_multi_plan(c, default_split(S));
+  P.sync.alloc(4 * (size_t)nsn + 8);  // + 2 claim counters of the task kernels, 2 of the subtree kernels
+  upload_tree_plan(c, default_tree_level(S), default_split(S), true);
+  P.tree.tuned = false;
+  TEMF_CUDA(cudaStreamSynchronize(st));
+}
+
+// The 64-column block sweeps' schedules (64-row chunks) at a queue split:
+// the levels above it ordered for in-order claiming (build_sched).
+void upload_multi_plan(temf_ctx& c, int split) {
+  const Symbolic& S = c.sym;
+  SolvePlan& P = c.splan;
+  const int nsn = S.nsn;
+  cudaStream_t st = c.stream;
   Sched b;
-  build_sched(S, kChunkRowsMulti, b);
+  build_sched(S, kChunkRowsMulti, b, 0, INT_MAX, split);
   P.n_mftask = (int)b.ft.size();
   P.n_mbtask = (int)b.bt.size();
   P.mftask.upload(b.ft.data(), b.ft.size(), st);
@@ -2360,11 +2376,7 @@ void build_solve_plan(temf_ctx& c) {
   for (int s = 0; s < nsn; ++s) aoff[s + 1] = aoff[s] + (b.nch[s] > 1 ? S.sn_first[s + 1] - S.sn_first[s] : 0);
   P.macc_len = aoff[nsn];
   P.macc_off.upload(aoff.data(), aoff.size(), st);
-  upload_queue_plan(b, S, default_split(S), P.qm, st);
-  P.sync.alloc(4 * (size_t)nsn + 8);  // + 2 claim counters of the task kernels, 2 of the subtree kernels
-  upload_tree_plan(c, default_tree_level(S), default_split(S), true);
-  P.tree.tuned = false;
-  TEMF_CUDA(cudaStreamSynchronize(st));
+  upload_queue_plan(b, S, split, P.qm, st);  // synchronises: the host vectors go out of scope
 }
 
 void ensure_update_buffer(temf_ctx& c, int nrhs) {
@@ -2856,7 +2868,7 @@ std::string check_schedules(const Symbolic& S) {
     if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ", grouped levels: " + w;
     w = check_schedule(S, kChunkRows, sp, 0, sp, true);
     if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ", run leaders: " + w;
-    w = check_schedule(S, kChunkRowsMulti, sp);
+    w = check_schedule(S, kChunkRowsMulti, sp, 0, INT_MAX, true);
     if (!w.empty()) return "64-row chunks, split " + std::to_string(sp) + ": " + w;
   }
   // the single-column plans with subtrees: every level the tuner may pick,
@@ -2887,7 +2899,7 @@ int tune_solve(temf_ctx& c, int slot, int nrhs) {
   QueuePlan& Q = block ? P.qm : P.q1;
   cudaStream_t st = c.stream;
   Sched a;
-  build_sched(S, block ? kChunkRowsMulti : kChunkRows, a);
+  if (!block) build_sched(S, kChunkRows, a);
   std::vector<int> cand = {0, level_below_width(S, 4096), level_below_width(S, 1024), level_below_width(S, 512),
                            level_below_width(S, 148), level_below_width(S, 32), S.nlevels};
   std::sort(cand.begin(), cand.end());
@@ -2909,7 +2921,8 @@ int tune_solve(temf_ctx& c, int slot, int nrhs) {
   int best = Q.split;
   double best_ms = 1e30;
   for (int sp : cand) {
-    upload_queue_plan(a, S, sp, Q, st);
+    if (block) upload_multi_plan(c, sp);
+    else upload_queue_plan(a, S, sp, Q, st);
     double tot = 0.0;
     for (int rep = 0; rep < 4; ++rep) {
       TEMF_CUDA(cudaMemcpyAsync(x.p, ones.p, vec * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -2931,7 +2944,8 @@ int tune_solve(temf_ctx& c, int slot, int nrhs) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  upload_queue_plan(a, S, best, Q, st);
+  if (block) upload_multi_plan(c, best);
+  else upload_queue_plan(a, S, best, Q, st);
   Q.tuned = true;
   return best;
 }
