@@ -2046,9 +2046,10 @@ void upload_queue_plan(const Sched& a, const Symbolic& S, int split, QueuePlan& 
 // round, the ordered tasks' completions feeding the queue.  Returns an empty
 // string or the first violation.
 std::string check_schedule(const Symbolic& S, int CH, int split, int min_level = 0, int lead_level = INT_MAX,
-                           bool grouped = false) {
+                           bool grouped = false, int group_at = -1) {
   Sched a;
-  build_sched(S, CH, a, min_level, lead_level, grouped ? std::max(split, min_level) : INT_MAX);
+  build_sched(S, CH, a, min_level, lead_level,
+              grouped ? (group_at >= 0 ? group_at : std::max(split, min_level)) : INT_MAX);
   int f_hi = 0, b_lo = 0;
   split_ranges(a, S, split, f_hi, b_lo);
   QueueData q;
@@ -2331,7 +2332,7 @@ void build_solve_plan(temf_ctx& c) {
   P.u_len = (int64_t)S.sn_rows.size();
   cudaStream_t st = c.stream;
   Sched a;
-  build_sched(S, kChunkRows, a);
+  build_sched(S, kChunkRows, a, 0, INT_MAX, default_split(S));  // above the split: ordered for claiming
   P.n_ftask = (int)a.ft.size();
   P.n_btask = (int)a.bt.size();
   P.ftask.upload(a.ft.data(), a.ft.size(), st);
@@ -2866,6 +2867,12 @@ std::string check_schedules(const Symbolic& S) {
     if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ": " + w;
     w = check_schedule(S, kChunkRows, sp, 0, INT_MAX, true);
     if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ", grouped levels: " + w;
+    // the allocation-free path (everything claimed in order) and the model batches (queue split
+    // at the default): their schedule is grouped at the default split
+    if (sp <= default_split(S)) {
+      w = check_schedule(S, kChunkRows, sp, 0, INT_MAX, true, default_split(S));
+      if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ", grouped at the default: " + w;
+    }
     w = check_schedule(S, kChunkRows, sp, 0, sp, true);
     if (!w.empty()) return "128-row chunks, split " + std::to_string(sp) + ", run leaders: " + w;
     w = check_schedule(S, kChunkRowsMulti, sp, 0, INT_MAX, true);
