@@ -391,13 +391,13 @@ def batched_measure(local: int, plain_value: float, check_cols=(0, 27, 36, 63)):
 def layered_models(n_models: int = 16, seed: int = 5):
     """Independent 1-D layered models (3-6 layers, conductivities log-uniform
     in [1e-4, 1e-1] S/m, thicknesses log-uniform in [10, 300] m) on graded
-    meshes of uneven size (mesh density drawn log-uniformly; about 0.1M to
-    0.7M edges)."""
+    meshes of uneven size (mesh density drawn log-uniformly in [0.26, 1.5];
+    with seed 5 the 16 meshes hold 101 525 to 986 423 edges)."""
     from temf3dt_b200 import synth
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n_models):
-        sc = float(np.exp(rng.uniform(np.log(0.3), np.log(0.9))))
+        sc = float(np.exp(rng.uniform(np.log(0.26), np.log(1.5))))
         kw = dict(COMMON)
         out.append(synth.build_model("layered", seed=100 + i, scale=sc, ratio=2.0, **kw))
     return out
