@@ -279,7 +279,8 @@ def adjoint_measure(local: int, fd_cells: int = 0):
             hit = np.unique(md["cell"][md["cell"] >= 0])
             pick = np.random.default_rng(32).choice(hit, size=min(fd_cells, len(hit)), replace=False)
             h = 1e-3
-            rel = []
+            scale = float(np.abs(grad).max())
+            rel, fds, tol_used = [], [], []
             for k in pick:
                 Jpm = []
                 for sgn in (1.0, -1.0):
@@ -290,10 +291,16 @@ def adjoint_measure(local: int, fd_cells: int = 0):
                     ok = g.run(*args, forced=forced)
                     Jpm.append(inversion.dbdt_misfit(ok.fields, ok.times, GATES, d_obs)[0])
                 fd = (Jpm[0] - Jpm[1]) / (2 * h)
+                fds.append(float(fd))
                 rel.append(abs(fd - grad[k]) / max(abs(fd), 1e-300))
-            scale = float(np.abs(grad).max())
+                # the GPU test's bound: 1e-4 relative, plus 1e-6 of the largest cell gradient
+                tol_used.append(abs(fd - grad[k]) / (1e-4 * abs(fd) + 1e-6 * scale))
+                print("fd cell %d: fd %.9e adjoint %.9e rel %.2e" % (k, fd, grad[k], rel[-1]),
+                      file=sys.stderr, flush=True)
             out["fd"] = {"cells": [int(k) for k in pick], "max_rel_err": float(max(rel)),
-                         "median_rel_err": float(np.median(rel)), "step": h, "grad_max": scale}
+                         "median_rel_err": float(np.median(rel)), "step": h, "grad_max": scale,
+                         "fd": fds, "adjoint": [float(grad[k]) for k in pick],
+                         "max_err_over_test_bound": float(max(tol_used))}
     return out
 
 
