@@ -137,9 +137,7 @@ int temf_solve(temf_ctx* ctx, int slot, int nrhs, const double* b, double* x, in
  *   Serialise them.
  * - The call runs on the context's stream and blocks: it synchronises that
  *   stream and returns after the solve finished, with the status of its
- *   waits.  So it cannot itself be recorded into a CUDA graph (a stream
- *   synchronise is not allowed during capture); what it avoids is allocating
- *   while other work is being captured. */
+ *   waits. */
 int temf_solve_noalloc(temf_ctx* ctx, int slot, const double* b_dev, double* x_dev);
 /* Forget the factor in `slot` (pardiso_direct_3, src/FETD_UTILITY.f90:959-975).
  * Device memory is kept for reuse until temf_destroy. */
