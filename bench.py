@@ -400,14 +400,19 @@ def layered_models(n_models: int = 16, seed: int = 5):
     in [1e-4, 1e-1] S/m, thicknesses log-uniform in [10, 300] m) on graded
     meshes of uneven size (mesh density drawn log-uniformly in [0.26, 1.5];
     with seed 5 the 16 meshes hold 101 525 to 986 423 edges)."""
-    from temf3dt_b200 import synth
+    return [layered_model(i, sc) for i, sc in enumerate(layered_model_scales(n_models, seed))]
+
+
+def layered_model_scales(n_models: int = 16, seed: int = 5):
+    """The mesh-density scale of each layered model (log-uniform in [0.26, 1.5])."""
     rng = np.random.default_rng(seed)
-    out = []
-    for i in range(n_models):
-        sc = float(np.exp(rng.uniform(np.log(0.26), np.log(1.5))))
-        kw = dict(COMMON)
-        out.append(synth.build_model("layered", seed=100 + i, scale=sc, ratio=2.0, **kw))
-    return out
+    return [float(np.exp(rng.uniform(np.log(0.26), np.log(1.5)))) for _ in range(n_models)]
+
+
+def layered_model(i: int, scale: float):
+    """Layered model i of the batch (its own seed) at the given mesh scale."""
+    from temf3dt_b200 import synth
+    return synth.build_model("layered", seed=100 + i, scale=scale, ratio=2.0, **COMMON)
 
 
 def models_measure(local: int, n_models: int = 16):

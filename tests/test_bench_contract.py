@@ -35,3 +35,21 @@ def test_gpu_line_cpu_baseline_runs_in_a_fresh_process():
     assert cpu.get("value") and cpu["value"] > 0, cpu
     assert cpu["unit"] == "steps*RHS/s" and cpu["kind"] == "port" and cpu["cores"] >= 1
     assert "amortised" in cpu["sample"]
+
+
+def test_model_batch_spans_100k_to_1m_edges():
+    """The bench's 16 layered models have the uneven sizes of the multi-model
+    batch they stand for (100k to 1M edges): the two coarsest hold 101 525
+    and 105 367 edges, the finest 986 423."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from temf3dt_b200 import fetd
+    sc = bench.layered_model_scales()
+    assert len(sc) == 16 and 0.26 <= min(sc) and max(sc) <= 1.5
+    order = sorted(range(16), key=lambda i: sc[i])
+
+    def edges(i):
+        return fetd.mesh_topology(bench.layered_model(i, sc[i]).mesh.tet_vex)[0].shape[0]
+
+    assert sorted([edges(order[0]), edges(order[1])]) == [101525, 105367]
+    assert edges(order[-1]) == 986423
