@@ -14,7 +14,8 @@ and sign conventions can be compared line by line.
 
 Parity is pinned against the reference's shipped example outputs
 ``LINUX/mod_big_sig_0.001.field`` and ``LINUX/mod_small_sig_0.001.field``
-(see ``tests/test_oracle_golden.py``).
+(row for row) and ``src_small/mod_small_sig_0.001.field`` (5 digits, up to
+the first trial decided by solver noise), in ``tests/test_oracle.py``.
 """
 from __future__ import annotations
 
