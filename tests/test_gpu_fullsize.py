@@ -1,4 +1,4 @@
-"""Parity at the bench's full size: the first time steps of the 1.2M-edge
+"""Parity at the bench's full size: the first time steps of the 1.48M-edge
 block model on the GPU against the oracle's adaptive loop on the CPU
 supernodal Cholesky (an independent factor/solve on the host cores, same
 ordering), receiver by receiver."""
