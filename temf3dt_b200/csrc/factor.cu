@@ -188,7 +188,7 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 constexpr int kLdsU = kUpdTile + 8;  // 72 doubles: two 128-byte wavefronts per fragment load
 
 // Bulk global -> shared copies on the TMA engine (cp.async.bulk, this GPU's
-// own memory, no multicast), completed on an mbarrier: one instruction per
+// own memory, each CTA its own copy), completed on an mbarrier: one instruction per
 // panel column segment instead of one 8-byte copy per element.  Addresses
 // and sizes must be multiples of 16 bytes: a segment that starts at an odd
 // double is copied from one double earlier (its rows then start at offset 1
